@@ -1,0 +1,102 @@
+"""ctypes bindings of the CPU restatements (oracle/_build/liboracle.so).
+
+ORACLE -- test infrastructure only: imported by tests/, by __graft_entry__.smoke() as the
+checker and by bench.py's cpu_baseline leg. The product never imports this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_F32P = ctypes.POINTER(ctypes.c_float)
+_F64P = ctypes.POINTER(ctypes.c_double)
+_I32P = ctypes.POINTER(ctypes.c_int)
+
+
+class OracleAfdCfg(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("nz", ctypes.c_int), ("pml", ctypes.c_int), ("nt", ctypes.c_int),
+        ("dx", ctypes.c_float), ("dz", ctypes.c_float), ("dt", ctypes.c_float),
+        ("radius", ctypes.c_int), ("sx", ctypes.c_int), ("sz", ctypes.c_int),
+        ("nrec", ctypes.c_int), ("rec_x", _I32P), ("rec_z", _I32P), ("snap_step", ctypes.c_int),
+    ]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.oracle_afd_f32.argtypes = [ctypes.POINTER(OracleAfdCfg), _F32P, _F32P, _F32P, _F32P, _F32P, _F32P]
+        _lib.oracle_afd_f64.argtypes = [ctypes.POINTER(OracleAfdCfg), _F32P, _F32P, _F32P, _F64P, _F64P, _F64P]
+        _lib.oracle_afd_sponge.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P]
+        _lib.oracle_afd_coeffs.argtypes = [ctypes.c_int, _F32P]
+        _lib.oracle_wavelet_afd.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, _F32P]
+        _lib.oracle_wavelet_ric.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, _F32P]
+        _lib.oracle_wavelet_afd.restype = None
+        _lib.oracle_wavelet_ric.restype = None
+    return _lib
+
+
+def _p(a, t=_F32P):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def afd_sponge(nx: int, nz: int, pml: int) -> np.ndarray:
+    out = np.empty((nx, nz), np.float32)
+    assert lib().oracle_afd_sponge(nx, nz, pml, _p(out)) == 0
+    return out
+
+
+def afd_coeffs(radius: int) -> np.ndarray:
+    out = np.zeros(8, np.float32)
+    assert lib().oracle_afd_coeffs(radius, _p(out)) == 0
+    return out[:radius]
+
+
+def wavelet_afd(nt: int, dt: float, freq: float) -> np.ndarray:
+    out = np.empty(nt, np.float32)
+    lib().oracle_wavelet_afd(nt, dt, freq, _p(out))
+    return out
+
+
+def wavelet_ric(nt: int, dt: float, f0: int, delay: int = 150) -> np.ndarray:
+    out = np.empty(nt, np.float32)
+    lib().oracle_wavelet_ric(nt, dt, int(f0), int(delay), _p(out))
+    return out
+
+
+def afd_forward(nx, nz, pml, nt, dx, dz, dt, vp, den, wavelet, sx, sz, rec_x, rec_z,
+                radius=8, snap_step=-1, fp64=False, want_state=False):
+    """Run the restated AFD time loop. Returns (record[nrec, nt], snap_vx[nx, nz] or None,
+    final_state[3, nx, nz] (P, Vx, Vz after the sponge) or None)."""
+    rec_x = np.ascontiguousarray(rec_x, np.int32)
+    rec_z = np.ascontiguousarray(rec_z, np.int32)
+    vp = np.ascontiguousarray(vp, np.float32)
+    den = np.ascontiguousarray(den, np.float32)
+    wavelet = np.ascontiguousarray(wavelet, np.float32)
+    assert vp.shape == (nx, nz) and den.shape == (nx, nz) and wavelet.shape[0] >= nt
+    cfg = OracleAfdCfg(nx, nz, pml, nt, dx, dz, dt, radius, sx, sz, len(rec_x),
+                       _p(rec_x, _I32P), _p(rec_z, _I32P), snap_step)
+    dt_ = np.float64 if fp64 else np.float32
+    tp = _F64P if fp64 else _F32P
+    rec = np.zeros((len(rec_x), nt), dt_)
+    snap = np.zeros((nx, nz), dt_) if snap_step >= 0 else None
+    state = np.zeros((3, nx, nz), dt_) if want_state else None
+    fn = lib().oracle_afd_f64 if fp64 else lib().oracle_afd_f32
+    rc = fn(ctypes.byref(cfg), _p(vp), _p(den), _p(wavelet), _p(rec, tp), _p(snap, tp), _p(state, tp))
+    if rc != 0:
+        raise ValueError(f"oracle_afd rejected the configuration (rc={rc})")
+    return rec, snap, state

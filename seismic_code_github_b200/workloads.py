@@ -1,0 +1,121 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+No dataset ships with the reference; every model here is generated from a fixed numpy seed.
+Arrays follow the reference's in-memory layout: x-major, z fastest, float32
+(forward/Acoustic_FD_by_ss/src/Acoustic_1order_FD.cpp:51-100, tools/get_vel_model.cpp:26-45).
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+
+def pad_edges(a: np.ndarray, pml_x: int, pml_z: int) -> np.ndarray:
+    """Edge-replicated padding of an interior (nx, nz) model, the padding rule of
+    forward/Q_forward/Q_multishot_fd_subroutine_fsbc_zy_rotated.f90:340-372."""
+    return np.pad(a, ((pml_x, pml_x), (pml_z, pml_z)), mode="edge").astype(np.float32)
+
+
+@dataclass
+class AcousticCase:
+    name: str
+    NX: int            # interior cells along x
+    NZ: int            # interior cells along z
+    PML: int           # sponge width (cells)
+    nt: int
+    dx: float
+    dz: float
+    dt: float
+    vp: np.ndarray     # padded (Nx, Nz) float32
+    den: np.ndarray    # padded (Nx, Nz) float32
+    src_x: List[int]   # padded source cells, one per shot
+    src_z: List[int]
+    rec_z: int         # padded depth of the horizontal receiver line (every interior x)
+    f0: float
+    radius: int = 8
+    nt_per_shot: Optional[List[int]] = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def Nx(self) -> int:
+        return self.NX + 2 * self.PML
+
+    @property
+    def Nz(self) -> int:
+        return self.NZ + 2 * self.PML
+
+    @property
+    def nshot(self) -> int:
+        return len(self.src_x)
+
+    def receivers(self):
+        rx = np.arange(self.PML, self.Nx - self.PML, dtype=np.int32)
+        return rx, np.full_like(rx, self.rec_z)
+
+
+def config1() -> AcousticCase:
+    """Plain 2-D constant-density acoustic, single shot: 251 x 251, dx = dz = 10 m,
+    dt = 1 ms, nt = 1000, two-layer vp (2000 m/s above interior z = 125, 3000 below),
+    50-cell sponge, 25 Hz Ricker (tools/ricker.cpp:44 formula) at interior (z=2, x=125),
+    receivers at every interior x on z = 2. 16th order (the reference's)."""
+    NX = NZ = 251
+    PML = 50
+    z = np.arange(NZ)
+    col = np.where(z < 125, 2000.0, 3000.0).astype(np.float32)
+    vp = pad_edges(np.tile(col, (NX, 1)), PML, PML)
+    den = np.full_like(vp, 2400.0)
+    return AcousticCase("config1_plain_251x251", NX, NZ, PML, 1000, 10.0, 10.0, 1e-3, vp, den,
+                        [PML + 125], [PML + 2], PML + 2, 25.0)
+
+
+def layered_model(NX, NZ, nlayer, vmin, vmax, seed, lateral=0.05, anomalies=4, radius=40.0,
+                  amp=400.0, dx=5.0):
+    """Layered vp increasing with depth, a smooth +-`lateral` relative lateral field and
+    Gaussian anomalies of +-`amp` m/s. Interior (NX, NZ) float32."""
+    rng = np.random.default_rng(seed)
+    bounds = np.sort(rng.uniform(0.05, 0.95, nlayer - 1)) * NZ
+    vel = np.linspace(vmin, vmax, nlayer)
+    z = np.arange(NZ)
+    col = vel[np.searchsorted(bounds, z, side="right")]
+    v = np.tile(col, (NX, 1)).astype(np.float64)
+    x = np.arange(NX)
+    # smooth lateral perturbation: a few low-wavenumber cosines in x and z
+    lat = np.zeros((NX, NZ))
+    for _ in range(4):
+        kx, kz = rng.uniform(0.5, 3.0, 2) * 2 * np.pi
+        px, pz = rng.uniform(0, 2 * np.pi, 2)
+        lat += np.cos(kx * x[:, None] / NX + px) * np.cos(kz * z[None, :] / NZ + pz)
+    lat /= np.abs(lat).max() + 1e-12
+    v *= 1.0 + lateral * lat
+    for _ in range(anomalies):
+        cx, cz = rng.uniform(0.15, 0.85) * NX, rng.uniform(0.2, 0.85) * NZ
+        sgn = rng.choice([-1.0, 1.0])
+        v += sgn * amp * np.exp(-((x[:, None] - cx) ** 2 + (z[None, :] - cz) ** 2) / (2 * radius ** 2))
+    return v.astype(np.float32)
+
+
+def config2(nshot: int = 64, nt: int = 4000) -> AcousticCase:
+    """Batched 2-D acoustic forward: 512 (z) x 2048 (x), dx = dz = 5 m, dt = 0.5 ms, nt = 4000,
+    12 layers 1500-4500 m/s with +-5% lateral variation and 4 Gaussian anomalies (radius 40
+    cells, +-400 m/s), 64 shots evenly spaced on interior z = 2, 30 Hz Ricker, 2048 receivers
+    per shot (every interior x on z = 2), 50-cell sponge. Velocities are clipped at 4700 m/s
+    so the 16th-order CFL number stays below 0.5 (limit 0.516)."""
+    NX, NZ, PML = 2048, 512, 50
+    v = np.clip(layered_model(NX, NZ, 12, 1500.0, 4500.0, seed=20261203), 1400.0, 4700.0)
+    vp = pad_edges(v, PML, PML)
+    den = np.full_like(vp, 2400.0)
+    sx = [PML + int(round((i + 0.5) * NX / nshot)) for i in range(nshot)]
+    return AcousticCase("config2_batched_512x2048", NX, NZ, PML, nt, 5.0, 5.0, 5e-4, vp, den,
+                        sx, [PML + 2] * nshot, PML + 2, 30.0)
+
+
+def small_varden(seed: int = 7) -> AcousticCase:
+    """Non-square, variable-density case used to pin the restatement against the reference
+    build: 80 (x) x 60 (z) interior, 15-cell sponge, 300 steps, off-centre source."""
+    NX, NZ, PML = 80, 60, 15
+    rng = np.random.default_rng(seed)
+    v = layered_model(NX, NZ, 4, 1800.0, 3200.0, seed=seed, anomalies=2, radius=8.0, amp=200.0)
+    d = (2000.0 + 400.0 * rng.random((NX, NZ))).astype(np.float32)
+    return AcousticCase("small_varden_80x60", NX, NZ, PML, 300, 10.0, 10.0, 1e-3,
+                        pad_edges(v, PML, PML), pad_edges(d, PML, PML), [PML + 30], [PML + 20],
+                        PML + 3, 20.0)
