@@ -1,0 +1,343 @@
+"""Benchmark of the batched 2-D acoustic forward (config 2 of the benchmark set).
+
+One bench step = one batched forward of all shots of the workload (every shot's full time
+loop) with model, wavelets and receiver tables already resident in HBM.  `value` is grid-point
+updates per second (padded points x steps x shots) over all ranks, timed with CUDA events on
+the library's stream; `e2e` is the same metric through the C ABI with host buffers (model
+upload and record download inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--exact]
+
+Under torchrun each rank runs its own full workload on its GPU (shots are independent; no
+collective on the data path): weak scaling.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gpts/s & % HBM roofline; gradient shots/s batched vs plain @ relL2≤1e-4"
+BYTES_PER_POINT = {False: 28, True: 32}  # algorithmic bytes per grid-point update (const / variable density)
+FALLBACK_HBM_GBS = 6650.0
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "acoustic2d_step_config2.md")
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def read_profile_traffic():
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if present
+    (line `dram_bytes_per_launch: <int>`)."""
+    try:
+        with open(PROFILE_SUMMARY) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU baselines (the reference's own AFD build; the oracle port only if that build is absent)
+# ----------------------------------------------------------------------------------------------
+
+def cpu_reference_sample(case, steps_per_proc: int):
+    """One process per host core, each running one shot of `case` (full grid) for
+    `steps_per_proc` steps with the reference's own time loop (oracle/_ref/afd_ref), shots
+    distributed like forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90:124."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    procs = os.cpu_count() or 1
+    pts = case.Nx * case.Nz * steps_per_proc
+    if ref_runner.available():
+        from seismic_code_github_b200 import seisfd as S
+        w = S.wavelet(S.WAVELET_RIC, steps_per_proc, case.dt, case.f0, 150)
+        cfgs = [ref_runner.AfdRefConfig(NX=case.NX, NZ=case.NZ, PML=case.PML, Nt=steps_per_proc, dx=case.dx,
+                                        dz=case.dz, dt=case.dt, vp=case.vp, den=case.den, wavelet=w,
+                                        sx=case.src_x[i % case.nshot], sz=case.src_z[i % case.nshot],
+                                        rec_z=case.rec_z, snap=-1, pall=False) for i in range(procs)]
+        r = ref_runner.run_many(cfgs, procs=procs)
+        return {"value": procs * pts / r["wall_s"] / 1e9, "unit": "Gpts/s", "cores": procs, "kind": "reference",
+                "sample": f"{procs} concurrent single-shot runs of the reference AFD build (g++ -O3, "
+                          f"oracle/_ref/afd_ref) on the {case.Nx}x{case.Nz} padded grid, {steps_per_proc} steps each",
+                "wall_s": r["wall_s"]}
+    import oracle_lib as ol
+    from seismic_code_github_b200 import seisfd as S
+    w = S.wavelet(S.WAVELET_RIC, steps_per_proc, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    t0 = time.perf_counter()
+    ol.afd_forward(case.Nx, case.Nz, case.PML, steps_per_proc, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                   case.src_x[0], case.src_z[0], rx, rz)
+    wall = time.perf_counter() - t0
+    return {"value": pts / wall / 1e9, "unit": "Gpts/s", "cores": procs, "kind": "port",
+            "sample": f"one shot of the oracle restatement (OpenMP, {procs} threads), {steps_per_proc} steps",
+            "wall_s": wall}
+
+
+# ----------------------------------------------------------------------------------------------
+
+def make_case(args):
+    from seismic_code_github_b200 import workloads as W
+    return W.config2(nshot=args.nshot, nt=args.nt)
+
+
+def build_shots(case):
+    from seismic_code_github_b200 import seisfd as S
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    return [S.ShotSpec(sx, sz, rx, rz, w) for sx, sz in zip(case.src_x, case.src_z)]
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    case = make_case(args)
+    steps_per_proc = args.ref_steps
+    for _ in range(args.warmup):
+        cpu_reference_sample(case, max(5, steps_per_proc // 4))
+    vals, walls = [], []
+    for _ in range(args.steps):
+        r = cpu_reference_sample(case, steps_per_proc)
+        vals.append(r["value"])
+        walls.append(r["wall_s"])
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gpts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(walls)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered model, config-2 geometry)",
+            "config": config_dict(case, args),
+            "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(case, args):
+    return {"workload": f"batched 2-D acoustic forward, {case.NZ}x{case.NX} interior "
+                        f"({case.Nz}x{case.Nx} padded, {case.PML}-cell sponge), {case.nshot} shots, nt={case.nt}, "
+                        f"16th-order staggered v-p, {len(case.receivers()[0])} receivers/shot",
+            "nshot": case.nshot, "nt": case.nt, "grid_padded": [case.Nx, case.Nz], "order": 16,
+            "mode": "exact" if args.exact else "fma",
+            "l2_policy": "inputs larger than L2 (wavefield state ~2.3 GB per rank)",
+            "parallelism": f"shots x {max(1, int(os.environ.get('WORLD_SIZE', '1')))} GPUs (independent)"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from seismic_code_github_b200 import seisfd as S
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if torch.cuda.is_available() else 0
+    torch.cuda.set_device(dev)
+    case = make_case(args)
+    shots = build_shots(case)
+    flags = S.EXACT if args.exact else 0
+    eng = S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16, flags=flags,
+                   device=dev)
+    eng.set_model(case.vp, case.den)
+    eng.set_shots(shots)
+    varden = not np.all(case.den == case.den.flat[0])
+
+    for _ in range(args.warmup):
+        eng.forward_device(0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(dev)
+    barrier()
+    sampler.start()
+    dev_ms, loop_ms, launches, pts = 0.0, 0.0, 0, 0.0
+    for _ in range(args.steps):
+        eng.forward_device(0)
+        t = eng.timing()
+        dev_ms += t["device_ms"]
+        loop_ms += t["loop_ms"]
+        launches += t["launches"]
+        pts += t["point_updates"]
+    barrier()
+    clocks = sampler.stop()
+
+    # e2e: model upload from pinned host memory + forward + record download to pinned memory
+    nrec_total = eng.record_size()
+    pinned_rec = torch.empty(nrec_total, dtype=torch.float32, pin_memory=True).numpy()
+    pinned_vp = torch.empty(case.vp.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pinned_vp[...] = case.vp
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.set_model(pinned_vp, case.den)
+        eng.forward(pinned_rec)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    h2d = case.vp.nbytes + (0 if not varden else case.den.nbytes)
+    d2h = pinned_rec.nbytes
+
+    tot = torch.tensor([dev_ms, pts, loop_ms, e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist is not None:
+        mx = tot.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tot.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        dev_ms_max, pts_all, loop_max, e2e_max = mx[0].item(), sm[1].item(), mx[2].item(), mx[3].item()
+    else:
+        dev_ms_max, pts_all, loop_max, e2e_max = dev_ms, pts, loop_ms, e2e_s
+
+    # plain per-shot path (one launch per step per shot, no graph) on a subset of shots
+    plain = None
+    if rank == 0 and args.plain_shots > 0:
+        sub = shots[: args.plain_shots]
+        eng.set_shots(sub)
+        eng.forward_per_shot()
+        tp = eng.timing()
+        eng.set_shots(sub)
+        eng.forward_device(0)
+        tb = eng.timing()
+        plain = {"shots": len(sub), "plain_ms": tp["device_ms"], "plain_launches": tp["launches"],
+                 "batched_ms_same_shots": tb["device_ms"],
+                 "plain_shots_per_s": len(sub) / (tp["device_ms"] / 1e3),
+                 "batched_full_shots_per_s": world * case.nshot * args.steps / (dev_ms_max / 1e3)}
+
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    value = pts_all / (dev_ms_max / 1e3) / 1e9
+    e2e_val = world * e2e_steps * (pts / args.steps) / e2e_max / 1e9
+    peak, peak_kind = read_peaks()
+    bpp = BYTES_PER_POINT[bool(varden)]
+    achieved = bpp * pts / (loop_ms / 1e3) / 1e9  # GB/s on rank 0's kernel time
+    traffic = read_profile_traffic()
+    launches_per_call = launches / args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered model with Gaussian anomalies, config-2 geometry)",
+        "config": config_dict(case, args),
+        "shots_per_s": world * case.nshot * args.steps / (dev_ms_max / 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s", "frac_of_nominal_8tbs": achieved / 8000.0,
+                     "bytes_per_point": bpp, "traffic": traffic,
+                     "traffic_source": os.path.relpath(PROFILE_SUMMARY, ROOT) if traffic else None},
+        "e2e": {"value": e2e_val, "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "launches_per_step": launches_per_call,
+        "clocks": clocks,
+    }
+    if plain is not None:
+        line["plain_vs_batched"] = plain
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_reference_sample(case, args.ref_steps).items() if k != "wall_s"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--exact", action="store_true", help="reference operation order (SFD_EXACT)")
+    ap.add_argument("--nshot", type=int, default=64)
+    ap.add_argument("--nt", type=int, default=4000)
+    ap.add_argument("--plain-shots", type=int, default=4)
+    ap.add_argument("--ref-steps", type=int, default=100, help="time steps per process in a CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

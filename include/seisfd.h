@@ -1,0 +1,173 @@
+/*
+ * seisfd.h -- C ABI of the B200 finite-difference wave-propagation engine.
+ *
+ * The reference (stone0312/Seismic_code_github) has no in-process API: its hot path is two
+ * standalone programs that talk through files.  Each entry point below replaces one step of
+ * those programs; the reference location it replaces is cited beside it.
+ *
+ *   forward/Acoustic_FD_by_ss/src/Acoustic_1order_FD.cpp                    (AFD)
+ *   forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90               (QM)
+ *   forward/Q_forward/Q_multishot_fd_subroutine_fsbc_zy_rotated.f90         (QS)
+ *   tools/ricker.cpp                                                        (RIC)
+ *
+ * Conventions (the reference's in-memory and file layouts):
+ *   - grids are x-major with z fastest: a[x * nz + z] (AFD:51-100 `P[i][j]`, i = x, j = z;
+ *     QS:257 `vp(nz,nx)` column-major).  3-D grids are a[(x * ny + y) * nz + z].
+ *   - all sizes are cells of the PADDED grid (interior + sponge), as AFD's Nx = NX + 2*PML.
+ *   - records are trace-major, time fastest: rec[(shot_offset + r) * nt_shot + t]
+ *     (AFD:385-393 `record.dat`; QM:456 `record1(nt, nxe)`).
+ *   - float32 everywhere on the interface.
+ * Errors: every call returns an int status (SFD_OK = 0).  Nothing calls exit/abort/trap; a
+ * bounded device wait that runs out returns SFD_ERR_TIMEOUT; the last message is available
+ * from sfd_last_error.  Threading: one context per host thread, one CUDA stream per context.
+ */
+#ifndef SEISFD_H
+#define SEISFD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFD_ABI_VERSION 1
+
+/* ---- status codes (the reference stops the process instead: QS:463, QS:897, QS:960) ---- */
+#define SFD_OK 0
+#define SFD_ERR_ARG 1          /* invalid argument or configuration                        */
+#define SFD_ERR_IO 2           /* file open/read/write failure                             */
+#define SFD_ERR_CUDA 3         /* CUDA runtime error (message in sfd_last_error)           */
+#define SFD_ERR_TIMEOUT 4      /* a bounded device-side wait gave up                       */
+#define SFD_ERR_NAN 5          /* non-finite value detected in the receiver traces         */
+#define SFD_ERR_NOMEM 6        /* device or host allocation failed                         */
+#define SFD_ERR_UNSUPPORTED 7  /* valid request this build does not implement              */
+#define SFD_ERR_STATE 8        /* call order (e.g. forward before set_model)               */
+
+/* ---- schemes ---- */
+#define SFD_ACOUSTIC_2D 0  /* velocity-pressure staggered grid, sponge: AFD:237-380          */
+#define SFD_VISCOAC_2D 1   /* rotated staggered grid, 1 SLS memory variable, vs = 0:
+                              QS:695-839 in its acoustic reduction                          */
+#define SFD_ACOUSTIC_3D 2  /* 3-D velocity-pressure staggered grid (no reference counterpart) */
+
+/* ---- flags (sfd_grid.flags) ---- */
+#define SFD_EXACT 0x1      /* reference operation order: every multiply and add rounded
+                              separately, double-precision scale factors (AFD:259,276,293) */
+#define SFD_NAN_CHECK 0x2  /* scan receiver traces for NaN/Inf after each forward           */
+
+/* ---- wavelet conventions (sfd_wavelet) ---- */
+#define SFD_WAVELET_AFD 0  /* AFD:199-209: 50(1-2pi^2f^2(t-1/f)^2)exp(-pi^2f^2(t-1/f)^2)    */
+#define SFD_WAVELET_RIC 1  /* RIC:44: (1-2a^2)exp(-a^2), a = pi f0 (j-delay) dt, f0 integer  */
+#define SFD_WAVELET_Q 2    /* QS:1376 (single precision): exp(-b^2)(1-2b^2),
+                              b = pi f0 (it dt - 1.2/f0), it = j+1                           */
+
+/* ---- wavefield selectors (sfd_get_wavefield) ---- */
+#define SFD_FIELD_P 0      /* pressure (AFD P1) / stress sigma (QS strxx)                   */
+#define SFD_FIELD_VX 1
+#define SFD_FIELD_VZ 2
+#define SFD_FIELD_VY 3
+#define SFD_FIELD_R 4      /* memory variable r (QS rxx)                                     */
+
+typedef struct sfd_ctx sfd_ctx;
+
+/* Grid and scheme.  Replaces the hard-coded block AFD:28-45 and the .par cards QS:162-231. */
+typedef struct {
+    int scheme;            /* SFD_ACOUSTIC_2D, SFD_VISCOAC_2D or SFD_ACOUSTIC_3D          */
+    int nx, ny, nz;        /* padded grid; ny = 1 for 2-D                                   */
+    int pml;               /* sponge width in cells (AFD:30 PML; QS: npxn = npxp = npzn = npzp) */
+    float dx, dy, dz, dt;  /* metres, seconds                                              */
+    int order;             /* spatial order 2R: 16 (AFD), 10 (QS), 8, 4 or 2               */
+    int flags;             /* SFD_EXACT | SFD_NAN_CHECK                                     */
+    float f0;              /* SLS reference frequency (QS:509 fup = 2.5 f0 2 pi); 0 = unused */
+} sfd_grid;
+
+/* One shot.  Replaces AFD:199-216 and AFD:376-377 (one source, one receiver line) and
+ * QM:124-129 (per-shot source position, aperture window and record length). */
+typedef struct {
+    int sx, sy, sz;        /* source cell (shot-local padded coordinates)                  */
+    int nt;                /* time steps of this shot (record length), >= 1               */
+    int nrec;              /* receivers                                                     */
+    const int* rec_x;      /* nrec cells, shot-local padded coordinates                     */
+    const int* rec_y;      /* NULL for 2-D                                                   */
+    const int* rec_z;
+    const float* wavelet;  /* nt samples (host); injected as AFD:247-251 / QS:1376-1387       */
+    int ap_x0;             /* aperture window: shot column i reads model column ap_x0 + i   */
+    int ap_nx;             /* window width in cells; 0 = the whole model width              */
+} sfd_shot;
+
+/* Device timing of the last sfd_forward / sfd_gradient call (CUDA events on the context's
+ * stream around the time loop) and the number of kernel launches it issued. */
+typedef struct {
+    double loop_ms;        /* device time of the time loop (all shots)                      */
+    double device_ms;      /* device time of the whole call: state reset, loop, record transpose */
+    double total_ms;       /* host wall time of the whole call incl. copies                  */
+    double point_updates;  /* grid-point updates performed (padded points x steps x shots)   */
+    long long launches;    /* kernels launched by the call                                   */
+    long long h2d_bytes;
+    long long d2h_bytes;
+    int graph;             /* 1 if the time loop ran as a CUDA graph                          */
+    int kernel_variant;    /* implementation detail: which step kernel ran                    */
+} sfd_timing;
+
+int sfd_abi_version(void);
+const char* sfd_status_string(int status);
+
+/* Context lifetime.  Replaces the allocation blocks AFD:51-132 and QM:283-409. */
+int sfd_create(const sfd_grid* grid, int device, sfd_ctx** out);
+int sfd_destroy(sfd_ctx* ctx);
+int sfd_last_error(const sfd_ctx* ctx, char* buf, size_t len);
+
+/* Model, padded grid (x-major, z fastest), host pointers, copied to the device.
+ * Replaces AFD:137-142 (Vp, DEN) and QS:238-284 + QS:434-551 (read_data, substagger, pcalpas).
+ * den may be NULL (constant 2400 kg/m^3, AFD:141); q (SFD_VISCOAC_2D only) may be NULL (no
+ * attenuation: Q = 1e5, the QM:418-419 override). */
+int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* q);
+
+/* Shots.  Replaces the shot loop QM:124-141 (one launch for all shots instead of one process
+ * per shot).  Wavelets and receiver lists are copied; the caller keeps ownership. */
+int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots);
+
+/* Forward modelling of all shots in one batched time loop.  Replaces the time loop AFD:237-380
+ * and QM:439-484.  records: host buffer of sum_s nrec_s * nt_s floats (trace-major per shot,
+ * shots concatenated in order) or NULL. */
+int sfd_forward(sfd_ctx* ctx, float* records);
+
+/* Same, with the records left in device memory (caller-owned, same layout) and no host copy. */
+int sfd_forward_device(sfd_ctx* ctx, float* records_dev);
+
+/* Plain per-shot path: shots one after another, one kernel launch per time step each, no
+ * graph -- the unbatched baseline the batched loop is measured against. */
+int sfd_forward_per_shot(sfd_ctx* ctx, float* records);
+
+/* Final wavefield of one shot after the last forward step (after the sponge, as AFD stores
+ * it at AFD:329-340), padded grid.  Replaces the snapshot writes AFD:343-355, QM:462-481. */
+int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out);
+
+/* Full-waveform gradient: forward with checkpoints, adjoint of the discrete time loop,
+ * zero-lag cross-correlation imaging.  obs: observed records in the sfd_forward layout.
+ * misfit = 0.5 * sum (pred - obs)^2.  grad_vp: d misfit / d vp on the padded grid.
+ * grad_invq: d misfit / d (1/Q) (SFD_VISCOAC_2D only; may be NULL).  No reference
+ * counterpart (the reference has no adjoint). */
+int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);
+
+/* Checkpoint interval of sfd_gradient in steps (0 = ceil(sqrt(nt))). */
+int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps);
+
+int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);
+
+/* Host helpers (no context). */
+/* Source wavelet in one of the reference's three conventions (AFD:199-209, RIC:44, QS:1376).
+ * delay: RIC only, in samples (RIC uses 150). */
+int sfd_wavelet(int convention, int nt, float dt, float f0, int delay, float* out);
+/* AFD sponge factors absorb[x][z] (AFD:164-194; bottom loop bound j < Nz, see AFD:190). */
+int sfd_afd_sponge(int nx, int nz, int pml, float* absorb);
+/* Staggered first-derivative coefficients for order 2R (AFD:38-45 for 16, QS:9-28 otherwise). */
+int sfd_fd_coeffs(int order, float* coeffs);
+/* Edge-replicated padding of an interior model (QS:340-372): in (nx_in, nz_in) ->
+ * out (nx_in + pxn + pxp, nz_in + pzn + pzp). */
+int sfd_pad_model(const float* in, int nx_in, int nz_in, int pxn, int pxp, int pzn, int pzp, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEISFD_H */

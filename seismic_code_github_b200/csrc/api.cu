@@ -1,0 +1,631 @@
+// C ABI implementation: context, model and shot upload, the batched time loop (one CUDA graph
+// per shot set), the per-shot baseline path and read-back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "sfd_internal.h"
+
+using namespace sfd;
+
+namespace sfd {
+struct Engine2DState;  // scheme-specific device state (defined below)
+}
+
+struct sfd_ctx {
+    sfd_grid g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs = nullptr, eve = nullptr;  // loop / whole call
+    std::string err;
+    int radius = 0;
+    float coef[kMaxRadius] = {};
+
+    // model (host copies are kept for the source scale factors and the gradient)
+    bool have_model = false;
+    std::vector<float> h_vp, h_den;
+    bool varden = false;
+    float den_c = 2400.0f;
+    float* d_vp = nullptr;
+    float* d_den = nullptr;
+    float* d_q = nullptr;
+    int mpitch = 0;
+
+    // shots
+    bool have_shots = false;
+    int nshot = 0;
+    int nt_max = 0;
+    std::vector<ShotDev> h_shots;
+    std::vector<int> h_rec_x, h_rec_z;
+    std::vector<float> h_wav;
+    std::vector<long long> rec_out_off;  // trace-major output offset per shot
+    long long rec_total = 0;
+    std::vector<int> order;              // shots sorted by nt, longest first
+    std::vector<int> active_at;          // not stored per step; computed on the fly
+
+    // device buffers for the acoustic 2-D scheme
+    Acou2DPlan plan{};
+    Layout2D L{};
+    ShotDev* d_shots = nullptr;
+    int* d_slot = nullptr;     // sorted order
+    int* d_ident = nullptr;    // identity (per-shot path)
+    float* d_wav = nullptr;
+    int* d_rec_x = nullptr;
+    int* d_rec_z = nullptr;
+    int* d_trp = nullptr;      // per-tile receiver CSR pointers
+    int* d_tri = nullptr;      // per-tile receiver indices
+    float* d_rec_tn = nullptr; // [nt][nrec] per shot
+    float* d_rec_nt = nullptr; // [nrec][nt] per shot (output layout)
+    float* d_state = nullptr;  // 6 fields: p0 p1 vx0 vx1 vz0 vz1, each nshot * shot_stride
+    size_t state_floats = 0;
+    int* d_flag = nullptr;
+
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+
+    int ckpt_interval = 0;
+    sfd_timing timing{};
+
+    ~sfd_ctx();
+};
+
+namespace {
+
+int set_err(sfd_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? SFD_ERR_NOMEM : SFD_ERR_CUDA, \
+                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+void free_shot_buffers(sfd_ctx* c) {
+    dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
+    dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri);
+    dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_valid = false;
+}
+
+}  // namespace
+
+sfd_ctx::~sfd_ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    free_shot_buffers(this);
+    dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (evs) cudaEventDestroy(evs);
+    if (eve) cudaEventDestroy(eve);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+namespace {
+
+// Fill the kernel argument block for step `step`; buffers alternate each step.
+Acou2DArgs make_args(const sfd_ctx* c, int step) {
+    Acou2DArgs a{};
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    float* P[2] = {c->d_state, c->d_state + fs};
+    float* VX[2] = {c->d_state + 2 * fs, c->d_state + 3 * fs};
+    float* VZ[2] = {c->d_state + 4 * fs, c->d_state + 5 * fs};
+    const int i = step & 1, o = (step + 1) & 1;
+    a.p_in = P[i]; a.p_out = P[o];
+    a.vx_in = VX[i]; a.vx_out = VX[o];
+    a.vz_in = VZ[i]; a.vz_out = VZ[o];
+    a.L = c->L;
+    a.nz = c->g.nz;
+    a.pml = c->g.pml;
+    a.vp = c->d_vp;
+    a.den = c->varden ? c->d_den : nullptr;
+    a.mpitch = c->mpitch;
+    a.nx_model = c->g.nx;
+    a.den_c = c->den_c;
+    a.dt = c->g.dt;
+    a.dtdx = c->g.dt / c->g.dx;
+    a.dtdz = c->g.dt / c->g.dz;
+    a.rdx_d = 1.0 / (double)c->g.dx;
+    a.rdz_d = 1.0 / (double)c->g.dz;
+    a.bx_d = (1.0 / (double)c->den_c) * (double)a.dtdx;
+    a.bz_d = (1.0 / (double)c->den_c) * (double)a.dtdz;
+    a.bx_f = (float)a.bx_d;
+    a.bz_f = (float)a.bz_d;
+    a.rdx_f = 1.0f / c->g.dx;
+    a.rdz_f = 1.0f / c->g.dz;
+    for (int m = 0; m < c->radius; m++) a.coef[m] = c->coef[m];
+    for (int q = 0; q < c->g.pml && q < 256; q++)
+        a.sponge[q] = -0.38 * q * q / (1.0 * c->g.pml * c->g.pml) + 1;
+    a.shots = c->d_shots;
+    a.slot_to_shot = c->d_slot;
+    a.wavelets = c->d_wav;
+    a.rec_x = c->d_rec_x;
+    a.rec_z = c->d_rec_z;
+    a.tile_rec_ptr = c->d_trp;
+    a.tile_rec_idx = c->d_tri;
+    a.records = c->d_rec_tn;
+    a.step = step;
+    return a;
+}
+
+int active_shots(const sfd_ctx* c, int step) {
+    int n = 0;
+    for (int s : c->order)
+        if (c->h_shots[s].nt > step) n++;
+    return n;
+}
+
+// Zero the wavefields and the record buffer, inject the step-0 source sample.
+int prologue(sfd_ctx* ctx) {
+    CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_rec_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
+    Acou2DArgs a = make_args(ctx, -1);  // step -1 writes into buffer 0
+    CK(acoustic2d_launch_inject0(a, ctx->nshot, (ctx->g.flags & SFD_EXACT) != 0, ctx->stream));
+    return SFD_OK;
+}
+
+int enqueue_loop(sfd_ctx* ctx, long long* launches) {
+    const bool exact = (ctx->g.flags & SFD_EXACT) != 0;
+    for (int k = 0; k < ctx->nt_max; k++) {
+        const int act = active_shots(ctx, k);
+        if (act == 0) break;
+        Acou2DArgs a = make_args(ctx, k);
+        CK(acoustic2d_launch_step(ctx->plan, a, act, exact, ctx->varden, ctx->stream));
+        (*launches)++;
+    }
+    return SFD_OK;
+}
+
+int epilogue(sfd_ctx* ctx, float* out_dev) {
+    int nrec_max = 0;
+    for (const auto& s : ctx->h_shots) nrec_max = std::max(nrec_max, s.nrec);
+    CK(launch_records_transpose(ctx->d_rec_tn, out_dev, ctx->d_shots, ctx->nshot, nrec_max, ctx->nt_max,
+                                ctx->stream));
+    if (ctx->g.flags & SFD_NAN_CHECK) {
+        CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+        CK(launch_nan_scan(out_dev, ctx->rec_total, ctx->d_flag, ctx->stream));
+    }
+    return SFD_OK;
+}
+
+int check_ready(sfd_ctx* ctx) {
+    if (!ctx) return SFD_ERR_ARG;
+    if (!ctx->have_model) return set_err(ctx, SFD_ERR_STATE, "sfd_set_model has not been called");
+    if (!ctx->have_shots) return set_err(ctx, SFD_ERR_STATE, "sfd_set_shots has not been called");
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d forward is not implemented", ctx->g.scheme);
+    CK(cudaSetDevice(ctx->device));
+    return SFD_OK;
+}
+
+int finish_nan(sfd_ctx* ctx) {
+    if (ctx->g.flags & SFD_NAN_CHECK) {
+        int flag = 0;
+        CK(cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) return set_err(ctx, SFD_ERR_NAN, "non-finite value in the receiver traces");
+    }
+    return SFD_OK;
+}
+
+int run_forward(sfd_ctx* ctx, float* out_dev) {
+    int rc;
+    long long launches = 0;
+    if (!ctx->graph_valid) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_loop(ctx, &launches);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc != SFD_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        CK(e);
+        if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+        e = cudaGraphInstantiate(&ctx->graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        ctx->graph_valid = true;
+    } else {
+        for (int k = 0; k < ctx->nt_max && active_shots(ctx, k) > 0; k++) launches++;
+    }
+    CK(cudaEventRecord(ctx->evs, ctx->stream));
+    if ((rc = prologue(ctx)) != SFD_OK) return rc;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((rc = epilogue(ctx, out_dev)) != SFD_OK) return rc;
+    CK(cudaEventRecord(ctx->eve, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.0f, dms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    CK(cudaEventElapsedTime(&dms, ctx->evs, ctx->eve));
+    ctx->timing.loop_ms = ms;
+    ctx->timing.device_ms = dms;
+    ctx->timing.launches = launches + 2 + ((ctx->g.flags & SFD_NAN_CHECK) ? 1 : 0);
+    ctx->timing.graph = 1;
+    ctx->timing.kernel_variant = 1;
+    double pts = 0;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
+    ctx->timing.point_updates = pts;
+    return finish_nan(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfd_abi_version(void) { return SFD_ABI_VERSION; }
+
+const char* sfd_status_string(int s) {
+    switch (s) {
+    case SFD_OK: return "ok";
+    case SFD_ERR_ARG: return "invalid argument";
+    case SFD_ERR_IO: return "i/o error";
+    case SFD_ERR_CUDA: return "cuda error";
+    case SFD_ERR_TIMEOUT: return "device wait timed out";
+    case SFD_ERR_NAN: return "non-finite values detected";
+    case SFD_ERR_NOMEM: return "out of memory";
+    case SFD_ERR_UNSUPPORTED: return "unsupported";
+    case SFD_ERR_STATE: return "invalid call order";
+    default: return "unknown status";
+    }
+}
+
+int sfd_last_error(const sfd_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || len == 0) return SFD_ERR_ARG;
+    std::snprintf(buf, len, "%s", ctx->err.c_str());
+    return SFD_OK;
+}
+
+int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
+    if (!g || !out) return SFD_ERR_ARG;
+    *out = nullptr;
+    if (g->scheme != SFD_ACOUSTIC_2D && g->scheme != SFD_VISCOAC_2D && g->scheme != SFD_ACOUSTIC_3D)
+        return SFD_ERR_ARG;
+    const bool is3d = g->scheme == SFD_ACOUSTIC_3D;
+    if (g->nx <= 0 || g->nz <= 0 || (is3d ? g->ny <= 0 : g->ny > 1)) return SFD_ERR_ARG;
+    if (!(g->dx > 0) || !(g->dz > 0) || !(g->dt > 0) || (is3d && !(g->dy > 0))) return SFD_ERR_ARG;
+    if (g->pml < 0 || g->pml > 256 || 2 * g->pml > g->nx || 2 * g->pml > g->nz) return SFD_ERR_ARG;
+    float cf[8];
+    if (sfd_fd_coeffs(g->order, cf) != SFD_OK) return SFD_ERR_ARG;
+    const int R = g->order / 2;
+    if (g->nx <= 2 * R || g->nz <= 2 * R) return SFD_ERR_ARG;
+    std::unique_ptr<sfd_ctx> c(new sfd_ctx());
+    c->g = *g;
+    if (c->g.ny <= 0) c->g.ny = 1;
+    c->device = device;
+    c->radius = R;
+    std::memcpy(c->coef, cf, sizeof(float) * R);
+    sfd_ctx* ctx = c.get();
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    CK(cudaEventCreate(&c->evs));
+    CK(cudaEventCreate(&c->eve));
+    CK(cudaMalloc(&c->d_flag, sizeof(int)));
+    if (g->scheme == SFD_ACOUSTIC_2D && !acoustic2d_plan(R, &c->plan))
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "no kernel for radius %d", R);
+    *out = c.release();
+    return SFD_OK;
+}
+
+int sfd_destroy(sfd_ctx* ctx) {
+    delete ctx;
+    return SFD_OK;
+}
+
+int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* q) {
+    if (!ctx || !vp) return SFD_ERR_ARG;
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    for (size_t i = 0; i < n; i++)
+        if (!(vp[i] > 0.0f) || !std::isfinite(vp[i]))
+            return set_err(ctx, SFD_ERR_ARG, "vp[%zu] = %g is not a positive finite velocity", i, (double)vp[i]);
+    if (den)
+        for (size_t i = 0; i < n; i++)
+            if (!(den[i] > 0.0f) || !std::isfinite(den[i]))
+                return set_err(ctx, SFD_ERR_ARG, "den[%zu] = %g is not a positive finite density", i, (double)den[i]);
+    CK(cudaSetDevice(ctx->device));
+    ctx->h_vp.assign(vp, vp + n);
+    ctx->varden = false;
+    ctx->den_c = 2400.0f;
+    ctx->h_den.clear();
+    if (den) {
+        ctx->h_den.assign(den, den + n);
+        bool uniform = true;
+        for (size_t i = 1; i < n && uniform; i++) uniform = den[i] == den[0];
+        if (uniform) ctx->den_c = den[0];
+        else ctx->varden = true;
+    }
+    const int cols = ctx->g.nx * ctx->g.ny;
+    ctx->mpitch = round_up(ctx->g.nz, 32);
+    const size_t mbytes = sizeof(float) * (size_t)cols * ctx->mpitch;
+    // Buffers are allocated once per context and refilled in place, so a captured time loop
+    // (which bakes these pointers and the density constant in) stays valid across model updates.
+    const float den_c_old = ctx->have_model ? ctx->den_c : -1.0f;
+    const bool varden_old = ctx->have_model && ctx->d_den != nullptr;
+    if (!ctx->d_vp) CK(cudaMalloc(&ctx->d_vp, mbytes));
+    CK(cudaMemcpy2D(ctx->d_vp, sizeof(float) * ctx->mpitch, vp, sizeof(float) * ctx->g.nz,
+                    sizeof(float) * ctx->g.nz, cols, cudaMemcpyHostToDevice));
+    if (ctx->varden) {
+        if (!ctx->d_den) CK(cudaMalloc(&ctx->d_den, mbytes));
+        CK(cudaMemcpy2D(ctx->d_den, sizeof(float) * ctx->mpitch, den, sizeof(float) * ctx->g.nz,
+                        sizeof(float) * ctx->g.nz, cols, cudaMemcpyHostToDevice));
+    } else {
+        dfree(ctx->d_den);
+    }
+    (void)q;
+    if (ctx->varden != varden_old || (!ctx->varden && ctx->den_c != den_c_old)) ctx->graph_valid = false;
+    ctx->have_model = true;
+    // source scale factors depend on the model
+    if (ctx->have_shots) {
+        for (auto& s : ctx->h_shots) {
+            const size_t mi = (size_t)(s.x0 + s.sx) * ctx->g.nz + s.sz;
+            const float d = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
+            float sc = ctx->g.dt * d;
+            sc = sc * ctx->h_vp[mi];
+            s.inj_scale = sc;
+        }
+        CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
+    }
+    return SFD_OK;
+}
+
+int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
+    if (!ctx || nshot <= 0 || !shots) return SFD_ERR_ARG;
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d is not implemented", ctx->g.scheme);
+    CK(cudaSetDevice(ctx->device));
+    const int nxm = ctx->g.nx, nz = ctx->g.nz;
+    std::vector<ShotDev> hs(nshot);
+    std::vector<int> rx, rz;
+    std::vector<float> wav;
+    std::vector<long long> out_off(nshot);
+    long long rec_total = 0;
+    int nx_max = 0, nt_max = 0;
+    for (int s = 0; s < nshot; s++) {
+        const sfd_shot& sh = shots[s];
+        const int nxs = sh.ap_nx > 0 ? sh.ap_nx : nxm;
+        if (sh.ap_x0 < 0 || sh.ap_x0 + nxs > nxm || nxs <= 2 * ctx->radius || 2 * ctx->g.pml > nxs)
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: aperture [%d, %d) outside the model (nx=%d)", s, sh.ap_x0,
+                           sh.ap_x0 + nxs, nxm);
+        if (sh.nt < 1 || !sh.wavelet)
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: nt=%d or wavelet missing", s, sh.nt);
+        if (sh.sx < 0 || sh.sx >= nxs || sh.sz < 0 || sh.sz >= nz)
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: source (%d, %d) outside the grid", s, sh.sx, sh.sz);
+        if (sh.nrec < 0 || (sh.nrec > 0 && (!sh.rec_x || !sh.rec_z)))
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: receiver list missing", s);
+        ShotDev d{};
+        d.nx = nxs; d.x0 = sh.ap_x0; d.nt = sh.nt; d.sx = sh.sx; d.sy = 0; d.sz = sh.sz;
+        d.nrec = sh.nrec;
+        d.rec_base = rec_total;
+        d.rec_list = (int)rx.size();
+        d.wav_off = (int)wav.size();
+        for (int r = 0; r < sh.nrec; r++) {
+            if (sh.rec_x[r] < 0 || sh.rec_x[r] >= nxs || sh.rec_z[r] < 0 || sh.rec_z[r] >= nz)
+                return set_err(ctx, SFD_ERR_ARG, "shot %d: receiver %d (%d, %d) outside the grid", s, r,
+                               sh.rec_x[r], sh.rec_z[r]);
+            rx.push_back(sh.rec_x[r]);
+            rz.push_back(sh.rec_z[r]);
+        }
+        wav.insert(wav.end(), sh.wavelet, sh.wavelet + sh.nt);
+        out_off[s] = rec_total;
+        rec_total += (long long)sh.nrec * sh.nt;
+        nx_max = std::max(nx_max, nxs);
+        nt_max = std::max(nt_max, sh.nt);
+        hs[s] = d;
+    }
+    free_shot_buffers(ctx);
+    // layout of the state slabs
+    Layout2D L{};
+    L.tx = ctx->plan.tx;
+    L.tz = ctx->plan.tz;
+    L.gx = 2 * ctx->radius;
+    L.gz = (2 * ctx->radius + 3) & ~3;
+    L.ntx = (nx_max + L.tx - 1) / L.tx;
+    L.ntz = (nz + L.tz - 1) / L.tz;
+    L.pitch = round_up(L.gz + L.ntz * L.tz + L.gz, 32);
+    L.cols = L.gx + L.ntx * L.tx + L.gx;
+    L.shot_stride = (long long)L.cols * L.pitch;
+    ctx->L = L;
+    // per-tile receiver CSR
+    const int ntiles = L.ntx * L.ntz;
+    std::vector<int> trp, tri;
+    for (int s = 0; s < nshot; s++) {
+        hs[s].tile_rec_base = (int)trp.size();
+        std::vector<std::vector<int>> bucket(ntiles);
+        for (int r = 0; r < hs[s].nrec; r++) {
+            const int x = rx[hs[s].rec_list + r], z = rz[hs[s].rec_list + r];
+            bucket[(x / L.tx) * L.ntz + z / L.tz].push_back(r);
+        }
+        for (int t = 0; t < ntiles; t++) {
+            trp.push_back((int)tri.size());
+            tri.insert(tri.end(), bucket[t].begin(), bucket[t].end());
+        }
+        trp.push_back((int)tri.size());
+    }
+    // source scale ((dt * DEN) * Vp) in float, AFD:250
+    for (auto& d : hs) {
+        if (ctx->have_model) {
+            const size_t mi = (size_t)(d.x0 + d.sx) * nz + d.sz;
+            const float den = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
+            float sc = ctx->g.dt * den;
+            sc = sc * ctx->h_vp[mi];
+            d.inj_scale = sc;
+        }
+    }
+    std::vector<int> order(nshot);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return hs[a].nt > hs[b].nt; });
+    std::vector<int> ident(nshot);
+    std::iota(ident.begin(), ident.end(), 0);
+
+    ctx->h_shots = hs;
+    ctx->h_rec_x = rx;
+    ctx->h_rec_z = rz;
+    ctx->h_wav = wav;
+    ctx->rec_out_off = out_off;
+    ctx->rec_total = rec_total;
+    ctx->nshot = nshot;
+    ctx->nt_max = nt_max;
+    ctx->order = order;
+
+    auto up = [&](auto** dst, const auto& v) -> int {
+        using E = typename std::remove_reference<decltype(v)>::type::value_type;
+        const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(E);
+        CK(cudaMalloc(dst, bytes));
+        if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice));
+        return SFD_OK;
+    };
+    int rc;
+    if ((rc = up(&ctx->d_shots, hs)) || (rc = up(&ctx->d_slot, order)) || (rc = up(&ctx->d_ident, ident)) ||
+        (rc = up(&ctx->d_wav, wav)) || (rc = up(&ctx->d_rec_x, rx)) || (rc = up(&ctx->d_rec_z, rz)) ||
+        (rc = up(&ctx->d_trp, trp)) || (rc = up(&ctx->d_tri, tri)))
+        return rc;
+    const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
+    CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
+    CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
+    ctx->state_floats = 6 * (size_t)nshot * L.shot_stride;
+    CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
+    ctx->have_shots = true;
+    ctx->graph_valid = false;
+    return SFD_OK;
+}
+
+int sfd_forward_device(sfd_ctx* ctx, float* records_dev) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    rc = run_forward(ctx, records_dev ? records_dev : ctx->d_rec_nt);
+    ctx->timing.h2d_bytes = 0;
+    ctx->timing.d2h_bytes = 0;
+    ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+int sfd_forward(sfd_ctx* ctx, float* records) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    rc = run_forward(ctx, ctx->d_rec_nt);
+    if (rc) return rc;
+    if (records && ctx->rec_total > 0)
+        CK(cudaMemcpy(records, ctx->d_rec_nt, sizeof(float) * ctx->rec_total, cudaMemcpyDeviceToHost));
+    ctx->timing.h2d_bytes = 0;
+    ctx->timing.d2h_bytes = records ? (long long)sizeof(float) * ctx->rec_total : 0;
+    ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SFD_OK;
+}
+
+int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    const bool exact = (ctx->g.flags & SFD_EXACT) != 0;
+    CK(cudaEventRecord(ctx->evs, ctx->stream));
+    if ((rc = prologue(ctx)) != SFD_OK) return rc;
+    long long launches = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int s = 0; s < ctx->nshot; s++) {
+        for (int k = 0; k < ctx->h_shots[s].nt; k++) {
+            Acou2DArgs a = make_args(ctx, k);
+            a.slot_to_shot = ctx->d_ident + s;
+            CK(acoustic2d_launch_step(ctx->plan, a, 1, exact, ctx->varden, ctx->stream));
+            launches++;
+        }
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((rc = epilogue(ctx, ctx->d_rec_nt)) != SFD_OK) return rc;
+    CK(cudaEventRecord(ctx->eve, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0, dms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    CK(cudaEventElapsedTime(&dms, ctx->evs, ctx->eve));
+    ctx->timing.device_ms = dms;
+    if (records && ctx->rec_total > 0)
+        CK(cudaMemcpy(records, ctx->d_rec_nt, sizeof(float) * ctx->rec_total, cudaMemcpyDeviceToHost));
+    ctx->timing.loop_ms = ms;
+    ctx->timing.launches = launches + 2;
+    ctx->timing.graph = 0;
+    ctx->timing.kernel_variant = 1;
+    double pts = 0;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
+    ctx->timing.point_updates = pts;
+    ctx->timing.h2d_bytes = 0;
+    ctx->timing.d2h_bytes = records ? (long long)sizeof(float) * ctx->rec_total : 0;
+    ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return finish_nan(ctx);
+}
+
+int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
+    if (!ctx || !out) return SFD_ERR_ARG;
+    if (!ctx->have_shots || shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
+    if (field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+    CK(cudaSetDevice(ctx->device));
+    const ShotDev& sd = ctx->h_shots[shot];
+    const int buf = sd.nt & 1;  // state after nt steps lives in buffer nt % 2
+    const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+    const int fidx = field == SFD_FIELD_P ? 0 : (field == SFD_FIELD_VX ? 2 : 4);
+    const float* base = ctx->d_state + (fidx + buf) * fs + (long long)shot * ctx->L.shot_stride +
+                        (long long)ctx->L.gx * ctx->L.pitch + ctx->L.gz;
+    const int nz = ctx->g.nz;
+    CK(cudaMemcpy2D(out, sizeof(float) * nz, base, sizeof(float) * ctx->L.pitch, sizeof(float) * nz, sd.nx,
+                    cudaMemcpyDeviceToHost));
+    if (field != SFD_FIELD_P) {
+        // velocities are stored before the sponge multiply; return them as AFD holds them
+        std::vector<float> a((size_t)sd.nx * nz);
+        sfd_afd_sponge(sd.nx, nz, ctx->g.pml, a.data());
+        for (size_t i = 0; i < a.size(); i++) out[i] = out[i] * a[i];
+    }
+    return SFD_OK;
+}
+
+int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps) {
+    if (!ctx || steps < 0) return SFD_ERR_ARG;
+    ctx->ckpt_interval = steps;
+    return SFD_OK;
+}
+
+int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq) {
+    (void)obs; (void)misfit; (void)grad_vp; (void)grad_invq;
+    if (!ctx) return SFD_ERR_ARG;
+    return set_err(ctx, SFD_ERR_UNSUPPORTED, "gradient is not implemented yet");
+}
+
+int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out) {
+    if (!ctx || !out) return SFD_ERR_ARG;
+    *out = ctx->timing;
+    return SFD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// Internal definitions shared by the host library and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/seisfd.h"
+
+namespace sfd {
+
+constexpr int kMaxRadius = 8;
+
+// Per-shot descriptor in device memory (one entry per shot, indexed by shot id).
+struct ShotDev {
+    int nx;            // shot-local padded width (aperture)
+    int x0;            // model column of shot column 0
+    int nt;            // steps
+    int sx, sy, sz;    // source cell
+    int nrec;
+    long long rec_base;   // offset (floats) of this shot's [nt][nrec] block in the record buffer
+    int rec_list;         // offset of this shot's receivers in rec_x/rec_z
+    int wav_off;          // offset of this shot's wavelet
+    int tile_rec_base;    // offset of this shot's per-tile receiver CSR (ntiles + 1 entries)
+    float inj_scale;      // ((dt * den_src) * vp_src), float, AFD:250 order
+};
+
+// Field storage of one 2-D scheme: per shot a (cols x pitch) slab, z fastest, with zero ghost
+// margins of gx columns and gz rows so halo reads never leave the allocation.
+struct Layout2D {
+    int gx, gz;        // ghost margins
+    int pitch;         // floats per column (multiple of 32)
+    int cols;          // columns incl. ghosts
+    long long shot_stride;  // floats per shot
+    int ntx, ntz;      // tiles per shot along x and z
+    int tx, tz;        // tile shape
+};
+
+// Arguments of the acoustic 2-D step kernels (passed by value; pointers are device memory).
+struct Acou2DArgs {
+    const float* p_in;  float* p_out;
+    const float* vx_in; float* vx_out;
+    const float* vz_in; float* vz_out;
+    Layout2D L;
+    int nz;                 // padded grid nz (same for every shot)
+    int pml;
+    const float* vp;        // model, (nx_model x mpitch)
+    const float* den;       // NULL for constant density
+    int mpitch;
+    int nx_model;
+    float den_c;            // constant density
+    float dt;
+    float dtdx, dtdz;       // float(dt/dx), float(dt/dz) (AFD:259, 276)
+    double rdx_d, rdz_d;    // 1.0/dx, 1.0/dz in double (AFD:293, 302)
+    double bx_d, bz_d;      // (1.0/den_c)*(dt/dx) in double, constant density
+    float bx_f, bz_f;       // float versions for the fast path
+    float rdx_f, rdz_f;
+    float coef[kMaxRadius];
+    float sponge[256];      // sponge profile tab[q] = 1 - 0.38 q^2 / pml^2, q < pml (AFD:164-194)
+    const ShotDev* shots;
+    const int* slot_to_shot;   // active-slot -> shot id (shots sorted by nt, longest first)
+    const float* wavelets;
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr;   // per shot: ntiles + 1 offsets into tile_rec_idx
+    const int* tile_rec_idx;   // receiver index within the shot
+    float* records;            // [nt][nrec] per shot at ShotDev::rec_base
+    int step;
+};
+
+// Host-side launchers (acoustic2d.cu).
+struct Acou2DPlan {
+    int radius;
+    int tx, tz, threads;
+    size_t smem_bytes;
+};
+bool acoustic2d_plan(int radius, Acou2DPlan* plan);
+cudaError_t acoustic2d_launch_step(const Acou2DPlan& plan, const Acou2DArgs& a, int active_shots,
+                                   bool exact, bool varden, cudaStream_t st);
+cudaError_t acoustic2d_launch_inject0(const Acou2DArgs& a, int nshot, bool exact, cudaStream_t st);
+cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const ShotDev* shots, int nshot,
+                                     int nrec_max, int nt_max, cudaStream_t st);
+cudaError_t launch_nan_scan(const float* rec, long long n, int* flag, cudaStream_t st);
+
+}  // namespace sfd

@@ -1,0 +1,256 @@
+"""ctypes binding of the C ABI in include/seisfd.h (libseisfd.so, built by build.py).
+
+There is no CPU fallback: if the native library is missing, importing this module raises.
+"""
+import ctypes
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libseisfd.so")
+
+OK, ERR_ARG, ERR_IO, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE = range(9)
+ACOUSTIC_2D, VISCOAC_2D, ACOUSTIC_3D = 0, 1, 2
+EXACT, NAN_CHECK = 0x1, 0x2
+WAVELET_AFD, WAVELET_RIC, WAVELET_Q = 0, 1, 2
+FIELD_P, FIELD_VX, FIELD_VZ, FIELD_VY, FIELD_R = 0, 1, 2, 3, 4
+
+_F32P = ctypes.POINTER(ctypes.c_float)
+_I32P = ctypes.POINTER(ctypes.c_int)
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("pml", ctypes.c_int), ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("order", ctypes.c_int), ("flags", ctypes.c_int), ("f0", ctypes.c_float)]
+
+
+class Shot(ctypes.Structure):
+    _fields_ = [("sx", ctypes.c_int), ("sy", ctypes.c_int), ("sz", ctypes.c_int), ("nt", ctypes.c_int),
+                ("nrec", ctypes.c_int), ("rec_x", _I32P), ("rec_y", _I32P), ("rec_z", _I32P),
+                ("wavelet", _F32P), ("ap_x0", ctypes.c_int), ("ap_nx", ctypes.c_int)]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [("loop_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("point_updates", ctypes.c_double),
+                ("launches", ctypes.c_longlong), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
+                ("graph", ctypes.c_int), ("kernel_variant", ctypes.c_int)]
+
+
+# Every symbol include/seisfd.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "sfd_abi_version": (ctypes.c_int, []),
+    "sfd_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "sfd_create": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "sfd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sfd_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "sfd_set_model": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P]),
+    "sfd_set_shots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Shot)]),
+    "sfd_forward": (ctypes.c_int, [ctypes.c_void_p, _F32P]),
+    "sfd_forward_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "sfd_forward_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P]),
+    "sfd_get_wavefield": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _F32P]),
+    "sfd_gradient": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
+    "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
+    "sfd_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _F32P]),
+    "sfd_afd_sponge": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P]),
+    "sfd_fd_coeffs": (ctypes.c_int, [ctypes.c_int, _F32P]),
+    "sfd_pad_model": (ctypes.c_int, [_F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, _F32P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libseisfd.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m seismic_code_github_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class SfdError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{load().sfd_status_string(status).decode()} ({status}): {msg}")
+        self.status = status
+
+
+def _fp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_F32P)
+
+
+def _ip(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_I32P)
+
+
+def wavelet(convention: int, nt: int, dt: float, f0: float, delay: int = 150) -> np.ndarray:
+    out = np.empty(nt, np.float32)
+    rc = load().sfd_wavelet(convention, nt, dt, f0, delay, _fp(out))
+    if rc:
+        raise SfdError(rc, "sfd_wavelet")
+    return out
+
+
+def afd_sponge(nx: int, nz: int, pml: int) -> np.ndarray:
+    out = np.empty((nx, nz), np.float32)
+    rc = load().sfd_afd_sponge(nx, nz, pml, _fp(out))
+    if rc:
+        raise SfdError(rc, "sfd_afd_sponge")
+    return out
+
+
+def fd_coeffs(order: int) -> np.ndarray:
+    out = np.zeros(8, np.float32)
+    rc = load().sfd_fd_coeffs(order, _fp(out))
+    if rc:
+        raise SfdError(rc, "sfd_fd_coeffs")
+    return out[: order // 2]
+
+
+def pad_model(a: np.ndarray, pxn: int, pxp: int, pzn: int, pzp: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.float32)
+    out = np.empty((a.shape[0] + pxn + pxp, a.shape[1] + pzn + pzp), np.float32)
+    rc = load().sfd_pad_model(_fp(a), a.shape[0], a.shape[1], pxn, pxp, pzn, pzp, _fp(out))
+    if rc:
+        raise SfdError(rc, "sfd_pad_model")
+    return out
+
+
+class ShotSpec:
+    """One shot: source cell, receiver cells, wavelet (nt samples), optional aperture."""
+
+    def __init__(self, sx: int, sz: int, rec_x: Sequence[int], rec_z: Sequence[int], wavelet: np.ndarray,
+                 sy: int = 0, rec_y: Optional[Sequence[int]] = None, ap_x0: int = 0, ap_nx: int = 0):
+        self.sx, self.sy, self.sz = int(sx), int(sy), int(sz)
+        self.rec_x = np.ascontiguousarray(rec_x, np.int32)
+        self.rec_z = np.ascontiguousarray(rec_z, np.int32)
+        self.rec_y = None if rec_y is None else np.ascontiguousarray(rec_y, np.int32)
+        self.wavelet = np.ascontiguousarray(wavelet, np.float32)
+        self.ap_x0, self.ap_nx = int(ap_x0), int(ap_nx)
+
+    @property
+    def nt(self) -> int:
+        return int(self.wavelet.shape[0])
+
+    @property
+    def nrec(self) -> int:
+        return int(self.rec_x.shape[0])
+
+
+class Engine:
+    """Owns one sfd_ctx (one device, one stream)."""
+
+    def __init__(self, scheme: int, nx: int, nz: int, dx: float, dz: float, dt: float, pml: int, order: int = 16,
+                 ny: int = 1, dy: float = 0.0, flags: int = 0, f0: float = 0.0, device: int = 0):
+        self._lib = load()
+        self.grid = Grid(scheme, nx, ny, nz, pml, dx, dy, dz, dt, order, flags, f0)
+        h = ctypes.c_void_p()
+        rc = self._lib.sfd_create(ctypes.byref(self.grid), device, ctypes.byref(h))
+        if rc:
+            raise SfdError(rc, "sfd_create")
+        self._h = h
+        self._shots: List[ShotSpec] = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sfd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def last_error(self) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        self._lib.sfd_last_error(self._h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc: int, what: str):
+        if rc:
+            raise SfdError(rc, f"{what}: {self.last_error()}")
+
+    def set_model(self, vp: np.ndarray, den: Optional[np.ndarray] = None, q: Optional[np.ndarray] = None):
+        vp = np.ascontiguousarray(vp, np.float32)
+        den = None if den is None else np.ascontiguousarray(den, np.float32)
+        q = None if q is None else np.ascontiguousarray(q, np.float32)
+        self._keep_model = (vp, den, q)
+        self._check(self._lib.sfd_set_model(self._h, _fp(vp), _fp(den), _fp(q)), "sfd_set_model")
+
+    def set_shots(self, shots: Sequence[ShotSpec]):
+        arr = (Shot * len(shots))()
+        for i, s in enumerate(shots):
+            arr[i] = Shot(s.sx, s.sy, s.sz, s.nt, s.nrec, _ip(s.rec_x), _ip(s.rec_y), _ip(s.rec_z),
+                          _fp(s.wavelet), s.ap_x0, s.ap_nx)
+        self._shots = list(shots)
+        self._check(self._lib.sfd_set_shots(self._h, len(shots), arr), "sfd_set_shots")
+
+    def record_size(self) -> int:
+        return sum(s.nrec * s.nt for s in self._shots)
+
+    def split_records(self, flat: np.ndarray) -> List[np.ndarray]:
+        out, off = [], 0
+        for s in self._shots:
+            n = s.nrec * s.nt
+            out.append(flat[off:off + n].reshape(s.nrec, s.nt))
+            off += n
+        return out
+
+    def forward(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        rec = out if out is not None else np.empty(self.record_size(), np.float32)
+        self._check(self._lib.sfd_forward(self._h, _fp(rec)), "sfd_forward")
+        return rec
+
+    def forward_per_shot(self) -> np.ndarray:
+        rec = np.empty(self.record_size(), np.float32)
+        self._check(self._lib.sfd_forward_per_shot(self._h, _fp(rec)), "sfd_forward_per_shot")
+        return rec
+
+    def forward_device(self, dev_ptr: int):
+        self._check(self._lib.sfd_forward_device(self._h, ctypes.c_void_p(dev_ptr)), "sfd_forward_device")
+
+    def wavefield(self, shot: int, field: int) -> np.ndarray:
+        s = self._shots[shot]
+        nx = s.ap_nx if s.ap_nx > 0 else self.grid.nx
+        out = np.empty((nx, self.grid.ny, self.grid.nz) if self.grid.ny > 1 else (nx, self.grid.nz), np.float32)
+        self._check(self._lib.sfd_get_wavefield(self._h, shot, field, _fp(out)), "sfd_get_wavefield")
+        return out
+
+    def gradient(self, obs: np.ndarray, want_invq: bool = False):
+        obs = np.ascontiguousarray(obs, np.float32)
+        mis = np.zeros(1, np.float32)
+        n = self.grid.nx * self.grid.ny * self.grid.nz
+        g = np.empty(n, np.float32)
+        gq = np.empty(n, np.float32) if want_invq else None
+        self._check(self._lib.sfd_gradient(self._h, _fp(obs), _fp(mis), _fp(g), _fp(gq)), "sfd_gradient")
+        shape = (self.grid.nx, self.grid.nz) if self.grid.ny == 1 else (self.grid.nx, self.grid.ny, self.grid.nz)
+        return float(mis[0]), g.reshape(shape), (None if gq is None else gq.reshape(shape))
+
+    def set_checkpoint_interval(self, steps: int):
+        self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
+
+    def timing(self) -> dict:
+        t = Timing()
+        self._check(self._lib.sfd_get_timing(self._h, ctypes.byref(t)), "sfd_get_timing")
+        return {k: getattr(t, k) for k, _ in Timing._fields_}

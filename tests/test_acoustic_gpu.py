@@ -1,0 +1,250 @@
+"""GPU parity of the 2-D acoustic path (SFD_ACOUSTIC_2D) through the C ABI.
+
+Bars: with SFD_EXACT the kernel keeps the reference's operation order and must be bit-exact
+against the reference's outputs; the default (FMA) path must stay within relative L2 <= 1e-5
+of the reference gathers (max-abs printed).  Every case also reports the error against the
+FP64 oracle of the same scheme.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from conftest import bits_equal, rel_l2
+from seismic_code_github_b200 import seisfd as S
+from seismic_code_github_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL_FWD = 1e-5  # relative L2, FP32 forward vs the reference gathers
+
+
+def engine_for(case, flags=0, order=16):
+    e = S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=order, flags=flags)
+    e.set_model(case.vp, case.den)
+    return e
+
+
+def afd_default_case():
+    """AFD's own hard-coded configuration (AFD:28-45, 199-216, 376-377)."""
+    NX = NZ = 100
+    PML = 20
+    Nx = Nz = NX + 2 * PML
+    vp = np.full((Nx, Nz), 2000, np.float32)
+    den = np.full((Nx, Nz), 2400, np.float32)
+    case = W.AcousticCase("afd_default", NX, NZ, PML, 2000, 10.0, 10.0, 0.0005, vp, den, [Nx // 2], [Nz // 2],
+                          -1, 28.0)
+    rx = np.full(NX, Nx // 2, np.int32)
+    rz = np.arange(PML, Nx - PML, dtype=np.int32)
+    return case, rx, rz
+
+
+@pytest.mark.parametrize("flags", [S.EXACT, 0])
+def test_afd_default_against_shipped_record(golden, flags):
+    case, rx, rz = afd_default_case()
+    w = S.wavelet(S.WAVELET_AFD, case.nt, case.dt, case.f0)
+    ref = np.fromfile(os.path.join(golden, "afd_default", "record.dat"), np.float32).reshape(100, 2000)
+    with engine_for(case, flags) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        rec = e.forward().reshape(100, 2000)
+    err = rel_l2(rec, ref)
+    print(f"afd_default flags={flags}: relL2={err:.3e} maxabs={np.abs(rec - ref).max():.3e} (max|ref|={np.abs(ref).max():.3e})")
+    if flags & S.EXACT:
+        assert bits_equal(rec, ref)
+    assert err <= TOL_FWD
+
+
+@pytest.mark.parametrize("flags", [S.EXACT, 0])
+def test_afd_default_snapshot(golden, flags):
+    """Snap.dat is Vx1 after the sponge at k = 500 (AFD:343-355): run 501 steps, read Vx."""
+    case, rx, rz = afd_default_case()
+    w = S.wavelet(S.WAVELET_AFD, 501, case.dt, case.f0)
+    ref = np.fromfile(os.path.join(golden, "afd_default", "Snap.dat"), np.float32).reshape(100, 100)
+    with engine_for(case, flags) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        e.forward()
+        vx = e.wavefield(0, S.FIELD_VX)[20:-20, 20:-20]
+    if flags & S.EXACT:
+        assert bits_equal(vx, ref)
+    assert rel_l2(vx, ref) <= TOL_FWD
+
+
+@pytest.mark.parametrize("flags", [S.EXACT, 0])
+@pytest.mark.parametrize("case_fn,fname", [(W.config1, "config1_record.f32"),
+                                           (W.small_varden, "small_varden_record.f32")])
+def test_reference_cases(golden, flags, case_fn, fname):
+    case = case_fn()
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    ref = np.fromfile(os.path.join(golden, fname), np.float32).reshape(len(rx), case.nt)
+    with engine_for(case, flags) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        rec = e.forward().reshape(ref.shape)
+        t = e.timing()
+    r64, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, case.nt, case.dx, case.dz, case.dt, case.vp, case.den,
+                               w, case.src_x[0], case.src_z[0], rx, rz, fp64=True)
+    err, err64 = rel_l2(rec, ref), rel_l2(rec, r64)
+    print(f"{case.name} flags={flags}: relL2 vs reference={err:.3e} maxabs={np.abs(rec - ref).max():.3e}; "
+          f"vs FP64 oracle={err64:.3e}; reference vs FP64={rel_l2(ref, r64):.3e}; loop {t['loop_ms']:.2f} ms")
+    if flags & S.EXACT:
+        assert bits_equal(rec, ref)
+    assert err <= TOL_FWD
+
+
+@pytest.mark.parametrize("order", [10, 8, 4])
+def test_other_orders_exact_against_oracle(order):
+    case = W.small_varden()
+    w = S.wavelet(S.WAVELET_RIC, 200, case.dt, case.f0, 60)
+    rx, rz = case.receivers()
+    with engine_for(case, S.EXACT, order=order) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        rec = e.forward().reshape(len(rx), 200)
+    ref, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, 200, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                               case.src_x[0], case.src_z[0], rx, rz, radius=order // 2)
+    assert bits_equal(rec, ref)
+
+
+def _multi_shot_setup(nshot=5, seed=3):
+    case = W.small_varden()
+    rng = np.random.default_rng(seed)
+    shots, refs = [], []
+    for s in range(nshot):
+        nt = int(rng.integers(120, 260))
+        sx = int(rng.integers(case.PML, case.Nx - case.PML))
+        sz = int(rng.integers(case.PML, case.Nz - case.PML))
+        w = S.wavelet(S.WAVELET_RIC, nt, case.dt, 20.0 + 3 * s, 40)
+        nrec = int(rng.integers(1, 50))
+        rx = rng.integers(0, case.Nx, nrec).astype(np.int32)
+        rz = rng.integers(0, case.Nz, nrec).astype(np.int32)
+        shots.append(S.ShotSpec(sx, sz, rx, rz, w))
+        ref, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, nt, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                                   sx, sz, rx, rz)
+        refs.append(ref)
+    return case, shots, refs
+
+
+def test_batched_uneven_nt_matches_oracle_and_per_shot():
+    case, shots, refs = _multi_shot_setup()
+    with engine_for(case, S.EXACT) as e:
+        e.set_shots(shots)
+        batched = e.split_records(e.forward())
+        plain = e.split_records(e.forward_per_shot())
+        t = e.timing()
+        assert t["graph"] == 0 and t["launches"] >= sum(s.nt for s in shots)
+    for b, p, r in zip(batched, plain, refs):
+        assert bits_equal(b, r)
+        assert bits_equal(p, r)
+
+
+def test_repeated_forward_is_deterministic():
+    case, shots, _ = _multi_shot_setup(3, seed=11)
+    with engine_for(case) as e:
+        e.set_shots(shots)
+        a = e.forward()
+        b = e.forward()
+    assert bits_equal(a, b)
+
+
+def test_aperture_window_equals_submodel_run():
+    """A shot with an aperture window [x0, x0 + n) of the model equals a run on the cropped
+    model (the window's own sponge sits at its edges)."""
+    case = W.small_varden()
+    x0, n = 7, 70
+    w = S.wavelet(S.WAVELET_RIC, 150, case.dt, case.f0, 40)
+    rx = np.arange(5, 60, dtype=np.int32)
+    rz = np.full_like(rx, case.PML + 2)
+    with engine_for(case, S.EXACT) as e:
+        e.set_shots([S.ShotSpec(30, case.PML + 5, rx, rz, w, ap_x0=x0, ap_nx=n)])
+        rec = e.forward()
+    sub = W.AcousticCase("sub", n - 2 * case.PML, case.NZ, case.PML, 150, case.dx, case.dz, case.dt,
+                         np.ascontiguousarray(case.vp[x0:x0 + n]), np.ascontiguousarray(case.den[x0:x0 + n]),
+                         [30], [case.PML + 5], 0, case.f0)
+    ref, _, _ = ol.afd_forward(n, case.Nz, case.PML, 150, case.dx, case.dz, case.dt, sub.vp, sub.den, w, 30,
+                               case.PML + 5, rx, rz)
+    assert bits_equal(rec.reshape(ref.shape), ref)
+
+
+def test_edge_cases_source_in_frozen_rim_and_single_step():
+    """Source inside the never-updated rim (AFD updates only [8, N-8)), one time step, a
+    receiver on the source and one in the sponge corner."""
+    case = W.small_varden()
+    for sx, sz, nt in ((3, 4, 1), (case.Nx - 2, case.Nz - 9, 40), (8, 8, 25)):
+        w = S.wavelet(S.WAVELET_RIC, nt, case.dt, 30.0, 2)
+        rx = np.array([sx, 0, case.Nx - 1, 9], np.int32)
+        rz = np.array([sz, 0, case.Nz - 1, 9], np.int32)
+        with engine_for(case, S.EXACT) as e:
+            e.set_shots([S.ShotSpec(sx, sz, rx, rz, w)])
+            rec = e.forward().reshape(4, nt)
+        ref, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, nt, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                                   sx, sz, rx, rz)
+        assert bits_equal(rec, ref), (sx, sz, nt)
+
+
+def test_zero_receivers_and_errors():
+    case = W.small_varden()
+    w = S.wavelet(S.WAVELET_RIC, 10, case.dt, 30.0, 2)
+    with engine_for(case) as e:
+        e.set_shots([S.ShotSpec(30, 30, np.zeros(0, np.int32), np.zeros(0, np.int32), w)])
+        assert e.forward().size == 0
+        with pytest.raises(S.SfdError) as ei:
+            e.set_shots([S.ShotSpec(case.Nx + 3, 30, [1], [1], w)])
+        assert ei.value.status == S.ERR_ARG
+        with pytest.raises(S.SfdError):
+            e.set_shots([S.ShotSpec(30, 30, [1], [case.Nz], w)])
+        with pytest.raises(S.SfdError) as ei:
+            e.set_model(np.zeros_like(case.vp))
+        assert ei.value.status == S.ERR_ARG
+    e2 = S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML)
+    with pytest.raises(S.SfdError) as ei:
+        e2.forward()
+    assert ei.value.status == S.ERR_STATE
+    e2.close()
+
+
+def test_nan_watchdog():
+    """An unstable time step (CFL far above the limit) must be reported as SFD_ERR_NAN."""
+    case = W.small_varden()
+    w = S.wavelet(S.WAVELET_RIC, 400, case.dt, 30.0, 10)
+    e = S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, 0.02, case.PML, flags=S.NAN_CHECK)
+    e.set_model(case.vp, case.den)
+    e.set_shots([S.ShotSpec(40, 40, [40], [40], w)])
+    with pytest.raises(S.SfdError) as ei:
+        e.forward()
+    assert ei.value.status == S.ERR_NAN
+    e.close()
+
+
+def test_config2_geometry_one_shot_exact_vs_oracle():
+    """Full config-2 grid (612 x 2148 padded, 16th order), one shot, 600 steps: bit-exact
+    against the oracle restatement (itself pinned to the reference)."""
+    case = W.config2(nshot=1, nt=600)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 60)
+    rx, rz = case.receivers()
+    with engine_for(case, S.EXACT) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        rec = e.forward().reshape(len(rx), case.nt)
+    ref, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, case.nt, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                               case.src_x[0], case.src_z[0], rx, rz)
+    assert bits_equal(rec, ref)
+
+
+def test_config2_full_size_linearity_and_batch_consistency():
+    """Size-independent properties at the full config-2 workload size (612 x 2148, 64 shots,
+    shortened to 300 steps to bound test time): scaling every wavelet by 2 scales every
+    record exactly by 2 (the scheme is linear and power-of-two scaling is exact in IEEE
+    arithmetic), and the batched launch equals the plain per-shot path bit for bit."""
+    case = W.config2(nshot=64, nt=300)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 60)
+    rx, rz = case.receivers()
+    shots = [S.ShotSpec(sx, sz, rx, rz, w) for sx, sz in zip(case.src_x, case.src_z)]
+    shots2 = [S.ShotSpec(sx, sz, rx, rz, 2 * w) for sx, sz in zip(case.src_x, case.src_z)]
+    with engine_for(case) as e:
+        e.set_shots(shots)
+        a = e.forward()
+        b = e.forward_per_shot()
+        e.set_shots(shots2)
+        c = e.forward()
+    assert np.isfinite(a).all() and np.abs(a).max() > 0
+    assert bits_equal(a, b)
+    assert bits_equal(2 * a, c)
