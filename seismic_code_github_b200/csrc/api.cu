@@ -146,8 +146,8 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.L = c->L;
     a.nz = c->g.nz;
     a.pml = c->g.pml;
-    a.vp = c->d_vp;
-    a.den = c->varden ? c->d_den : nullptr;
+    a.vp = c->d_vp + kModelGhostZ;  // row z = 0 of column 0
+    a.den = c->varden ? c->d_den + kModelGhostZ : nullptr;
     a.mpitch = c->mpitch;
     a.nx_model = c->g.nx;
     a.den_c = c->den_c;
@@ -367,19 +367,33 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
         else ctx->varden = true;
     }
     const int cols = ctx->g.nx * ctx->g.ny;
-    ctx->mpitch = round_up(ctx->g.nz, 32);
-    const size_t mbytes = sizeof(float) * (size_t)cols * ctx->mpitch;
+    const int nz = ctx->g.nz;
+    const int nzt = (nz + kTileZ - 1) / kTileZ * kTileZ;  // tiles may read past nz
+    ctx->mpitch = round_up(2 * kModelGhostZ + nzt, 32);
+    const size_t mfloats = (size_t)cols * ctx->mpitch;
     // Buffers are allocated once per context and refilled in place, so a captured time loop
     // (which bakes these pointers and the density constant in) stays valid across model updates.
     const float den_c_old = ctx->have_model ? ctx->den_c : -1.0f;
     const bool varden_old = ctx->have_model && ctx->d_den != nullptr;
-    if (!ctx->d_vp) CK(cudaMalloc(&ctx->d_vp, mbytes));
-    CK(cudaMemcpy2D(ctx->d_vp, sizeof(float) * ctx->mpitch, vp, sizeof(float) * ctx->g.nz,
-                    sizeof(float) * ctx->g.nz, cols, cudaMemcpyHostToDevice));
+    // column-wise copy with kModelGhostZ replicated rows above and replicated rows below
+    auto upload = [&](float** dst, const float* src) -> int {
+        std::vector<float> staged(mfloats);
+        for (int c = 0; c < cols; c++) {
+            const float* s = src + (size_t)c * nz;
+            float* d = staged.data() + (size_t)c * ctx->mpitch;
+            for (int k = 0; k < ctx->mpitch; k++) {
+                const int z = std::min(std::max(k - kModelGhostZ, 0), nz - 1);
+                d[k] = s[z];
+            }
+        }
+        if (!*dst) CK(cudaMalloc(dst, mfloats * sizeof(float)));
+        CK(cudaMemcpy(*dst, staged.data(), mfloats * sizeof(float), cudaMemcpyHostToDevice));
+        return SFD_OK;
+    };
+    int urc = upload(&ctx->d_vp, vp);
+    if (urc) return urc;
     if (ctx->varden) {
-        if (!ctx->d_den) CK(cudaMalloc(&ctx->d_den, mbytes));
-        CK(cudaMemcpy2D(ctx->d_den, sizeof(float) * ctx->mpitch, den, sizeof(float) * ctx->g.nz,
-                        sizeof(float) * ctx->g.nz, cols, cudaMemcpyHostToDevice));
+        if ((urc = upload(&ctx->d_den, den))) return urc;
     } else {
         dfree(ctx->d_den);
     }
@@ -450,7 +464,7 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     L.tx = ctx->plan.tx;
     L.tz = ctx->plan.tz;
     L.gx = 2 * ctx->radius;
-    L.gz = (2 * ctx->radius + 3) & ~3;
+    L.gz = ctx->plan.gz;
     L.ntx = (nx_max + L.tx - 1) / L.tx;
     L.ntz = (nz + L.tz - 1) / L.tz;
     L.pitch = round_up(L.gz + L.ntz * L.tz + L.gz, 32);

@@ -11,6 +11,10 @@
 namespace sfd {
 
 constexpr int kMaxRadius = 8;
+// Both 2-D acoustic step kernels work on the same 64 x 64 tiles, so they share the field
+// layout and the per-tile receiver tables.
+constexpr int kTileX = 64;
+constexpr int kTileZ = 64;
 
 // Per-shot descriptor in device memory (one entry per shot, indexed by shot id).
 struct ShotDev {
@@ -73,7 +77,11 @@ struct Acou2DPlan {
     int radius;
     int tx, tz, threads;
     size_t smem_bytes;
+    int gz;  // z ghost margin the step kernels need (multiple of 4)
 };
+// Model arrays on the device carry this many replicated rows above z = 0 and below z = nz - 1
+// so that vectorised halo reads stay inside the allocation and see finite values.
+constexpr int kModelGhostZ = 16;
 bool acoustic2d_plan(int radius, Acou2DPlan* plan);
 cudaError_t acoustic2d_launch_step(const Acou2DPlan& plan, const Acou2DArgs& a, int active_shots,
                                    bool exact, bool varden, cudaStream_t st);

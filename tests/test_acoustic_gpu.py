@@ -233,7 +233,8 @@ def test_config2_full_size_linearity_and_batch_consistency():
     """Size-independent properties at the full config-2 workload size (612 x 2148, 64 shots,
     shortened to 300 steps to bound test time): scaling every wavelet by 2 scales every
     record exactly by 2 (the scheme is linear and power-of-two scaling is exact in IEEE
-    arithmetic), and the batched launch equals the plain per-shot path bit for bit."""
+    arithmetic outside the gradual-underflow range, where products round to the subnormal
+    grid), and the batched launch equals the plain per-shot path bit for bit."""
     case = W.config2(nshot=64, nt=300)
     w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 60)
     rx, rz = case.receivers()
@@ -247,4 +248,7 @@ def test_config2_full_size_linearity_and_batch_consistency():
         c = e.forward()
     assert np.isfinite(a).all() and np.abs(a).max() > 0
     assert bits_equal(a, b)
-    assert bits_equal(2 * a, c)
+    normal = np.abs(a) > 1e-30  # far above FLT_MIN * 2^23, where the subnormal rounding lives
+    assert normal.sum() > 1_000_000
+    assert bits_equal((2 * a)[normal], c[normal])
+    assert np.abs(2 * a - c)[~normal].max(initial=0.0) < 1e-30
