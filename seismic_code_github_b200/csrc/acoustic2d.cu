@@ -293,6 +293,21 @@ __device__ __forceinline__ float4 fma4(float c, float4 a, float4 b) {
 }
 __device__ __forceinline__ float comp(float4 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
 
+// Asynchronous global -> shared copy of a ROWS x (4*W4) block (rows `gpitch` floats apart in
+// global memory, SPITCH floats apart in shared memory), 16 bytes per copy, L2-only caching.
+template <int ROWS, int W4, int SPITCH>
+__device__ __forceinline__ void stage_async(float* dst, const float* src, int gpitch, int tid) {
+    constexpr int N = ROWS * W4;
+#pragma unroll 4
+    for (int i = tid; i < N; i += kThreads) {
+        const int r = i / W4, c = i - r * W4;
+        const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst + r * SPITCH + 4 * c);
+        const float* g = src + (long long)r * gpitch + 4 * c;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int R, bool VARDEN>
 __global__ void __launch_bounds__(kThreads, 2)
 acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a) {
@@ -341,28 +356,11 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a) {
         sAz[i] = az;
         sMz[i] = mz;
     }
-    // ---- stage P(t), Vx(t-1), Vz(t-1) (float4, coalesced along z) ----
-    {
-        constexpr int W4 = T::SP_W / 4;
-        for (int i = tid; i < T::SP_ROWS * W4; i += kThreads) {
-            const int r = i / W4, c = i - r * W4;
-            st4(sP + r * T::SP_P + 4 * c, __ldg(reinterpret_cast<const float4*>(a.p_in + cell(x0 - T::HX + r, z0 - T::HZ + 4 * c))));
-        }
-    }
-    {
-        constexpr int W4 = T::TZ / 4;
-        for (int i = tid; i < T::SVX_ROWS * W4; i += kThreads) {
-            const int r = i / W4, c = i - r * W4;
-            st4(sVx + r * T::SVX_P + 4 * c, __ldg(reinterpret_cast<const float4*>(a.vx_in + cell(x0 - R + r, z0 + 4 * c))));
-        }
-    }
-    {
-        constexpr int W4 = T::SVZ_W / 4;
-        for (int i = tid; i < T::TX * W4; i += kThreads) {
-            const int r = i / W4, c = i - r * W4;
-            st4(sVz + r * T::SVZ_P + 4 * c, __ldg(reinterpret_cast<const float4*>(a.vz_in + cell(x0 + r, z0 - T::RQ + 4 * c))));
-        }
-    }
+    // ---- stage P(t), Vx(t-1), Vz(t-1): 16-byte asynchronous copies, all in flight at once ----
+    stage_async<T::SP_ROWS, T::SP_W / 4, T::SP_P>(sP, a.p_in + cell(x0 - T::HX, z0 - T::HZ), pitch, tid);
+    stage_async<T::SVX_ROWS, T::TZ / 4, T::SVX_P>(sVx, a.vx_in + cell(x0 - R, z0), pitch, tid);
+    stage_async<T::TX, T::SVZ_W / 4, T::SVZ_P>(sVz, a.vz_in + cell(x0, z0 - T::RQ), pitch, tid);
+    cp_async_wait_all();
     __syncthreads();
 
     float C[R];

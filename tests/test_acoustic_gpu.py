@@ -232,9 +232,10 @@ def test_config2_geometry_one_shot_exact_vs_oracle():
 def test_config2_full_size_linearity_and_batch_consistency():
     """Size-independent properties at the full config-2 workload size (612 x 2148, 64 shots,
     shortened to 300 steps to bound test time): scaling every wavelet by 2 scales every
-    record exactly by 2 (the scheme is linear and power-of-two scaling is exact in IEEE
-    arithmetic outside the gradual-underflow range, where products round to the subnormal
-    grid), and the batched launch equals the plain per-shot path bit for bit."""
+    record by 2 (the scheme is linear; power-of-two scaling is exact in IEEE arithmetic except
+    where products round to the subnormal grid ahead of the wavefront, and such one-ulp
+    differences then spread at the ulp level, hence a 1e-6 bound rather than bit equality),
+    and the batched launch equals the plain per-shot path bit for bit."""
     case = W.config2(nshot=64, nt=300)
     w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 60)
     rx, rz = case.receivers()
@@ -248,7 +249,7 @@ def test_config2_full_size_linearity_and_batch_consistency():
         c = e.forward()
     assert np.isfinite(a).all() and np.abs(a).max() > 0
     assert bits_equal(a, b)
-    normal = np.abs(a) > 1e-30  # far above FLT_MIN * 2^23, where the subnormal rounding lives
-    assert normal.sum() > 1_000_000
-    assert bits_equal((2 * a)[normal], c[normal])
-    assert np.abs(2 * a - c)[~normal].max(initial=0.0) < 1e-30
+    diff = np.abs(2.0 * a.astype(np.float64) - c)
+    assert diff.max() <= 1e-6 * np.abs(c).max()
+    assert rel_l2(c, 2.0 * a.astype(np.float64)) < 1e-7
+    assert (diff == 0).mean() > 0.9
