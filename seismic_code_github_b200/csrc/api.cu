@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "sfd_internal.h"
 
 using namespace sfd;
@@ -67,7 +69,9 @@ struct sfd_ctx {
     float* d_rec_nt = nullptr; // [nrec][nt] per shot (output layout)
     float* d_state = nullptr;  // 6 fields: p0 p1 vx0 vx1 vz0 vz1, each nshot * shot_stride
     size_t state_floats = 0;
-    int* d_flag = nullptr;
+    int* d_flag = nullptr;     // NaN watchdog
+    int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
+    CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
 
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
@@ -108,6 +112,34 @@ void dfree(T*& p) {
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D float32 tensor map over one field buffer: dims (pitch, cols, nshot), box (z, x, 1).
+int encode_field_map(sfd_ctx* ctx, CUtensorMap* m, float* base, const Layout2D& L, int nshot, const int box[2]) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return set_err(ctx, SFD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)L.pitch, (cuuint64_t)L.cols, (cuuint64_t)nshot};
+    const cuuint64_t strides[2] = {(cuuint64_t)L.pitch * 4, (cuuint64_t)L.shot_stride * 4};
+    const cuuint32_t bdim[3] = {(cuuint32_t)box[0], (cuuint32_t)box[1], 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, bdim, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(ctx, SFD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SFD_OK;
+}
+
 void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
     dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri);
@@ -122,7 +154,7 @@ void free_shot_buffers(sfd_ctx* c) {
 sfd_ctx::~sfd_ctx() {
     if (device >= 0) cudaSetDevice(device);
     free_shot_buffers(this);
-    dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag);
+    dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag); dfree(d_err);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evs) cudaEventDestroy(evs);
@@ -173,6 +205,10 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.tile_rec_ptr = c->d_trp;
     a.tile_rec_idx = c->d_tri;
     a.records = c->d_rec_tn;
+    a.tm_p = c->tmaps[i];
+    a.tm_vx = c->tmaps[2 + i];
+    a.tm_vz = c->tmaps[4 + i];
+    a.err_flag = c->d_err;
     a.step = step;
     return a;
 }
@@ -187,6 +223,7 @@ int active_shots(const sfd_ctx* c, int step) {
 // Zero the wavefields and the record buffer, inject the step-0 source sample.
 int prologue(sfd_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_rec_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
     Acou2DArgs a = make_args(ctx, -1);  // step -1 writes into buffer 0
     CK(acoustic2d_launch_inject0(a, ctx->nshot, (ctx->g.flags & SFD_EXACT) != 0, ctx->stream));
@@ -228,6 +265,9 @@ int check_ready(sfd_ctx* ctx) {
 }
 
 int finish_nan(sfd_ctx* ctx) {
+    int err = 0;
+    CK(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_err(ctx, SFD_ERR_TIMEOUT, "a step kernel gave up waiting for its tile loads");
     if (ctx->g.flags & SFD_NAN_CHECK) {
         int flag = 0;
         CK(cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
@@ -236,10 +276,48 @@ int finish_nan(sfd_ctx* ctx) {
     return SFD_OK;
 }
 
+// Tuner for the FMA step kernel's schedule (one tile per CTA with two CTAs per SM, or
+// persistent CTAs with double-buffered TMA): a few steps of each on the real shot set, the
+// faster one is kept.  SFD_FMA_STAGES=1|2 in the environment forces a schedule.
+int tune_schedule(sfd_ctx* ctx) {
+    if (ctx->g.flags & SFD_EXACT) return SFD_OK;
+    if (const char* env = std::getenv("SFD_FMA_STAGES")) {
+        const int s = std::atoi(env);
+        if (s == 1 || s == 2) {
+            ctx->plan.stages = s;
+            return SFD_OK;
+        }
+    }
+    const int act = active_shots(ctx, 0);
+    const int steps = std::min(ctx->nt_max, 6);
+    float best = 1e30f;
+    int best_s = 1;
+    for (int s = 1; s <= 2; s++) {
+        ctx->plan.stages = s;
+        int rc = prologue(ctx);
+        if (rc) return rc;
+        for (int k = 0; k < steps; k++) {
+            if (k == 2) CK(cudaEventRecord(ctx->ev0, ctx->stream));
+            CK(acoustic2d_launch_step(ctx->plan, make_args(ctx, k), act, false, ctx->varden, ctx->stream));
+        }
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        float ms = 0.0f;
+        if (steps > 2) CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (ms < best) {
+            best = ms;
+            best_s = s;
+        }
+    }
+    ctx->plan.stages = best_s;
+    return SFD_OK;
+}
+
 int run_forward(sfd_ctx* ctx, float* out_dev) {
     int rc;
     long long launches = 0;
     if (!ctx->graph_valid) {
+        if ((rc = tune_schedule(ctx)) != SFD_OK) return rc;
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         rc = enqueue_loop(ctx, &launches);
@@ -272,7 +350,7 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
     ctx->timing.device_ms = dms;
     ctx->timing.launches = launches + 2 + ((ctx->g.flags & SFD_NAN_CHECK) ? 1 : 0);
     ctx->timing.graph = 1;
-    ctx->timing.kernel_variant = 1;
+    ctx->timing.kernel_variant = (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
     double pts = 0;
     for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
     ctx->timing.point_updates = pts;
@@ -333,6 +411,8 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     CK(cudaEventCreate(&c->evs));
     CK(cudaEventCreate(&c->eve));
     CK(cudaMalloc(&c->d_flag, sizeof(int)));
+    CK(cudaMalloc(&c->d_err, sizeof(int)));
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
     if (g->scheme == SFD_ACOUSTIC_2D && !acoustic2d_plan(R, &c->plan))
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "no kernel for radius %d", R);
     *out = c.release();
@@ -530,6 +610,17 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
     ctx->state_floats = 6 * (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
+    {
+        // TMA descriptors of the six field buffers: 3-D (z, column, shot), one box per field
+        int bp[2], bvx[2], bvz[2];
+        acoustic2d_fma_boxes(ctx->radius, bp, bvx, bvz);
+        const int* boxes[3] = {bp, bvx, bvz};
+        const long long fs = (long long)nshot * L.shot_stride;
+        for (int b = 0; b < 6; b++) {
+            const int rc2 = encode_field_map(ctx, &ctx->tmaps[b], ctx->d_state + b * fs, L, nshot, boxes[b / 2]);
+            if (rc2) return rc2;
+        }
+    }
     ctx->have_shots = true;
     ctx->graph_valid = false;
     return SFD_OK;
@@ -590,7 +681,7 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
     ctx->timing.loop_ms = ms;
     ctx->timing.launches = launches + 2;
     ctx->timing.graph = 0;
-    ctx->timing.kernel_variant = 1;
+    ctx->timing.kernel_variant = (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
     double pts = 0;
     for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
     ctx->timing.point_updates = pts;

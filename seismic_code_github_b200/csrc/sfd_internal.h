@@ -1,5 +1,6 @@
 // Internal definitions shared by the host library and the kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -43,6 +44,9 @@ struct Layout2D {
 
 // Arguments of the acoustic 2-D step kernels (passed by value; pointers are device memory).
 struct Acou2DArgs {
+    // TMA descriptors of this step's input fields (3-D: z, column, shot), used by the FMA kernel
+    CUtensorMap tm_p, tm_vx, tm_vz;
+    int* err_flag;          // set to 1 by a CTA whose bounded wait ran out (SFD_ERR_TIMEOUT)
     const float* p_in;  float* p_out;
     const float* vx_in; float* vx_out;
     const float* vz_in; float* vz_out;
@@ -77,7 +81,8 @@ struct Acou2DPlan {
     int radius;
     int tx, tz, threads;
     size_t smem_bytes;
-    int gz;  // z ghost margin the step kernels need (multiple of 4)
+    int gz;      // z ghost margin the step kernels need (multiple of 4)
+    int stages;  // FMA kernel schedule (1 or 2), chosen by the context's tuner
 };
 // Model arrays on the device carry this many replicated rows above z = 0 and below z = nz - 1
 // so that vectorised halo reads stay inside the allocation and see finite values.
@@ -85,6 +90,12 @@ constexpr int kModelGhostZ = 16;
 bool acoustic2d_plan(int radius, Acou2DPlan* plan);
 cudaError_t acoustic2d_launch_step(const Acou2DPlan& plan, const Acou2DArgs& a, int active_shots,
                                    bool exact, bool varden, cudaStream_t st);
+// stages: 1 = one tile per CTA, two CTAs per SM; 2 = persistent CTAs with double-buffered TMA
+cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, bool varden, int stages,
+                                 cudaStream_t st);
+int acoustic2d_fma_gz(int radius);
+// TMA box extents (z, x) the FMA kernel loads for P, Vx and Vz at this radius.
+void acoustic2d_fma_boxes(int radius, int box_p[2], int box_vx[2], int box_vz[2]);
 cudaError_t acoustic2d_launch_inject0(const Acou2DArgs& a, int nshot, bool exact, cudaStream_t st);
 cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const ShotDev* shots, int nshot,
                                      int nrec_max, int nt_max, cudaStream_t st);

@@ -105,6 +105,48 @@ def test_other_orders_exact_against_oracle(order):
     assert bits_equal(rec, ref)
 
 
+@pytest.mark.parametrize("order", [16, 10, 8, 4, 2])
+def test_fma_path_all_orders_against_oracle(order):
+    """The FMA kernel (paired FP32, register windows) at every supported order, on the
+    non-square variable-density case, within the forward tolerance of the oracle."""
+    case = W.small_varden()
+    w = S.wavelet(S.WAVELET_RIC, 200, case.dt, case.f0, 60)
+    rx, rz = case.receivers()
+    with engine_for(case, 0, order=order) as e:
+        e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+        rec = e.forward().reshape(len(rx), 200)
+    ref, _, _ = ol.afd_forward(case.Nx, case.Nz, case.PML, 200, case.dx, case.dz, case.dt, case.vp, case.den, w,
+                               case.src_x[0], case.src_z[0], rx, rz, radius=order // 2)
+    err = rel_l2(rec, ref)
+    print(f"order {order}: FMA path relL2 vs oracle {err:.3e}")
+    assert err <= TOL_FWD
+
+
+def test_fma_path_constant_density_interior_tiles():
+    """Constant density on a grid large enough to have sponge-free interior tiles (the
+    kernel's no-sponge branch) and edge tiles, several shots with uneven nt."""
+    NX, NZ, PML = 300, 200, 20
+    v = W.layered_model(NX, NZ, 5, 1800.0, 3500.0, seed=5, anomalies=2, radius=12.0, amp=250.0, dx=10.0)
+    vp = W.pad_edges(v, PML, PML)
+    den = np.full_like(vp, 2200.0)
+    case = W.AcousticCase("interior", NX, NZ, PML, 260, 10.0, 10.0, 1e-3, vp, den, [PML + 40], [PML + 3],
+                          PML + 2, 20.0)
+    rx, rz = case.receivers()
+    shots, refs = [], []
+    for i, (sx, sz, nt) in enumerate(((PML + 40, PML + 3, 260), (PML + 150, PML + 100, 200), (PML + 290, PML + 5, 130))):
+        w = S.wavelet(S.WAVELET_RIC, nt, case.dt, 20.0 + i, 50)
+        shots.append(S.ShotSpec(sx, sz, rx, rz, w))
+        ref, _, _ = ol.afd_forward(case.Nx, case.Nz, PML, nt, case.dx, case.dz, case.dt, vp, den, w, sx, sz, rx, rz)
+        refs.append(ref)
+    with engine_for(case) as e:
+        e.set_shots(shots)
+        got = e.split_records(e.forward())
+        plain = e.split_records(e.forward_per_shot())
+    for g, p, r in zip(got, plain, refs):
+        assert bits_equal(g, p)
+        assert rel_l2(g, r) <= TOL_FWD
+
+
 def _multi_shot_setup(nshot=5, seed=3):
     case = W.small_varden()
     rng = np.random.default_rng(seed)
