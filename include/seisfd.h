@@ -150,7 +150,18 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out);
  * counterpart (the reference has no adjoint). */
 int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);
 
-/* Checkpoint interval of sfd_gradient in steps (0 = ceil(sqrt(nt))). */
+/* Same gradient with the plain per-shot schedule: shots one after another, one kernel launch
+ * per time step, no graph -- the baseline the batched gradient is measured against. */
+int sfd_gradient_per_shot(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);
+
+/* Gradient of the misfit of the last sfd_gradient call with respect to the wavelet samples of
+ * one shot (nt_shot values).  With obs = F(w) - r this is F^T r, the adjoint of the
+ * wavelet-to-records map, used by the dot-product test. */
+int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out);
+
+/* Checkpoint interval of sfd_gradient in steps (0 = ceil(sqrt(nt))).  The forward state of
+ * every shot is kept every `steps` steps; each segment is recomputed once during the
+ * backward pass, so memory is O(nt/steps + steps) wavefields per shot. */
 int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps);
 
 int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);

@@ -27,6 +27,10 @@ int oracle_afd_f32(const OracleAfdCfg* g, const float* vp, const float* den, con
                    float* record, float* snap_vx, float* final_state);
 int oracle_afd_f64(const OracleAfdCfg* g, const float* vp, const float* den, const float* wavelet,
                    double* record, double* snap_vx, double* final_state);
+// FP64 misfit 0.5*sum (rec - obs)^2, its gradient w.r.t. Vp (padded grid) and w.r.t. the
+// wavelet samples, and the FP64 records; obs and records are [nrec][nt].  Any output may be NULL.
+int oracle_afd_gradient_f64(const OracleAfdCfg* g, const float* vp, const float* den, const float* wavelet,
+                            const float* obs, double* misfit, double* grad_vp, double* dw, double* records);
 void oracle_wavelet_afd(int nt, float dt, float freq, float* out);
 void oracle_wavelet_ric(int nt, float dt, int f0, int delay, float* out);
 

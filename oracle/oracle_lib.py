@@ -100,3 +100,31 @@ def afd_forward(nx, nz, pml, nt, dx, dz, dt, vp, den, wavelet, sx, sz, rec_x, re
     if rc != 0:
         raise ValueError(f"oracle_afd rejected the configuration (rc={rc})")
     return rec, snap, state
+
+
+def afd_gradient_f64(nx, nz, pml, nt, dx, dz, dt, vp, den, wavelet, sx, sz, rec_x, rec_z, obs, radius=8):
+    """FP64 misfit, d misfit/d vp (padded grid), d misfit/d wavelet and FP64 records
+    (oracle/adj_oracle.cpp)."""
+    L = lib()
+    if not hasattr(L, "_grad_sig"):
+        L.oracle_afd_gradient_f64.argtypes = [ctypes.POINTER(OracleAfdCfg), _F32P, _F32P, _F32P, _F32P, _F64P,
+                                              _F64P, _F64P, _F64P]
+        L._grad_sig = True
+    rec_x = np.ascontiguousarray(rec_x, np.int32)
+    rec_z = np.ascontiguousarray(rec_z, np.int32)
+    vp = np.ascontiguousarray(vp, np.float32)
+    den = np.ascontiguousarray(den, np.float32)
+    wavelet = np.ascontiguousarray(wavelet, np.float32)
+    obs = np.ascontiguousarray(obs, np.float32)
+    assert obs.shape == (len(rec_x), nt)
+    cfg = OracleAfdCfg(nx, nz, pml, nt, dx, dz, dt, radius, sx, sz, len(rec_x), _p(rec_x, _I32P),
+                       _p(rec_z, _I32P), -1)
+    mis = np.zeros(1, np.float64)
+    g = np.zeros((nx, nz), np.float64)
+    dw = np.zeros(nt, np.float64)
+    rec = np.zeros((len(rec_x), nt), np.float64)
+    rc = L.oracle_afd_gradient_f64(ctypes.byref(cfg), _p(vp), _p(den), _p(wavelet), _p(obs), _p(mis, _F64P),
+                                   _p(g, _F64P), _p(dw, _F64P), _p(rec, _F64P))
+    if rc != 0:
+        raise ValueError(f"oracle_afd_gradient_f64 rejected the configuration (rc={rc})")
+    return float(mis[0]), g, dw, rec

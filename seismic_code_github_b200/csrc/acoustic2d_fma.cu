@@ -368,8 +368,14 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(-a.dt));
             const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
             const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
-            float2 pl = fma2(kl, __fadd2_rn(lo(sx[o]), dl), lo(po));
-            float2 ph = fma2(kh, __fadd2_rn(hi(sx[o]), dh), hi(po));
+            const float2 divl = __fadd2_rn(lo(sx[o]), dl), divh = __fadd2_rn(hi(sx[o]), dh);
+            float2 pl = fma2(kl, divl, lo(po));
+            float2 ph = fma2(kh, divh, hi(po));
+            if (a.div_out != nullptr && gx < nx && gz < nz) {  // recomputation for the adjoint
+                float* dp = a.div_out + cell(gx, gz);
+                if (gz + 3 < nz) *reinterpret_cast<float4*>(dp) = cat(divl, divh);
+                else for (int qq = 0; qq < 4 && gz + qq < nz; qq++) dp[qq] = comp(cat(divl, divh), qq);
+            }
             if (EDGE) {
                 const float ax = sAx[row + R], mx = sMx[row + R];
                 const float4 sa = ax >= 0.0f ? make_float4(ax, ax, ax, ax) : az;

@@ -76,7 +76,23 @@ struct sfd_ctx {
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
+    // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
+    int grad_C = 0, grad_ncp = 0;
+    float* d_ckpt = nullptr;    // [ncp][3 fields][nshot * shot_stride]
+    float* d_div = nullptr;     // [C][nshot * shot_stride]: D_k of the segment being recomputed
+    float* d_adj = nullptr;     // adjoint state: q0 q1 x0 x1 z0 z1
+    float* d_gseg = nullptr;    // per-segment imaging sum (float)
+    double* d_gacc = nullptr;   // imaging sum over all segments (double)
+    float* d_obs_nt = nullptr;  // observed records as given ([nrec][nt] per shot)
+    float* d_obs_tn = nullptr;  // ... transposed to [nt][nrec]
+    float* d_res = nullptr;     // residuals [nt][nrec]
+    float* d_lam = nullptr;     // [nshot][nt_max] adjoint of P at the source cell
+    double* d_misfit = nullptr;
+    double* d_grad = nullptr;   // gradient on the model grid (double)
+    cudaGraphExec_t grad_graph = nullptr;
+    bool grad_valid = false;
+    bool have_grad = false;
     sfd_timing timing{};
 
     ~sfd_ctx();
@@ -147,6 +163,14 @@ void free_shot_buffers(sfd_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
     c->graph_valid = false;
+    dfree(c->d_ckpt); dfree(c->d_div); dfree(c->d_adj); dfree(c->d_gseg); dfree(c->d_gacc);
+    dfree(c->d_obs_nt); dfree(c->d_obs_tn); dfree(c->d_res); dfree(c->d_lam); dfree(c->d_misfit);
+    dfree(c->d_grad);
+    if (c->grad_graph) cudaGraphExecDestroy(c->grad_graph);
+    c->grad_graph = nullptr;
+    c->grad_valid = false;
+    c->have_grad = false;
+    c->grad_C = c->grad_ncp = 0;
 }
 
 }  // namespace
@@ -357,6 +381,268 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
     return finish_nan(ctx);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Gradient: forward with checkpoints every C steps, residuals and misfit, then for each segment
+// (last to first) restore its checkpoint, recompute its C forward steps keeping D_k, and run
+// the C adjoint steps backwards accumulating the zero-lag imaging sum.
+// ---------------------------------------------------------------------------------------------
+int grad_alloc(sfd_ctx* ctx) {
+    const int C = ctx->ckpt_interval > 0 ? std::min(ctx->ckpt_interval, ctx->nt_max)
+                                         : (int)std::ceil(std::sqrt((double)ctx->nt_max));
+    const int ncp = (ctx->nt_max + C - 1) / C;
+    if (ctx->d_ckpt && C == ctx->grad_C && ncp == ctx->grad_ncp) return SFD_OK;
+    dfree(ctx->d_ckpt); dfree(ctx->d_div);
+    if (ctx->grad_graph) cudaGraphExecDestroy(ctx->grad_graph);
+    ctx->grad_graph = nullptr;
+    ctx->grad_valid = false;
+    const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
+    const size_t nrec = std::max<long long>(1, ctx->rec_total);
+    CK(cudaMalloc(&ctx->d_ckpt, sizeof(float) * fs * 3 * ncp));
+    CK(cudaMalloc(&ctx->d_div, sizeof(float) * fs * C));
+    if (!ctx->d_adj) {
+        CK(cudaMalloc(&ctx->d_adj, sizeof(float) * fs * 6));
+        CK(cudaMalloc(&ctx->d_gseg, sizeof(float) * fs));
+        CK(cudaMalloc(&ctx->d_gacc, sizeof(double) * fs));
+        CK(cudaMalloc(&ctx->d_obs_nt, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_obs_tn, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_res, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_lam, sizeof(float) * (size_t)ctx->nshot * ctx->nt_max));
+        CK(cudaMalloc(&ctx->d_misfit, sizeof(double)));
+        CK(cudaMalloc(&ctx->d_grad, sizeof(double) * (size_t)ctx->g.nx * ctx->g.nz));
+    }
+    ctx->grad_C = C;
+    ctx->grad_ncp = ncp;
+    return SFD_OK;
+}
+
+// shots [first, first + count) as one schedule; `slots` maps launch slots to shots
+struct GradRange {
+    int first, count;
+    const int* slots;
+    bool batched;
+};
+
+int range_active(const sfd_ctx* ctx, const GradRange& r, int k) {
+    if (r.batched) return active_shots(ctx, k);
+    return ctx->h_shots[r.first].nt > k ? 1 : 0;
+}
+
+int grad_fwd_step(sfd_ctx* ctx, const GradRange& r, int k, int act, float* div_out) {
+    Acou2DArgs a = make_args(ctx, k);
+    a.slot_to_shot = r.slots;
+    a.div_out = div_out;
+    CK(acoustic2d_fma_launch(ctx->radius, a, act, ctx->varden, ctx->plan.stages, ctx->stream));
+    return SFD_OK;
+}
+
+int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
+    const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+    float* Q[2] = {ctx->d_adj, ctx->d_adj + fs};
+    float* X[2] = {ctx->d_adj + 2 * fs, ctx->d_adj + 3 * fs};
+    float* Z[2] = {ctx->d_adj + 4 * fs, ctx->d_adj + 5 * fs};
+    const int i = (k + 1) & 1, o = k & 1;
+    const Acou2DArgs f = make_args(ctx, k);
+    Adj2DArgs a{};
+    a.q_in = Q[i]; a.q_out = Q[o];
+    a.x_in = X[i]; a.x_out = X[o];
+    a.z_in = Z[i]; a.z_out = Z[o];
+    a.div = div;
+    a.g_seg = ctx->d_gseg;
+    a.L = ctx->L;
+    a.nz = ctx->g.nz;
+    a.pml = ctx->g.pml;
+    a.vp = f.vp;
+    a.den = f.den;
+    a.mpitch = ctx->mpitch;
+    a.nx_model = ctx->g.nx;
+    a.den_c = ctx->den_c;
+    a.dt = ctx->g.dt;
+    a.dtdx = f.dtdx;
+    a.dtdz = f.dtdz;
+    a.rdx = f.rdx_f;
+    a.rdz = f.rdz_f;
+    std::memcpy(a.coef, f.coef, sizeof(a.coef));
+    std::memcpy(a.sponge, f.sponge, sizeof(a.sponge));
+    a.shots = ctx->d_shots;
+    a.slot_to_shot = r.slots;
+    a.res = ctx->d_res;
+    a.rec_x = ctx->d_rec_x;
+    a.rec_z = ctx->d_rec_z;
+    a.tile_rec_ptr = ctx->d_trp;
+    a.tile_rec_idx = ctx->d_tri;
+    a.lam_src = ctx->d_lam;
+    a.nt_max = ctx->nt_max;
+    a.step = k;
+    CK(adjoint2d_launch_step(ctx->radius, a, act, ctx->varden, ctx->stream));
+    return SFD_OK;
+}
+
+// copy the three forward fields of parity b for the shots of r between the state and a
+// checkpoint slot (to_ckpt = save, else restore)
+int grad_copy_state(sfd_ctx* ctx, const GradRange& r, int slot, int b, bool to_ckpt) {
+    const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
+    const size_t off = (size_t)r.first * ctx->L.shot_stride, len = (size_t)r.count * ctx->L.shot_stride;
+    for (int f = 0; f < 3; f++) {
+        float* st = ctx->d_state + (2 * f + b) * fs + off;
+        float* ck = ctx->d_ckpt + ((size_t)slot * 3 + f) * fs + off;
+        CK(cudaMemcpyAsync(to_ckpt ? ck : st, to_ckpt ? st : ck, len * sizeof(float), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    }
+    return SFD_OK;
+}
+
+int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches) {
+    int rc;
+    const int C = ctx->grad_C, ncp = ctx->grad_ncp;
+    const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
+    const size_t off = (size_t)r.first * ctx->L.shot_stride, len = (size_t)r.count * ctx->L.shot_stride;
+    int nrec_max = 0;
+    for (int s = r.first; s < r.first + r.count; s++) nrec_max = std::max(nrec_max, ctx->h_shots[s].nrec);
+    // forward with checkpoints
+    for (int k = 0; k < ctx->nt_max; k++) {
+        const int act = range_active(ctx, r, k);
+        if (act == 0) break;
+        if (k % C == 0 && (rc = grad_copy_state(ctx, r, k / C, k & 1, true))) return rc;
+        if ((rc = grad_fwd_step(ctx, r, k, act, nullptr))) return rc;
+        (*launches)++;
+    }
+    // residuals of this range and the misfit
+    const ShotDev& s0 = ctx->h_shots[r.first];
+    const ShotDev& s1 = ctx->h_shots[r.first + r.count - 1];
+    const long long rb = s0.rec_base, re = s1.rec_base + (long long)s1.nrec * s1.nt;
+    CK(launch_residual(ctx->d_rec_tn + rb, ctx->d_obs_tn + rb, ctx->d_res + rb, re - rb, ctx->d_misfit, ctx->stream));
+    CK(launch_adjoint_init(ctx->d_adj, ctx->d_adj + fs, ctx->L, ctx->d_shots, r.first, r.count, ctx->d_res,
+                           ctx->d_rec_x, ctx->d_rec_z, nrec_max, ctx->stream));
+    *launches += 2;
+    // segments, last to first
+    for (int j = ncp - 1; j >= 0; j--) {
+        const int k0 = j * C, k1 = std::min(k0 + C, ctx->nt_max);
+        if (range_active(ctx, r, k0) == 0) continue;
+        if ((rc = grad_copy_state(ctx, r, j, k0 & 1, false))) return rc;
+        CK(cudaMemsetAsync(ctx->d_gseg + off, 0, len * sizeof(float), ctx->stream));
+        for (int k = k0; k < k1; k++) {
+            const int act = range_active(ctx, r, k);
+            if (act == 0) break;
+            if ((rc = grad_fwd_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * fs))) return rc;
+            (*launches)++;
+        }
+        for (int k = k1 - 1; k >= k0; k--) {
+            const int act = range_active(ctx, r, k);
+            if (act == 0) continue;
+            if ((rc = grad_adj_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * fs))) return rc;
+            (*launches)++;
+        }
+        CK(launch_accumulate(ctx->d_gacc + off, ctx->d_gseg + off, (long long)len, ctx->stream));
+        (*launches)++;
+    }
+    return SFD_OK;
+}
+
+int enqueue_gradient(sfd_ctx* ctx, bool batched, long long* launches) {
+    int rc;
+    const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
+    if ((rc = prologue(ctx))) return rc;
+    CK(cudaMemsetAsync(ctx->d_misfit, 0, sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_adj, 0, 6 * fs * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_gacc, 0, fs * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_lam, 0, sizeof(float) * (size_t)ctx->nshot * ctx->nt_max, ctx->stream));
+    int nrec_max = 0;
+    for (const auto& s : ctx->h_shots) nrec_max = std::max(nrec_max, s.nrec);
+    CK(launch_records_transpose_in(ctx->d_obs_nt, ctx->d_obs_tn, ctx->d_shots, ctx->nshot, nrec_max, ctx->nt_max,
+                                   ctx->stream));
+    *launches += 2;
+    if (batched) {
+        const GradRange r{0, ctx->nshot, ctx->d_slot, true};
+        if ((rc = enqueue_gradient_range(ctx, r, launches))) return rc;
+    } else {
+        for (int s = 0; s < ctx->nshot; s++) {
+            const GradRange r{s, 1, ctx->d_ident + s, false};
+            if ((rc = enqueue_gradient_range(ctx, r, launches))) return rc;
+        }
+    }
+    const Acou2DArgs f = make_args(ctx, 0);
+    CK(launch_gradient_reduce(ctx->d_gacc, ctx->L, ctx->d_shots, ctx->nshot, f.vp, f.den, ctx->den_c, ctx->mpitch,
+                              ctx->g.nx, ctx->g.nz, ctx->g.dt, ctx->d_grad, ctx->stream));
+    (*launches)++;
+    return SFD_OK;
+}
+
+int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq, bool batched) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!obs) return set_err(ctx, SFD_ERR_ARG, "observed records are required");
+    if (grad_invq) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
+    auto t0 = std::chrono::steady_clock::now();
+    if ((rc = grad_alloc(ctx))) return rc;
+    if (!ctx->graph_valid && (rc = tune_schedule(ctx))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total, cudaMemcpyHostToDevice, ctx->stream));
+    long long launches = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (batched) {
+        if (!ctx->grad_valid) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_gradient(ctx, true, &launches);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CK(e);
+            if (ctx->grad_graph) cudaGraphExecDestroy(ctx->grad_graph);
+            e = cudaGraphInstantiate(&ctx->grad_graph, g, 0);
+            cudaGraphDestroy(g);
+            CK(e);
+            ctx->grad_valid = true;
+            ctx->timing.launches = launches;
+        }
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        CK(cudaGraphLaunch(ctx->grad_graph, ctx->stream));
+    } else {
+        if ((rc = enqueue_gradient(ctx, false, &launches))) return rc;
+        ctx->timing.launches = launches;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    int err = 0;
+    CK(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_err(ctx, SFD_ERR_TIMEOUT, "a step kernel gave up waiting for its tile loads");
+    ctx->timing.loop_ms = ms;
+    ctx->timing.device_ms = ms;
+    ctx->timing.graph = batched ? 1 : 0;
+    ctx->timing.kernel_variant = 20 + ctx->plan.stages;
+    double pts = 0;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
+    ctx->timing.point_updates = 3 * pts;  // forward, recomputation, adjoint
+    double mis = 0;
+    CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
+    if (misfit) *misfit = (float)mis;
+    ctx->have_grad = true;
+    if (grad_vp) {
+        const size_t n = (size_t)ctx->g.nx * ctx->g.nz;
+        std::vector<double> g(n);
+        CK(cudaMemcpy(g.data(), ctx->d_grad, n * sizeof(double), cudaMemcpyDeviceToHost));
+        // source scaling: P[src] -= (dt DEN Vp) w[k]  ->  -dt DEN sum_k lambda_k[src] w[k]
+        std::vector<float> lam((size_t)ctx->nshot * ctx->nt_max);
+        CK(cudaMemcpy(lam.data(), ctx->d_lam, lam.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < ctx->nshot; s++) {
+            const ShotDev& sd = ctx->h_shots[s];
+            const size_t mi = (size_t)(sd.x0 + sd.sx) * ctx->g.nz + sd.sz;
+            const double den = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
+            double sw = 0;
+            for (int j = 0; j < sd.nt; j++) sw += (double)lam[(size_t)s * ctx->nt_max + j] * ctx->h_wav[sd.wav_off + j];
+            g[mi] += -(double)ctx->g.dt * den * sw;
+        }
+        for (size_t i = 0; i < n; i++) grad_vp[i] = (float)g[i];
+    }
+    ctx->timing.h2d_bytes = (long long)sizeof(float) * ctx->rec_total;
+    ctx->timing.d2h_bytes = grad_vp ? (long long)sizeof(float) * ctx->g.nx * ctx->g.nz : 0;
+    ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SFD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -478,7 +764,10 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
         dfree(ctx->d_den);
     }
     (void)q;
-    if (ctx->varden != varden_old || (!ctx->varden && ctx->den_c != den_c_old)) ctx->graph_valid = false;
+    if (ctx->varden != varden_old || (!ctx->varden && ctx->den_c != den_c_old)) {
+        ctx->graph_valid = false;
+        ctx->grad_valid = false;
+    }
     ctx->have_model = true;
     // source scale factors depend on the model
     if (ctx->have_shots) {
@@ -722,9 +1011,21 @@ int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps) {
 }
 
 int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq) {
-    (void)obs; (void)misfit; (void)grad_vp; (void)grad_invq;
-    if (!ctx) return SFD_ERR_ARG;
-    return set_err(ctx, SFD_ERR_UNSUPPORTED, "gradient is not implemented yet");
+    return run_gradient(ctx, obs, misfit, grad_vp, grad_invq, true);
+}
+
+int sfd_gradient_per_shot(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq) {
+    return run_gradient(ctx, obs, misfit, grad_vp, grad_invq, false);
+}
+
+int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out) {
+    if (!ctx || !out) return SFD_ERR_ARG;
+    if (!ctx->have_grad) return set_err(ctx, SFD_ERR_STATE, "sfd_gradient has not been called");
+    if (shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
+    const ShotDev& sd = ctx->h_shots[shot];
+    CK(cudaMemcpy(out, ctx->d_lam + (size_t)shot * ctx->nt_max, sizeof(float) * sd.nt, cudaMemcpyDeviceToHost));
+    for (int j = 0; j < sd.nt; j++) out[j] = -sd.inj_scale * out[j];  // d misfit / d w[j] = -s lambda_j[src]
+    return SFD_OK;
 }
 
 int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out) {

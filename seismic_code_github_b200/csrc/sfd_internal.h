@@ -74,7 +74,49 @@ struct Acou2DArgs {
     const int* tile_rec_idx;   // receiver index within the shot
     float* records;            // [nt][nrec] per shot at ShotDev::rec_base
     int step;
+    float* div_out;            // optional: D = rdx S-x Vx + rdz S-z Vz of this step (field layout)
 };
+
+// Arguments of the adjoint step kernel (adjoint2d.cu); field buffers share Layout2D.
+struct Adj2DArgs {
+    const float* q_in;  float* q_out;   // adjoint of P
+    const float* x_in;  float* x_out;   // adjoint of the unsponged Vx
+    const float* z_in;  float* z_out;   // adjoint of the unsponged Vz
+    const float* div;                   // D_k of the forward step being transposed
+    float* g_seg;                       // per-shot imaging accumulator (field layout)
+    Layout2D L;
+    int nz, pml;
+    const float* vp; const float* den;  // model (row z = 0 of column 0), den NULL = constant
+    int mpitch, nx_model;
+    float den_c, dt, dtdx, dtdz, rdx, rdz;
+    float coef[kMaxRadius];
+    float sponge[256];
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* res;                   // residuals, [nt][nrec] per shot at ShotDev::rec_base
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr; const int* tile_rec_idx;
+    float* lam_src;                     // [shot][nt_max]: adjoint of P at the source cell
+    int nt_max;
+    int step;
+};
+cudaError_t adjoint2d_launch_step(int radius, const Adj2DArgs& a, int active, bool varden, cudaStream_t st);
+// residual = pred - obs (both [nt][nrec] per shot), misfit += 0.5 sum residual^2 (double)
+cudaError_t launch_residual(const float* pred, const float* obs, float* res, long long n, double* misfit,
+                            cudaStream_t st);
+// records [nrec][nt] per shot -> [nt][nrec] per shot
+cudaError_t launch_records_transpose_in(const float* rec_nt, float* rec_tn, const ShotDev* shots, int nshot,
+                                        int nrec_max, int nt_max, cudaStream_t st);
+// adjoint initial state: Q(shot, buffer nt & 1) = R^T res[nt-1]
+cudaError_t launch_adjoint_init(float* q0, float* q1, const Layout2D& L, const ShotDev* shots, int first_shot,
+                                int nshot, const float* res, const int* rec_x, const int* rec_z, int nrec_max,
+                                cudaStream_t st);
+// acc (double) += seg (float) over n values
+cudaError_t launch_accumulate(double* acc, const float* seg, long long n, cudaStream_t st);
+// grad_model[x][z] = scale(x, z) * sum over shots of acc_s(x - ap_x0_s, z), scale = -2 den vp dt
+cudaError_t launch_gradient_reduce(const double* acc, const Layout2D& L, const ShotDev* shots, int nshot,
+                                   const float* vp, const float* den, float den_c, int mpitch, int nx_model,
+                                   int nz, float dt, double* grad_model, cudaStream_t st);
 
 // Host-side launchers (acoustic2d.cu).
 struct Acou2DPlan {

@@ -53,6 +53,8 @@ SIGNATURES = {
     "sfd_forward_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P]),
     "sfd_get_wavefield": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _F32P]),
     "sfd_gradient": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
+    "sfd_gradient_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
+    "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "sfd_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _F32P]),
@@ -237,15 +239,24 @@ class Engine:
         self._check(self._lib.sfd_get_wavefield(self._h, shot, field, _fp(out)), "sfd_get_wavefield")
         return out
 
-    def gradient(self, obs: np.ndarray, want_invq: bool = False):
-        obs = np.ascontiguousarray(obs, np.float32)
+    def gradient(self, obs: np.ndarray, want_invq: bool = False, per_shot: bool = False):
+        """misfit 0.5*sum (pred - obs)^2 and its gradient w.r.t. vp (and 1/Q for the
+        viscoacoustic scheme); obs in the record layout of forward()."""
+        obs = np.ascontiguousarray(obs, np.float32).reshape(-1)
+        assert obs.size == self.record_size()
         mis = np.zeros(1, np.float32)
         n = self.grid.nx * self.grid.ny * self.grid.nz
         g = np.empty(n, np.float32)
         gq = np.empty(n, np.float32) if want_invq else None
-        self._check(self._lib.sfd_gradient(self._h, _fp(obs), _fp(mis), _fp(g), _fp(gq)), "sfd_gradient")
+        fn = self._lib.sfd_gradient_per_shot if per_shot else self._lib.sfd_gradient
+        self._check(fn(self._h, _fp(obs), _fp(mis), _fp(g), _fp(gq)), "sfd_gradient")
         shape = (self.grid.nx, self.grid.nz) if self.grid.ny == 1 else (self.grid.nx, self.grid.ny, self.grid.nz)
         return float(mis[0]), g.reshape(shape), (None if gq is None else gq.reshape(shape))
+
+    def wavelet_gradient(self, shot: int) -> np.ndarray:
+        out = np.empty(self._shots[shot].nt, np.float32)
+        self._check(self._lib.sfd_get_wavelet_gradient(self._h, shot, _fp(out)), "sfd_get_wavelet_gradient")
+        return out
 
     def set_checkpoint_interval(self, steps: int):
         self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
