@@ -31,6 +31,22 @@ int oracle_afd_f64(const OracleAfdCfg* g, const float* vp, const float* den, con
 // wavelet samples, and the FP64 records; obs and records are [nrec][nt].  Any output may be NULL.
 int oracle_afd_gradient_f64(const OracleAfdCfg* g, const float* vp, const float* den, const float* wavelet,
                             const float* obs, double* misfit, double* grad_vp, double* dw, double* records);
+// Visco-elastic RSG modelling of one shot, forward/Q_forward (flat surface).  The model arrays
+// are the interior (nz, nx) Fortran arrays (x-major, z fastest); records are [nxe][nt].
+typedef struct {
+    int nx, nz;                    // interior model size (nx_v, nz_v)
+    float dx, dz, dt, f0;
+    int nt;                        // record length (samples after the decay steps)
+    int npxn, npxp, npzn, npzp;    // pad cells, nint(pml/d)+1 (QM:105-108)
+    int ixmine, ixmaxe;            // aperture window (QM:128-129), 1-based model columns
+    int isxe, isze;                // source cell in the padded grid, 1-based (QS:374-375)
+    int nrz0;                      // receiver row offset, nint(rz0/dz)+1 (QM:112)
+    int q_override;                // 1: Q = 1e5 everywhere (QM:418-419)
+} OracleQCfg;
+int oracle_q_f32(const OracleQCfg* c, const float* vp, const float* vs, const float* rho, const float* qp,
+                 const float* qs, float* rec1, float* rec2, float* final_sxx);
+int oracle_q_f64(const OracleQCfg* c, const float* vp, const float* vs, const float* rho, const float* qp,
+                 const float* qs, double* rec1, double* rec2, double* final_sxx);
 void oracle_wavelet_afd(int nt, float dt, float freq, float* out);
 void oracle_wavelet_ric(int nt, float dt, int f0, int delay, float* out);
 

@@ -128,3 +128,49 @@ def afd_gradient_f64(nx, nz, pml, nt, dx, dz, dt, vp, den, wavelet, sx, sz, rec_
     if rc != 0:
         raise ValueError(f"oracle_afd_gradient_f64 rejected the configuration (rc={rc})")
     return float(mis[0]), g, dw, rec
+
+
+class OracleQCfg(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int), ("npxn", ctypes.c_int),
+                ("npxp", ctypes.c_int), ("npzn", ctypes.c_int), ("npzp", ctypes.c_int), ("ixmine", ctypes.c_int),
+                ("ixmaxe", ctypes.c_int), ("isxe", ctypes.c_int), ("isze", ctypes.c_int), ("nrz0", ctypes.c_int),
+                ("q_override", ctypes.c_int)]
+
+
+def q_decay(f0: float, dt: float) -> int:
+    """QM:279-280: nwt = 2*nint(1.2/(f0*dt)) in single precision, decay = nint(nwt/2)."""
+    x = float(np.float32(1.2) / (np.float32(f0) * np.float32(dt)))
+    nwt = 2 * int(np.floor(x + 0.5))
+    return int(np.floor(nwt / 2.0 + 0.5))
+
+
+def q_forward(vp, vs, rho, qp, qs, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz0=1, ixmine=None, ixmaxe=None,
+              q_override=False, fp64=False, want_final=False):
+    """Restated Q_forward single-shot modelling (oracle/q_oracle.cpp). Model arrays are the
+    interior (nx, nz) float32 x-major arrays; returns (record1 = strzz, record2 = strxx, final
+    strxx or None), records [nxe][nt]."""
+    L = lib()
+    if not hasattr(L, "_q_sig"):
+        tp = ctypes.POINTER(OracleQCfg)
+        L.oracle_q_f32.argtypes = [tp, _F32P, _F32P, _F32P, _F32P, _F32P, _F32P, _F32P, _F32P]
+        L.oracle_q_f64.argtypes = [tp, _F32P, _F32P, _F32P, _F32P, _F32P, _F64P, _F64P, _F64P]
+        L._q_sig = True
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (vp, vs, rho, qp, qs)]
+    nx, nz = arrs[0].shape
+    ixmine = 0 if ixmine is None else ixmine
+    ixmaxe = nx - 1 if ixmaxe is None else ixmaxe
+    nxe = ixmaxe - ixmine + 1
+    cfg = OracleQCfg(nx, nz, dx, dz, dt, f0, nt, npx, npx, npz, npz, ixmine, ixmaxe, isxe, isze, nrz0,
+                     1 if q_override else 0)
+    dt_ = np.float64 if fp64 else np.float32
+    tp = _F64P if fp64 else _F32P
+    r1 = np.zeros((nxe, nt), dt_)
+    r2 = np.zeros((nxe, nt), dt_)
+    fin = np.zeros((nx + 2 * npx if ixmine == 0 and ixmaxe == nx - 1 else nxe + 2 * npx, nz + 2 * npz), dt_) \
+        if want_final else None
+    fn = L.oracle_q_f64 if fp64 else L.oracle_q_f32
+    rc = fn(ctypes.byref(cfg), *[_p(a) for a in arrs], _p(r1, tp), _p(r2, tp), _p(fin, tp))
+    if rc != 0:
+        raise ValueError(f"oracle_q rejected the configuration (rc={rc})")
+    return r1, r2, fin

@@ -76,6 +76,15 @@ struct sfd_ctx {
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
+    // viscoacoustic scheme: prepared model (QS:434-551), sponge tables, source stamps
+    float* q_busg = nullptr;
+    float* q_p1 = nullptr;
+    float* q_p2 = nullptr;
+    float q_rtau = 0.0f;
+    float* d_spg = nullptr;
+    int spg_stride = 0;
+    float* d_stamps = nullptr;
+
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
     int grad_C = 0, grad_ncp = 0;
@@ -159,7 +168,7 @@ int encode_field_map(sfd_ctx* ctx, CUtensorMap* m, float* base, const Layout2D& 
 void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
     dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri);
-    dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state);
+    dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
     c->graph_valid = false;
@@ -179,6 +188,7 @@ sfd_ctx::~sfd_ctx() {
     if (device >= 0) cudaSetDevice(device);
     free_shot_buffers(this);
     dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag); dfree(d_err);
+    dfree(q_busg); dfree(q_p1); dfree(q_p2); dfree(d_spg);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evs) cudaEventDestroy(evs);
@@ -244,24 +254,76 @@ int active_shots(const sfd_ctx* c, int step) {
     return n;
 }
 
+// Arguments of the viscoacoustic step (fields in place, eight slabs per shot).
+QArgs make_qargs(const sfd_ctx* c, int step) {
+    QArgs a{};
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    float* f[8];
+    for (int i = 0; i < 8; i++) f[i] = c->d_state + i * fs;
+    a.vx = f[0]; a.vz = f[1]; a.sx = f[2]; a.sz = f[3]; a.sr = f[4]; a.rx = f[5]; a.rz = f[6]; a.rr = f[7];
+    a.L = c->L;
+    a.nz = c->g.nz;
+    a.npx = a.npz = c->g.pml;
+    a.busg = c->q_busg + kModelGhostZ;
+    a.p1 = c->q_p1 + kModelGhostZ;
+    a.p2 = c->q_p2 + kModelGhostZ;
+    a.mpitch = c->mpitch;
+    a.nx_model = c->g.nx;
+    a.dt = c->g.dt;
+    a.f_mem = c->g.dt * (-1.0f * c->q_rtau);  // QS:1160 dt*(-1.0*rtaustss)
+    a.hx = 0.5f / c->g.dx;
+    a.hz = 0.5f / c->g.dz;
+    a.dz2 = c->g.dz * c->g.dz;
+    const float af[5] = {19845.0f / 16384.0f, -735.0f / 8192.0f, 567.0f / 40960.0f, -405.0f / 229376.0f,
+                         35.0f / 294912.0f};
+    std::memcpy(a.a, af, sizeof(af));
+    a.spg = c->d_spg;
+    a.spg_stride = c->spg_stride;
+    a.shots = c->d_shots;
+    a.slot_to_shot = c->d_slot;
+    a.wavelets = c->d_wav;
+    a.stamps = c->d_stamps;
+    a.rec_x = c->d_rec_x;
+    a.rec_z = c->d_rec_z;
+    a.tile_rec_ptr = c->d_trp;
+    a.tile_rec_idx = c->d_tri;
+    a.records = c->d_rec_tn;
+    a.step = step;
+    return a;
+}
+
+int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* launches) {
+    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        QArgs q = make_qargs(ctx, k);
+        q.slot_to_shot = slots;
+        CK(viscoac2d_launch_step(q, act, ctx->stream));
+        *launches += 2;
+        return SFD_OK;
+    }
+    Acou2DArgs a = make_args(ctx, k);
+    a.slot_to_shot = slots;
+    CK(acoustic2d_launch_step(ctx->plan, a, act, (ctx->g.flags & SFD_EXACT) != 0, ctx->varden, ctx->stream));
+    *launches += 1;
+    return SFD_OK;
+}
+
 // Zero the wavefields and the record buffer, inject the step-0 source sample.
 int prologue(sfd_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_rec_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return SFD_OK;  // its source is added inside every step
     Acou2DArgs a = make_args(ctx, -1);  // step -1 writes into buffer 0
     CK(acoustic2d_launch_inject0(a, ctx->nshot, (ctx->g.flags & SFD_EXACT) != 0, ctx->stream));
     return SFD_OK;
 }
 
 int enqueue_loop(sfd_ctx* ctx, long long* launches) {
-    const bool exact = (ctx->g.flags & SFD_EXACT) != 0;
     for (int k = 0; k < ctx->nt_max; k++) {
         const int act = active_shots(ctx, k);
         if (act == 0) break;
-        Acou2DArgs a = make_args(ctx, k);
-        CK(acoustic2d_launch_step(ctx->plan, a, act, exact, ctx->varden, ctx->stream));
-        (*launches)++;
+        const int rc = launch_one_step(ctx, k, ctx->d_slot, act, launches);
+        if (rc) return rc;
     }
     return SFD_OK;
 }
@@ -282,7 +344,7 @@ int check_ready(sfd_ctx* ctx) {
     if (!ctx) return SFD_ERR_ARG;
     if (!ctx->have_model) return set_err(ctx, SFD_ERR_STATE, "sfd_set_model has not been called");
     if (!ctx->have_shots) return set_err(ctx, SFD_ERR_STATE, "sfd_set_shots has not been called");
-    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D && ctx->g.scheme != SFD_VISCOAC_2D)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d forward is not implemented", ctx->g.scheme);
     CK(cudaSetDevice(ctx->device));
     return SFD_OK;
@@ -304,7 +366,7 @@ int finish_nan(sfd_ctx* ctx) {
 // persistent CTAs with double-buffered TMA): a few steps of each on the real shot set, the
 // faster one is kept.  SFD_FMA_STAGES=1|2 in the environment forces a schedule.
 int tune_schedule(sfd_ctx* ctx) {
-    if (ctx->g.flags & SFD_EXACT) return SFD_OK;
+    if ((ctx->g.flags & SFD_EXACT) || ctx->g.scheme != SFD_ACOUSTIC_2D) return SFD_OK;
     if (const char* env = std::getenv("SFD_FMA_STAGES")) {
         const int s = std::atoi(env);
         if (s == 1 || s == 2) {
@@ -313,27 +375,24 @@ int tune_schedule(sfd_ctx* ctx) {
         }
     }
     const int act = active_shots(ctx, 0);
-    const int steps = std::min(ctx->nt_max, 6);
-    float best = 1e30f;
-    int best_s = 1;
-    for (int s = 1; s <= 2; s++) {
-        ctx->plan.stages = s;
-        int rc = prologue(ctx);
-        if (rc) return rc;
-        for (int k = 0; k < steps; k++) {
-            if (k == 2) CK(cudaEventRecord(ctx->ev0, ctx->stream));
-            CK(acoustic2d_launch_step(ctx->plan, make_args(ctx, k), act, false, ctx->varden, ctx->stream));
+    const int steps = std::min(ctx->nt_max, 10);
+    float best[3] = {1e30f, 1e30f, 1e30f};
+    for (int round = 0; round < 2; round++)  // two rounds, best of each schedule
+        for (int s = 1; s <= 2; s++) {
+            ctx->plan.stages = s;
+            int rc = prologue(ctx);
+            if (rc) return rc;
+            for (int k = 0; k < steps; k++) {
+                if (k == 2) CK(cudaEventRecord(ctx->ev0, ctx->stream));
+                CK(acoustic2d_launch_step(ctx->plan, make_args(ctx, k), act, false, ctx->varden, ctx->stream));
+            }
+            CK(cudaEventRecord(ctx->ev1, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            float ms = 0.0f;
+            if (steps > 2) CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            best[s] = std::min(best[s], ms);
         }
-        CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        float ms = 0.0f;
-        if (steps > 2) CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        if (ms < best) {
-            best = ms;
-            best_s = s;
-        }
-    }
-    ctx->plan.stages = best_s;
+    ctx->plan.stages = best[2] < best[1] ? 2 : 1;
     return SFD_OK;
 }
 
@@ -571,6 +630,8 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (!obs) return set_err(ctx, SFD_ERR_ARG, "observed records are required");
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "the gradient is implemented for the acoustic scheme");
     if (grad_invq) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = grad_alloc(ctx))) return rc;
@@ -701,6 +762,17 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
     if (g->scheme == SFD_ACOUSTIC_2D && !acoustic2d_plan(R, &c->plan))
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "no kernel for radius %d", R);
+    if (g->scheme == SFD_VISCOAC_2D) {
+        // the rotated staggered grid of QS is 10th order only (a100..a104, QS:9-28)
+        if (g->order != 10) return set_err(ctx, SFD_ERR_UNSUPPORTED, "the viscoacoustic scheme is 10th order");
+        if (!(g->f0 > 0)) return set_err(ctx, SFD_ERR_ARG, "the viscoacoustic scheme needs f0 > 0 (QS:509)");
+        c->plan.radius = 5;
+        c->plan.tx = kTileX;
+        c->plan.tz = kTileZ;
+        c->plan.gz = 8;  // RSG halo 5, rounded for float4 staging
+        c->plan.stages = 1;
+    }
+    if (g->scheme == SFD_ACOUSTIC_3D) return set_err(ctx, SFD_ERR_UNSUPPORTED, "3-D scheme is not built yet");
     *out = c.release();
     return SFD_OK;
 }
@@ -763,7 +835,21 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     } else {
         dfree(ctx->d_den);
     }
-    (void)q;
+    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        // QS:434-551 on the padded grid: averaged density -> buoyancy, Lame and Blanch tau
+        if (q)
+            for (size_t i = 0; i < n; i++)
+                if (!(q[i] > 0.0f) || !std::isfinite(q[i]))
+                    return set_err(ctx, SFD_ERR_ARG, "q[%zu] = %g is not a positive finite quality factor", i,
+                                   (double)q[i]);
+        std::vector<float> rho(n, 2400.0f), busg(n), p1(n), p2(n);
+        if (den) rho.assign(den, den + n);
+        viscoac2d_prepare(ctx->g.nx, nz, vp, rho.data(), q, ctx->g.f0, busg.data(), p1.data(), p2.data(),
+                          &ctx->q_rtau);
+        if ((urc = upload(&ctx->q_busg, busg.data())) || (urc = upload(&ctx->q_p1, p1.data())) ||
+            (urc = upload(&ctx->q_p2, p2.data())))
+            return urc;
+    }
     if (ctx->varden != varden_old || (!ctx->varden && ctx->den_c != den_c_old)) {
         ctx->graph_valid = false;
         ctx->grad_valid = false;
@@ -785,7 +871,8 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
 
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     if (!ctx || nshot <= 0 || !shots) return SFD_ERR_ARG;
-    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d is not implemented", ctx->g.scheme);
     CK(cudaSetDevice(ctx->device));
     const int nxm = ctx->g.nx, nz = ctx->g.nz;
@@ -832,7 +919,7 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     Layout2D L{};
     L.tx = ctx->plan.tx;
     L.tz = ctx->plan.tz;
-    L.gx = 2 * ctx->radius;
+    L.gx = visco ? 8 : 2 * ctx->radius;
     L.gz = ctx->plan.gz;
     L.ntx = (nx_max + L.tx - 1) / L.tx;
     L.ntz = (nz + L.tz - 1) / L.tz;
@@ -897,9 +984,28 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
     CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
-    ctx->state_floats = 6 * (size_t)nshot * L.shot_stride;
+    ctx->state_floats = (visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
-    {
+    if (visco) {
+        // Gaussian source stamps (QS:1340-1444) and the split cosine sponge tables (QS:555-605)
+        std::vector<float> stamps;
+        for (int s = 0; s < nshot; s++) {
+            int box[4];
+            ctx->h_shots[s].stamp_off = (int)stamps.size();
+            viscoac2d_stamp(ctx->h_shots[s].nx, nz, ctx->h_shots[s].sx, ctx->h_shots[s].sz, box, &stamps);
+            ctx->h_shots[s].stamp_x0 = box[0];
+            ctx->h_shots[s].stamp_z0 = box[1];
+            ctx->h_shots[s].stamp_w = box[2];
+            ctx->h_shots[s].stamp_h = box[3];
+        }
+        if ((rc = up(&ctx->d_stamps, stamps))) return rc;
+        CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * nshot, cudaMemcpyHostToDevice));
+        ctx->spg_stride = ctx->g.pml + 1;
+        std::vector<float> tab(8 * (size_t)ctx->spg_stride);
+        viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
+        dfree(ctx->d_spg);
+        if ((rc = up(&ctx->d_spg, tab))) return rc;
+    } else {
         // TMA descriptors of the six field buffers: 3-D (z, column, shot), one box per field
         int bp[2], bvx[2], bvz[2];
         acoustic2d_fma_boxes(ctx->radius, bp, bvx, bvz);
@@ -944,19 +1050,13 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     auto t0 = std::chrono::steady_clock::now();
-    const bool exact = (ctx->g.flags & SFD_EXACT) != 0;
     CK(cudaEventRecord(ctx->evs, ctx->stream));
     if ((rc = prologue(ctx)) != SFD_OK) return rc;
     long long launches = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (int s = 0; s < ctx->nshot; s++) {
-        for (int k = 0; k < ctx->h_shots[s].nt; k++) {
-            Acou2DArgs a = make_args(ctx, k);
-            a.slot_to_shot = ctx->d_ident + s;
-            CK(acoustic2d_launch_step(ctx->plan, a, 1, exact, ctx->varden, ctx->stream));
-            launches++;
-        }
-    }
+    for (int s = 0; s < ctx->nshot; s++)
+        for (int k = 0; k < ctx->h_shots[s].nt; k++)
+            if ((rc = launch_one_step(ctx, k, ctx->d_ident + s, 1, &launches))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     if ((rc = epilogue(ctx, ctx->d_rec_nt)) != SFD_OK) return rc;
     CK(cudaEventRecord(ctx->eve, ctx->stream));
@@ -983,10 +1083,34 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
 int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
     if (!ctx || !out) return SFD_ERR_ARG;
     if (!ctx->have_shots || shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
-    if (field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ)
-        return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
     CK(cudaSetDevice(ctx->device));
     const ShotDev& sd = ctx->h_shots[shot];
+    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        // vx, vz, sigma = (sx + sz) + sr (QS strxx), r = (rx + rz) + rr (QS rxx)
+        const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+        const int nz = ctx->g.nz;
+        auto fetch = [&](int f, float* dst) -> int {
+            const float* base = ctx->d_state + f * fs + (long long)shot * ctx->L.shot_stride +
+                                (long long)ctx->L.gx * ctx->L.pitch + ctx->L.gz;
+            CK(cudaMemcpy2D(dst, sizeof(float) * nz, base, sizeof(float) * ctx->L.pitch, sizeof(float) * nz, sd.nx,
+                            cudaMemcpyDeviceToHost));
+            return SFD_OK;
+        };
+        const size_t n = (size_t)sd.nx * nz;
+        int rc2;
+        if (field == SFD_FIELD_VX) return fetch(0, out);
+        if (field == SFD_FIELD_VZ) return fetch(1, out);
+        if (field != SFD_FIELD_P && field != SFD_FIELD_R)
+            return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+        std::vector<float> a(n), b(n), c(n);
+        const int f0 = field == SFD_FIELD_P ? 2 : 5;
+        if ((rc2 = fetch(f0, a.data())) || (rc2 = fetch(f0 + 1, b.data())) || (rc2 = fetch(f0 + 2, c.data())))
+            return rc2;
+        for (size_t i = 0; i < n; i++) out[i] = (a[i] + b[i]) + c[i];
+        return SFD_OK;
+    }
+    if (field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
     const int buf = sd.nt & 1;  // state after nt steps lives in buffer nt % 2
     const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
     const int fidx = field == SFD_FIELD_P ? 0 : (field == SFD_FIELD_VX ? 2 : 4);

@@ -29,6 +29,9 @@ struct ShotDev {
     int wav_off;          // offset of this shot's wavelet
     int tile_rec_base;    // offset of this shot's per-tile receiver CSR (ntiles + 1 entries)
     float inj_scale;      // ((dt * den_src) * vp_src), float, AFD:250 order
+    // viscoacoustic scheme: Gaussian source stamp (QS:1340-1444), box of non-zero weights
+    int stamp_off;        // offset of the box's weights (x-major, z fastest) in the stamp array
+    int stamp_x0, stamp_z0, stamp_w, stamp_h;
 };
 
 // Field storage of one 2-D scheme: per shot a (cols x pitch) slab, z fastest, with zero ghost
@@ -41,6 +44,42 @@ struct Layout2D {
     int ntx, ntz;      // tiles per shot along x and z
     int tx, tz;        // tile shape
 };
+
+// Arguments of the viscoacoustic kernels (viscoac2d.cu): in-place fields, no ping-pong.
+struct QArgs {
+    float* vx; float* vz;                 // QS vxx (= vx), vzz (= vz) for vs = 0
+    float* sx; float* sz; float* sr;      // QS strxxx, strxxz, strxxr (= strzz parts for vs = 0)
+    float* rx; float* rz; float* rr;      // QS rxxx, rxxz, rxxr
+    Layout2D L;
+    int nz, npx, npz;                     // grid depth, pad cells (QS npxn = npxp, npzn = npzp)
+    const float* busg;                    // 1/averaged density (QS:434-469)
+    const float* p1;                      // lambmu * taupstinss (QS:473-551)
+    const float* p2;                      // lambmu * (taupstinss - 1)
+    int mpitch, nx_model;
+    float dt, f_mem;                      // f_mem = dt * (-1 * rtaustss)
+    float hx, hz;                         // 0.5/dx, 0.5/dz
+    float dz2;                            // dz*dz
+    float a[5];                           // a100..a104
+    const float* spg;                     // sponge tables: xn, xp, zn, zp, 1xn, 2xp, 1zn, 2zp
+    int spg_stride;
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* wavelets;
+    const float* stamps;
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr; const int* tile_rec_idx;
+    float* records;                       // [nt][nrec] per shot: strzz (= strxx) at the receivers
+    int step;
+};
+cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
+// host preparation, QS:434-551: busg, p1, p2 on the padded grid and rtaustss
+void viscoac2d_prepare(int nx, int nz, const float* vp, const float* rho, const float* q, float f0, float* busg,
+                       float* p1, float* p2, float* rtau);
+// QS:555-605 cosine sponge tables (8 arrays of stride npx+1 / npz+1 packed with `stride`)
+void viscoac2d_sponge_tables(int npx, int npz, float dx, float dz, int stride, float* out);
+// QS:1398-1444 normalised Gaussian over an n1 x n2 grid, non-zero box around the source:
+// returns the box (x0, z0, w, h) and appends its weights (x-major) to `out`
+void viscoac2d_stamp(int nx, int nz, int sx, int sz, int* box, std::vector<float>* out);
 
 // Arguments of the acoustic 2-D step kernels (passed by value; pointers are device memory).
 struct Acou2DArgs {

@@ -109,6 +109,26 @@ def config2(nshot: int = 64, nt: int = 4000) -> AcousticCase:
                         sx, [PML + 2] * nshot, PML + 2, 30.0)
 
 
+def config4(nshot: int = 32, nt: int = 3000):
+    """2-D acoustic adjoint gradient: 384 (z) x 1536 (x), dx = dz = 10 m, dt = 1 ms, nt = 3000,
+    32 shots on interior z = 2, receivers every x on z = 2, 25 Hz Ricker.  Returns
+    (start case, true vp): the true model is layered plus 3 Gaussian anomalies, the starting
+    model its Gaussian smoothing with sigma = 15 cells.  The checkpoint interval of the
+    gradient is 55 steps."""
+    from scipy.ndimage import gaussian_filter
+    NX, NZ, PML = 1536, 384, 50
+    true = np.clip(layered_model(NX, NZ, 10, 1500.0, 4000.0, seed=20261204, anomalies=3, radius=30.0, amp=350.0,
+                                 dx=10.0), 1400.0, 4300.0)
+    start = gaussian_filter(true.astype(np.float64), sigma=15.0, mode="nearest").astype(np.float32)
+    vp_true = pad_edges(true, PML, PML)
+    vp0 = pad_edges(start, PML, PML)
+    den = np.full_like(vp0, 2200.0)
+    sx = [PML + int(round((i + 0.5) * NX / nshot)) for i in range(nshot)]
+    case = AcousticCase("config4_gradient_384x1536", NX, NZ, PML, nt, 10.0, 10.0, 1e-3, vp0, den, sx,
+                        [PML + 2] * nshot, PML + 2, 25.0, extra={"checkpoint_interval": 55})
+    return case, vp_true
+
+
 def small_varden(seed: int = 7) -> AcousticCase:
     """Non-square, variable-density case used to pin the restatement against the reference
     build: 80 (x) x 60 (z) interior, 15-cell sponge, 300 steps, off-centre source."""

@@ -1,0 +1,100 @@
+"""GPU viscoacoustic path (SFD_VISCOAC_2D, the vs = 0 reduction of forward/Q_forward) through
+the C ABI, against the FP32 restatement of the Fortran code (oracle/q_oracle.cpp).  The GPU
+kernels keep the reference's operation order, so records must be bit-identical to the
+restatement; the FP64 restatement gives the reported precision error."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from conftest import bits_equal, rel_l2
+from seismic_code_github_b200 import seisfd as S
+
+pytestmark = pytest.mark.gpu
+
+
+def qmodel(nx=70, nz=56, seed=0, qlo=20.0, qhi=200.0, lens=True):
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz)
+    x = np.arange(nx)
+    vp = np.tile(np.where(z < nz // 2, 2000.0, 3000.0), (nx, 1)).astype(np.float32)
+    vp += (30.0 * rng.standard_normal((nx, nz))).astype(np.float32)
+    rho = (2000.0 + 200.0 * rng.random((nx, nz))).astype(np.float32)
+    q = qlo + (qhi - qlo) * rng.random((nx, nz))
+    if lens:
+        q = np.where((x[:, None] - nx / 2) ** 2 + (z[None, :] - nz / 2) ** 2 < (nz / 5) ** 2, qlo, q)
+    return vp, rho, q.astype(np.float32)
+
+
+def run_gpu(vp, rho, q, npx, f0, dt, dx, shots_spec, flags=0):
+    """shots_spec: list of (isxe, isze, nt_total, nrz0); interior model arrays (nx, nz)."""
+    vpp, rhop, qp = (S.pad_model(a, npx, npx, npx, npx) for a in (vp, rho, q))
+    nx, nz = vpp.shape
+    e = S.Engine(S.VISCOAC_2D, nx, nz, dx, dx, dt, npx, order=10, f0=f0, flags=flags)
+    e.set_model(vpp, rhop, qp)
+    shots = []
+    for isxe, isze, ntot, nrz0 in shots_spec:
+        rx = np.arange(npx, nx - npx, dtype=np.int32)
+        rz = np.full_like(rx, npx + nrz0)
+        w = S.wavelet(S.WAVELET_Q, ntot, dt, f0)
+        shots.append(S.ShotSpec(isxe - 1, isze - 1, rx, rz, w))
+    e.set_shots(shots)
+    recs = e.split_records(e.forward())
+    t = e.timing()
+    e.close()
+    return recs, t
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_single_shot_bitexact_against_restatement(seed):
+    vp, rho, q = qmodel(seed=seed)
+    npx, f0, dt, dx, nt = 11, 20.0, 5e-4, 10.0, 160
+    decay = ol.q_decay(f0, dt)
+    isxe, isze, nrz0 = npx + 25, npx + 4, 1
+    recs, t = run_gpu(vp, rho, q, npx, f0, dt, dx, [(isxe, isze, nt + decay, nrz0)])
+    r1, r2, _ = ol.q_forward(vp, vp * 0, rho, q, q, dx, dx, dt, f0, nt, npx, npx, isxe, isze, nrz0=nrz0)
+    r64, _, _ = ol.q_forward(vp, vp * 0, rho, q, q, dx, dx, dt, f0, nt, npx, npx, isxe, isze, nrz0=nrz0, fp64=True)
+    got = recs[0][:, decay:]
+    print(f"seed {seed}: GPU vs FP32 restatement relL2 {rel_l2(got, r1):.2e}; vs FP64 {rel_l2(got, r64):.2e}; "
+          f"{t['launches']} launches {t['loop_ms']:.2f} ms")
+    assert np.abs(got).max() > 0
+    assert bits_equal(got, r1)
+    assert bits_equal(r1, r2)  # strzz == strxx in the acoustic reduction
+
+
+def test_batched_uneven_shots_and_q_override():
+    vp, rho, q = qmodel(seed=3, nx=80, nz=50)
+    npx, f0, dt, dx = 10, 25.0, 5e-4, 10.0
+    decay = ol.q_decay(f0, dt)
+    spec = [(npx + 12, npx + 3, 150, 1), (npx + 60, npx + 8, 90, 2), (npx + 40, npx + 20, 120, 1)]
+    recs, _ = run_gpu(vp, rho, q, npx, f0, dt, dx, [(a, b, n + decay, c) for a, b, n, c in spec])
+    for (isxe, isze, nt, nrz0), got in zip(spec, recs):
+        ref, _, _ = ol.q_forward(vp, vp * 0, rho, q, q, dx, dx, dt, f0, nt, npx, npx, isxe, isze, nrz0=nrz0)
+        assert bits_equal(got[:, decay:], ref), (isxe, isze, nt)
+
+
+def test_attenuation_on_gpu():
+    vp, rho, _ = qmodel(seed=4, lens=False)
+    npx, f0, dt, dx, nt = 11, 20.0, 5e-4, 10.0, 300
+    decay = ol.q_decay(f0, dt)
+    energies = []
+    for qv in (1e5, 60.0, 15.0):
+        q = np.full_like(vp, qv)
+        recs, _ = run_gpu(vp, rho, q, npx, f0, dt, dx, [(npx + 30, npx + 4, nt + decay, 1)])
+        energies.append(float(np.sum(recs[0][:, decay:].astype(np.float64) ** 2)))
+    assert energies[0] > energies[1] > energies[2]
+
+
+def test_wavefield_readback():
+    vp, rho, q = qmodel(seed=5, nx=40, nz=40)
+    npx, f0, dt, dx = 8, 20.0, 5e-4, 10.0
+    vpp, rhop, qp = (S.pad_model(a, npx, npx, npx, npx) for a in (vp, rho, q))
+    with S.Engine(S.VISCOAC_2D, vpp.shape[0], vpp.shape[1], dx, dx, dt, npx, order=10, f0=f0) as e:
+        e.set_model(vpp, rhop, qp)
+        rx = np.array([20], np.int32)
+        e.set_shots([S.ShotSpec(25, 12, rx, rx, S.wavelet(S.WAVELET_Q, 150, dt, f0))])
+        rec = e.forward()
+        p = e.wavefield(0, S.FIELD_P)
+        r = e.wavefield(0, S.FIELD_R)
+        vx = e.wavefield(0, S.FIELD_VX)
+    assert np.isfinite(p).all() and np.abs(p).max() > 0 and np.abs(r).max() > 0 and np.abs(vx).max() > 0
+    assert p[20, 20] == rec[-1]
