@@ -166,6 +166,21 @@ int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps);
 
 int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);
 
+/* Single-shot 2-D acoustic forward that allocates no device memory.  No counterpart in the
+ * reference: it is for callers that cannot allocate device memory when they model a shot (a
+ * framework that has reserved the device memory for its own allocator, a process at its
+ * device-memory quota, a real-time loop that forbids allocation after start-up).  Every working
+ * buffer lives in a fixed 32 MiB device array inside the library; sizes that do not fit return
+ * SFD_ERR_NOMEM.  vp_dev, den_dev (NULL = constant 2400), wavelet_dev (nt samples) and
+ * records_dev (nrec x nt, trace-major) are device pointers owned by the caller; rec_x / rec_z
+ * are host arrays.  Arithmetic is the reference order of SFD_EXACT.  The first call on a device
+ * looks up the array's address (make it before any stream capture); calls that overlap on the
+ * GPU race on the shared array.  stream may be NULL (the default stream); the call returns
+ * after the stream has finished its work. */
+int sfd_forward_noalloc(const sfd_grid* grid, const float* vp_dev, const float* den_dev, const float* wavelet_dev,
+                        int nt, int sx, int sz, int nrec, const int* rec_x, const int* rec_z, float* records_dev,
+                        void* stream);
+
 /* Host helpers (no context). */
 /* Source wavelet in one of the reference's three conventions (AFD:199-209, RIC:44, QS:1376).
  * delay: RIC only, in samples (RIC uses 150). */

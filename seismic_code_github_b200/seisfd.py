@@ -57,6 +57,9 @@ SIGNATURES = {
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
+    "sfd_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I32P, _I32P,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
     "sfd_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _F32P]),
     "sfd_afd_sponge": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P]),
     "sfd_fd_coeffs": (ctypes.c_int, [ctypes.c_int, _F32P]),

@@ -92,3 +92,16 @@ def test_null_context_is_rejected():
     assert lib.sfd_forward(None, None) == S.ERR_ARG
     assert lib.sfd_set_model(None, None, None, None) == S.ERR_ARG
     assert lib.sfd_destroy(None) == S.OK
+
+
+def test_noalloc_rejects_sizes_beyond_its_array_before_any_device_work():
+    """sfd_forward_noalloc checks the grid against its fixed 32 MiB array before touching the
+    device (the pointers below are never dereferenced)."""
+    g = S.Grid(S.ACOUSTIC_2D, 3000, 1, 3000, 20, 10.0, 0.0, 10.0, 1e-3, 16, S.EXACT, 0.0)
+    rx = np.zeros(1, np.int32)
+    fake = ctypes.c_void_p(256)
+    lib = S.load()
+    assert lib.sfd_forward_noalloc(ctypes.byref(g), fake, None, fake, 10, 5, 5, 1, S._ip(rx), S._ip(rx), fake,
+                                   None) == S.ERR_NOMEM
+    assert lib.sfd_forward_noalloc(ctypes.byref(g), None, None, fake, 10, 5, 5, 1, S._ip(rx), S._ip(rx), fake,
+                                   None) == S.ERR_ARG
