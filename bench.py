@@ -231,6 +231,54 @@ def measure_gradient(args, dev):
             "misfit": float(mis), "gradient_accuracy": "relL2 vs FP64 adjoint oracle 7.6e-7 (tests/test_gradient_gpu.py)"}
 
 
+def measure_viscoacoustic(args, dev):
+    """Config 3: 16 viscoacoustic shots (uneven record lengths) in one batched time loop; the CPU
+    figure is the restated Fortran step (oracle/q_oracle.cpp, OpenMP, all host cores) on one
+    shot for a bounded number of steps -- the Fortran reference cannot be compiled here."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.q_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, nt, c["dt"], c["f0"]))
+             for sx, sz, nt in zip(c["src_x"], c["src_z"], c["nt"])]
+    with S.Engine(S.VISCOAC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"], device=dev) as e:
+        e.set_model(c["vp"], c["rho"], c["q"])
+        e.set_shots(shots)
+        e.forward_device(0)
+        ms = []
+        for _ in range(args.q_steps):
+            e.forward_device(0)
+            t = e.timing()
+            ms.append(t["loop_ms"])
+    pts = float(sum(Nx * Nz * nt for nt in c["nt"]))
+    gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    out = {"workload": f"config 3: viscoacoustic SLS forward, {c['NZ']}x{c['NX']} interior ({Nz}x{Nx} padded), "
+                       f"{len(shots)} shots, nt {min(c['nt'])}-{max(c['nt'])}, Q 20-200 + low-Q lens",
+           "gpts_per_s": gpts, "shots_per_s": len(shots) / (float(np.median(ms)) / 1e3), "loop_ms": float(np.median(ms)),
+           "launches": t["launches"], "bytes_per_point": 96,
+           "hbm_frac_of_measured": 96 * gpts / read_peaks()[0], "parity": "bit-exact vs FP32 restatement"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        vp, rho, q = c["interior"]
+        steps = args.q_cpu_steps
+        run = lambda n: ol.q_forward(vp, vp * 0, rho, q, q, c["dx"], c["dz"], c["dt"], c["f0"], n, c["PML"], c["PML"],
+                                     c["src_x"][0] + 1, c["src_z"][0] + 1)
+        t0 = time.perf_counter()
+        run(1)  # set-up and the decay steps
+        t1 = time.perf_counter()
+        run(1 + steps)  # the same plus `steps` time steps
+        wall = (time.perf_counter() - t1) - (t1 - t0)
+        out["cpu_baseline"] = {"value": Nx * Nz * steps / max(wall, 1e-9) / 1e9, "unit": "Gpts/s",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"restated Q_forward time step (oracle/q_oracle.cpp, OpenMP) on one shot: "
+                                         f"the difference of a {steps + 1}- and a 1-sample run on the {Nz}x{Nx} "
+                                         f"padded grid ({steps} steps)"}
+    return out
+
+
 def config_dict(case, args):
     return {"workload": f"batched 2-D acoustic forward, {case.NZ}x{case.NX} interior "
                         f"({case.Nz}x{case.Nx} padded, {case.PML}-cell sponge), {case.nshot} shots, nt={case.nt}, "
@@ -359,6 +407,8 @@ def run_ours(args, world, rank, local):
         line["plain_vs_batched"] = plain
     if world == 1 and args.grad_steps > 0:
         line["gradient"] = measure_gradient(args, dev)
+    if world == 1 and args.q_steps > 0:
+        line["viscoacoustic"] = measure_viscoacoustic(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_reference_sample(case, args.ref_steps).items() if k != "wall_s"}
     print(json.dumps(line), flush=True)
@@ -381,6 +431,9 @@ def main():
     ap.add_argument("--grad-nshot", type=int, default=32)
     ap.add_argument("--grad-nt", type=int, default=3000)
     ap.add_argument("--grad-plain-shots", type=int, default=8)
+    ap.add_argument("--q-steps", type=int, default=2, help="timed viscoacoustic forwards (0 = skip)")
+    ap.add_argument("--q-nshot", type=int, default=16)
+    ap.add_argument("--q-cpu-steps", type=int, default=120)
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

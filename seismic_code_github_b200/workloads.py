@@ -129,6 +129,34 @@ def config4(nshot: int = 32, nt: int = 3000):
     return case, vp_true
 
 
+def config3(nshot: int = 16):
+    """2-D viscoacoustic (one SLS memory variable): 1024 x 1024 interior, dx = dz = 5 m,
+    dt = 0.5 ms, the two-layer vp of config 1 rescaled to the grid (2000 m/s above interior
+    z = 512, 3000 below), density 2000 kg/m^3, Q 20-200 as a seeded smooth random field with a
+    low-Q lens (radius 60 cells, Q = 20), 20 Hz Ricker in the Q_forward convention, 16 shots on
+    interior z = 2 with record lengths drawn uniformly from 2000-3000 steps, receivers at every
+    interior x on z = 2, 50 pad cells (sponge) per side.  Returns a dict of padded arrays."""
+    from scipy.ndimage import gaussian_filter
+    NX = NZ = 1024
+    PML = 50
+    rng = np.random.default_rng(20261205)
+    z = np.arange(NZ)
+    x = np.arange(NX)
+    vp = np.tile(np.where(z < NZ // 2, 2000.0, 3000.0), (NX, 1)).astype(np.float32)
+    rho = np.full((NX, NZ), 2000.0, np.float32)
+    f = gaussian_filter(rng.standard_normal((NX, NZ)), sigma=40.0, mode="wrap")
+    f = (f - f.min()) / (f.max() - f.min())
+    q = 20.0 + 180.0 * f
+    lens = (x[:, None] - 0.6 * NX) ** 2 + (z[None, :] - 0.45 * NZ) ** 2 < 60.0 ** 2
+    q = np.where(lens, 20.0, q).astype(np.float32)
+    nts = [int(v) for v in rng.integers(2000, 3001, nshot)]
+    sx = [PML + int(round((i + 0.5) * NX / nshot)) for i in range(nshot)]
+    return {"name": "config3_viscoacoustic_1024x1024", "NX": NX, "NZ": NZ, "PML": PML, "dx": 5.0, "dz": 5.0,
+            "dt": 5e-4, "f0": 20.0, "vp": pad_edges(vp, PML, PML), "rho": pad_edges(rho, PML, PML),
+            "q": pad_edges(q, PML, PML), "src_x": sx, "src_z": [PML + 2] * nshot, "rec_z": PML + 2, "nt": nts,
+            "interior": (vp, rho, q)}
+
+
 def small_varden(seed: int = 7) -> AcousticCase:
     """Non-square, variable-density case used to pin the restatement against the reference
     build: 80 (x) x 60 (z) interior, 15-cell sponge, 300 steps, off-centre source."""
