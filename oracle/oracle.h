@@ -47,6 +47,23 @@ int oracle_q_f32(const OracleQCfg* c, const float* vp, const float* vs, const fl
                  const float* qs, float* rec1, float* rec2, float* final_sxx);
 int oracle_q_f64(const OracleQCfg* c, const float* vp, const float* vs, const float* rho, const float* qp,
                  const float* qs, double* rec1, double* rec2, double* final_sxx);
+// 3-D velocity-pressure staggered grid (the AFD scheme with a y axis; no reference counterpart).
+// Arrays are [x][y][z], z fastest; record[r*nt + k] = P after step k's sponge at receiver r.
+typedef struct {
+    int nx, ny, nz, pml, nt, radius;
+    float dx, dy, dz, dt;
+    int sx, sy, sz;
+    int nrec;
+    const int* rec_x;
+    const int* rec_y;
+    const int* rec_z;
+    float den_c;     // density where den is NULL
+} OracleAfd3Cfg;
+int oracle_afd3d_sponge(int nx, int ny, int nz, int pml, float* absorb);
+int oracle_afd3d_f32(const OracleAfd3Cfg* g, const float* vp, const float* den, const float* wavelet, float* record,
+                     float* final_p);
+int oracle_afd3d_f64(const OracleAfd3Cfg* g, const float* vp, const float* den, const float* wavelet, double* record,
+                     double* final_p);
 void oracle_wavelet_afd(int nt, float dt, float freq, float* out);
 void oracle_wavelet_ric(int nt, float dt, int f0, int delay, float* out);
 

@@ -174,3 +174,47 @@ def q_forward(vp, vs, rho, qp, qs, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz
     if rc != 0:
         raise ValueError(f"oracle_q rejected the configuration (rc={rc})")
     return r1, r2, fin
+
+
+class OracleAfd3Cfg(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("pml", ctypes.c_int),
+                ("nt", ctypes.c_int), ("radius", ctypes.c_int), ("dx", ctypes.c_float), ("dy", ctypes.c_float),
+                ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("sx", ctypes.c_int), ("sy", ctypes.c_int),
+                ("sz", ctypes.c_int), ("nrec", ctypes.c_int), ("rec_x", _I32P), ("rec_y", _I32P),
+                ("rec_z", _I32P), ("den_c", ctypes.c_float)]
+
+
+def afd3d_sponge(nx: int, ny: int, nz: int, pml: int) -> np.ndarray:
+    a = np.empty((nx, ny, nz), np.float32)
+    if lib().oracle_afd3d_sponge(nx, ny, nz, pml, _p(a)) != 0:
+        raise ValueError("bad sponge size")
+    return a
+
+
+def afd3d_forward(vp, den, wavelet, src, rec_x, rec_y, rec_z, pml, dx, dy, dz, dt, radius=4, fp64=True,
+                  den_c=2400.0, want_final=False):
+    """Restated 3-D scheme (oracle/afd3d_oracle.cpp) for one shot on the padded (nx, ny, nz) grid.
+    Returns records [nrec][nt] (float64 or float32) and the final P (or None)."""
+    L = lib()
+    if not hasattr(L, "_a3_sig"):
+        tp = ctypes.POINTER(OracleAfd3Cfg)
+        L.oracle_afd3d_f32.argtypes = [tp, _F32P, _F32P, _F32P, _F32P, _F32P]
+        L.oracle_afd3d_f64.argtypes = [tp, _F32P, _F32P, _F32P, _F64P, _F64P]
+        L._a3_sig = True
+    vp = np.ascontiguousarray(vp, np.float32)
+    nx, ny, nz = vp.shape
+    den = None if den is None else np.ascontiguousarray(den, np.float32)
+    w = np.ascontiguousarray(wavelet, np.float32)
+    rx, ry, rz = (np.ascontiguousarray(a, np.int32) for a in (rec_x, rec_y, rec_z))
+    cfg = OracleAfd3Cfg(nx, ny, nz, pml, len(w), radius, dx, dy, dz, dt, src[0], src[1], src[2], len(rx),
+                        rx.ctypes.data_as(_I32P), ry.ctypes.data_as(_I32P), rz.ctypes.data_as(_I32P), den_c)
+    dt_ = np.float64 if fp64 else np.float32
+    tp = _F64P if fp64 else _F32P
+    rec = np.zeros((len(rx), len(w)), dt_)
+    fin = np.zeros((nx, ny, nz), dt_) if want_final else None
+    fn = L.oracle_afd3d_f64 if fp64 else L.oracle_afd3d_f32
+    rc = fn(ctypes.byref(cfg), _p(vp), None if den is None else _p(den), _p(w), _p(rec, tp),
+            None if fin is None else _p(fin, tp))
+    if rc != 0:
+        raise ValueError("oracle_afd3d rejected the configuration")
+    return rec, fin

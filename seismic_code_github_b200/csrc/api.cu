@@ -73,6 +73,13 @@ struct sfd_ctx {
     int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
     CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
 
+    // 3-D scheme: dense [x][y][pitch] slabs, 8 fields (P, Vx, Vy, Vz, two buffers each)
+    Layout3D L3{};
+    CUtensorMap tmaps3[6];     // TMA descriptors: P0 P1 VY0 VY1 VZ0 VZ1
+    std::vector<int> h_rec_y;
+    int* d_rec_y = nullptr;
+    int nrec_max = 0;
+
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
@@ -165,9 +172,35 @@ int encode_field_map(sfd_ctx* ctx, CUtensorMap* m, float* base, const Layout2D& 
     return SFD_OK;
 }
 
+// 4-D float32 tensor map over one 3-D field buffer: dims (nz, ny, nx, nshot) with the exact grid
+// extents (boxes read zeros outside the grid), box (z, y, 1, 1).
+int encode_field_map3(sfd_ctx* ctx, CUtensorMap* m, float* base, const Layout3D& L, int nshot, const int box[2]) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return set_err(ctx, SFD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[4] = {(cuuint64_t)L.nz, (cuuint64_t)L.ny, (cuuint64_t)L.nx, (cuuint64_t)nshot};
+    const cuuint64_t strides[3] = {(cuuint64_t)L.pitch * 4, (cuuint64_t)L.xstride * 4, (cuuint64_t)L.shot_stride * 4};
+    const cuuint32_t bdim[4] = {(cuuint32_t)box[0], (cuuint32_t)box[1], 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, bdim, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(ctx, SFD_ERR_CUDA, "cuTensorMapEncodeTiled (4-D) failed (%d)", (int)r);
+    return SFD_OK;
+}
+
+// Sponge factor of the 3-D scheme at one cell: the AFD taper (AFD:164-194) of the x pad, else of
+// the y pad, else of the z pad, else 1.
+float sponge3(const sfd_grid& g, int x, int y, int z) {
+    auto q = [&](int d, int n) { return d < g.pml ? g.pml - d - 1 : (d >= n - g.pml ? d - n + g.pml : -1); };
+    int k = q(x, g.nx);
+    if (k < 0) k = q(y, g.ny);
+    if (k < 0) k = q(z, g.nz);
+    return k < 0 ? 1.0f : (float)(-0.38 * k * k / (1.0 * g.pml * g.pml) + 1);
+}
+
 void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
-    dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri);
+    dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri); dfree(c->d_rec_y);
     dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
@@ -254,6 +287,34 @@ int active_shots(const sfd_ctx* c, int step) {
     return n;
 }
 
+// Arguments of the 3-D step: buffers alternate each step like the 2-D ones.
+Acou3DArgs make_args3(const sfd_ctx* c, int step) {
+    Acou3DArgs a{};
+    const long long fs = (long long)c->nshot * c->L3.shot_stride;
+    const int i = step & 1, o = (step + 1) & 1;
+    float* F = c->d_state;
+    a.p_in = F + i * fs; a.p_out = F + o * fs;
+    a.vx_in = F + (2 + i) * fs; a.vx_out = F + (2 + o) * fs;
+    a.vy_out = F + (4 + o) * fs;
+    a.vz_out = F + (6 + o) * fs;
+    a.tm_p = c->tmaps3[i];
+    a.tm_vy = c->tmaps3[2 + i];
+    a.tm_vz = c->tmaps3[4 + i];
+    a.err_flag = c->d_err;
+    a.L = c->L3;
+    a.vp = c->d_vp;
+    a.den = c->varden ? c->d_den : nullptr;
+    a.den_c = c->den_c;
+    a.dt = c->g.dt;
+    a.rdx = 1.0f / c->g.dx; a.rdy = 1.0f / c->g.dy; a.rdz = 1.0f / c->g.dz;
+    a.dtdx = c->g.dt / c->g.dx; a.dtdy = c->g.dt / c->g.dy; a.dtdz = c->g.dt / c->g.dz;
+    for (int m = 0; m < c->radius; m++) a.coef[m] = c->coef[m];
+    a.pml = c->g.pml;
+    for (int q = 0; q < c->g.pml && q < 256; q++) a.sponge[q] = -0.38 * q * q / (1.0 * c->g.pml * c->g.pml) + 1;
+    a.slot_to_shot = c->d_slot;
+    return a;
+}
+
 // Arguments of the viscoacoustic step (fields in place, eight slabs per shot).
 QArgs make_qargs(const sfd_ctx* c, int step) {
     QArgs a{};
@@ -293,6 +354,17 @@ QArgs make_qargs(const sfd_ctx* c, int step) {
 }
 
 int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* launches) {
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D) {
+        Acou3DArgs a = make_args3(ctx, k);
+        a.slot_to_shot = slots;
+        float* p_in = const_cast<float*>(a.p_in);
+        CK(acoustic3d_launch_inject(p_in, ctx->L3, ctx->d_shots, slots, act, ctx->d_wav, k, ctx->stream));
+        CK(acoustic3d_launch_step(ctx->radius, a, act, ctx->varden, ctx->stream));
+        CK(acoustic3d_launch_gather(a.p_out, ctx->L3, ctx->d_shots, slots, act, ctx->d_rec_x, ctx->d_rec_y,
+                                    ctx->d_rec_z, ctx->d_rec_tn, ctx->nrec_max, k, ctx->stream));
+        *launches += 2 + (ctx->nrec_max > 0 ? 1 : 0);
+        return SFD_OK;
+    }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
         QArgs q = make_qargs(ctx, k);
         q.slot_to_shot = slots;
@@ -312,7 +384,8 @@ int prologue(sfd_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_rec_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
-    if (ctx->g.scheme == SFD_VISCOAC_2D) return SFD_OK;  // its source is added inside every step
+    // the viscoacoustic source is added inside every step, the 3-D one by its own launch
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D) return SFD_OK;
     Acou2DArgs a = make_args(ctx, -1);  // step -1 writes into buffer 0
     CK(acoustic2d_launch_inject0(a, ctx->nshot, (ctx->g.flags & SFD_EXACT) != 0, ctx->stream));
     return SFD_OK;
@@ -329,9 +402,7 @@ int enqueue_loop(sfd_ctx* ctx, long long* launches) {
 }
 
 int epilogue(sfd_ctx* ctx, float* out_dev) {
-    int nrec_max = 0;
-    for (const auto& s : ctx->h_shots) nrec_max = std::max(nrec_max, s.nrec);
-    CK(launch_records_transpose(ctx->d_rec_tn, out_dev, ctx->d_shots, ctx->nshot, nrec_max, ctx->nt_max,
+    CK(launch_records_transpose(ctx->d_rec_tn, out_dev, ctx->d_shots, ctx->nshot, ctx->nrec_max, ctx->nt_max,
                                 ctx->stream));
     if (ctx->g.flags & SFD_NAN_CHECK) {
         CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
@@ -344,8 +415,6 @@ int check_ready(sfd_ctx* ctx) {
     if (!ctx) return SFD_ERR_ARG;
     if (!ctx->have_model) return set_err(ctx, SFD_ERR_STATE, "sfd_set_model has not been called");
     if (!ctx->have_shots) return set_err(ctx, SFD_ERR_STATE, "sfd_set_shots has not been called");
-    if (ctx->g.scheme != SFD_ACOUSTIC_2D && ctx->g.scheme != SFD_VISCOAC_2D)
-        return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d forward is not implemented", ctx->g.scheme);
     CK(cudaSetDevice(ctx->device));
     return SFD_OK;
 }
@@ -396,6 +465,12 @@ int tune_schedule(sfd_ctx* ctx) {
     return SFD_OK;
 }
 
+int kernel_variant(const sfd_ctx* ctx) {
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return 40;
+    return (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
+}
+
 int run_forward(sfd_ctx* ctx, float* out_dev) {
     int rc;
     long long launches = 0;
@@ -433,9 +508,9 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
     ctx->timing.device_ms = dms;
     ctx->timing.launches = launches + 2 + ((ctx->g.flags & SFD_NAN_CHECK) ? 1 : 0);
     ctx->timing.graph = 1;
-    ctx->timing.kernel_variant = (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
+    ctx->timing.kernel_variant = kernel_variant(ctx);
     double pts = 0;
-    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.ny * ctx->g.nz * s.nt;
     ctx->timing.point_updates = pts;
     return finish_nan(ctx);
 }
@@ -704,6 +779,117 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     return SFD_OK;
 }
 
+// sfd_set_shots for the 3-D scheme: every shot covers the whole grid (no aperture windows);
+// sources must lie where the step updates P (R <= coordinate < n - R on every axis).
+int set_shots_3d(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
+    CK(cudaSetDevice(ctx->device));
+    const sfd_grid& g = ctx->g;
+    const int R = ctx->radius;
+    std::vector<ShotDev> hs(nshot);
+    std::vector<int> rx, ry, rz;
+    std::vector<float> wav;
+    std::vector<long long> out_off(nshot);
+    long long rec_total = 0;
+    int nt_max = 0, nrec_max = 0;
+    for (int s = 0; s < nshot; s++) {
+        const sfd_shot& sh = shots[s];
+        if (sh.ap_x0 != 0 || (sh.ap_nx != 0 && sh.ap_nx != g.nx))
+            return set_err(ctx, SFD_ERR_UNSUPPORTED, "shot %d: aperture windows are 2-D only", s);
+        if (sh.nt < 1 || !sh.wavelet) return set_err(ctx, SFD_ERR_ARG, "shot %d: nt=%d or wavelet missing", s, sh.nt);
+        if (sh.sx < R || sh.sx >= g.nx - R || sh.sy < R || sh.sy >= g.ny - R || sh.sz < R || sh.sz >= g.nz - R)
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: source (%d, %d, %d) outside the updated region", s, sh.sx,
+                           sh.sy, sh.sz);
+        if (sh.nrec < 0 || (sh.nrec > 0 && (!sh.rec_x || !sh.rec_y || !sh.rec_z)))
+            return set_err(ctx, SFD_ERR_ARG, "shot %d: receiver list missing (3-D needs rec_y)", s);
+        ShotDev d{};
+        d.nx = g.nx; d.x0 = 0; d.nt = sh.nt; d.sx = sh.sx; d.sy = sh.sy; d.sz = sh.sz;
+        d.nrec = sh.nrec;
+        d.rec_base = rec_total;
+        d.rec_list = (int)rx.size();
+        d.wav_off = (int)wav.size();
+        for (int r = 0; r < sh.nrec; r++) {
+            if (sh.rec_x[r] < 0 || sh.rec_x[r] >= g.nx || sh.rec_y[r] < 0 || sh.rec_y[r] >= g.ny || sh.rec_z[r] < 0 ||
+                sh.rec_z[r] >= g.nz)
+                return set_err(ctx, SFD_ERR_ARG, "shot %d: receiver %d outside the grid", s, r);
+            rx.push_back(sh.rec_x[r]);
+            ry.push_back(sh.rec_y[r]);
+            rz.push_back(sh.rec_z[r]);
+        }
+        wav.insert(wav.end(), sh.wavelet, sh.wavelet + sh.nt);
+        out_off[s] = rec_total;
+        rec_total += (long long)sh.nrec * sh.nt;
+        nt_max = std::max(nt_max, sh.nt);
+        nrec_max = std::max(nrec_max, sh.nrec);
+        if (ctx->have_model) {
+            const size_t mi = ((size_t)d.sx * g.ny + d.sy) * g.nz + d.sz;
+            float sc = g.dt * (ctx->varden ? ctx->h_den[mi] : ctx->den_c);
+            sc = sc * ctx->h_vp[mi];
+            d.inj_scale = sc;
+        }
+        hs[s] = d;
+    }
+    free_shot_buffers(ctx);
+    Layout3D L{};
+    L.nx = g.nx; L.ny = g.ny; L.nz = g.nz;
+    L.pitch = round_up(g.nz, 4);
+    L.xstride = (long long)g.ny * L.pitch;
+    L.shot_stride = (long long)g.nx * L.xstride;
+    L.nty = (g.ny + kTile3Y - 1) / kTile3Y;
+    L.ntz = (g.nz + kTile3Z - 1) / kTile3Z;
+    ctx->L3 = L;
+    std::vector<int> order(nshot), ident(nshot);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return hs[a].nt > hs[b].nt; });
+    std::iota(ident.begin(), ident.end(), 0);
+    ctx->h_shots = hs;
+    ctx->h_rec_x = rx;
+    ctx->h_rec_y = ry;
+    ctx->h_rec_z = rz;
+    ctx->h_wav = wav;
+    ctx->rec_out_off = out_off;
+    ctx->rec_total = rec_total;
+    ctx->nshot = nshot;
+    ctx->nt_max = nt_max;
+    ctx->nrec_max = nrec_max;
+    ctx->order = order;
+    auto up = [&](auto** dst, const auto& v) -> int {
+        using E = typename std::remove_reference<decltype(v)>::type::value_type;
+        const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(E);
+        CK(cudaMalloc(dst, bytes));
+        if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice));
+        return SFD_OK;
+    };
+    int rc;
+    if ((rc = up(&ctx->d_shots, hs)) || (rc = up(&ctx->d_slot, order)) || (rc = up(&ctx->d_ident, ident)) ||
+        (rc = up(&ctx->d_wav, wav)) || (rc = up(&ctx->d_rec_x, rx)) || (rc = up(&ctx->d_rec_y, ry)) ||
+        (rc = up(&ctx->d_rec_z, rz)))
+        return rc;
+    const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
+    CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
+    CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
+    ctx->state_floats = 8 * (size_t)nshot * L.shot_stride;
+    if (cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->d_state = nullptr;
+        return set_err(ctx, SFD_ERR_NOMEM, "3-D wavefields of %d shots need %.1f GB of device memory", nshot,
+                       ctx->state_floats * 4.0 / 1e9);
+    }
+    int bp[2], bvy[2], bvz[2];
+    acoustic3d_boxes(R, bp, bvy, bvz);
+    const int* boxes[3] = {bp, bvy, bvz};
+    const int field_of[3] = {0, 4, 6};  // P, Vy, Vz
+    const long long fs = (long long)nshot * L.shot_stride;
+    for (int f = 0; f < 3; f++)
+        for (int b = 0; b < 2; b++) {
+            const int rc2 = encode_field_map3(ctx, &ctx->tmaps3[2 * f + b], ctx->d_state + (field_of[f] + b) * fs, L,
+                                              nshot, boxes[f]);
+            if (rc2) return rc2;
+        }
+    ctx->have_shots = true;
+    ctx->graph_valid = false;
+    return SFD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -740,10 +926,11 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     if (g->nx <= 0 || g->nz <= 0 || (is3d ? g->ny <= 0 : g->ny > 1)) return SFD_ERR_ARG;
     if (!(g->dx > 0) || !(g->dz > 0) || !(g->dt > 0) || (is3d && !(g->dy > 0))) return SFD_ERR_ARG;
     if (g->pml < 0 || g->pml > 256 || 2 * g->pml > g->nx || 2 * g->pml > g->nz) return SFD_ERR_ARG;
+    if (is3d && 2 * g->pml > g->ny) return SFD_ERR_ARG;
     float cf[8];
     if (sfd_fd_coeffs(g->order, cf) != SFD_OK) return SFD_ERR_ARG;
     const int R = g->order / 2;
-    if (g->nx <= 2 * R || g->nz <= 2 * R) return SFD_ERR_ARG;
+    if (g->nx <= 2 * R || g->nz <= 2 * R || (is3d && g->ny <= 2 * R)) return SFD_ERR_ARG;
     std::unique_ptr<sfd_ctx> c(new sfd_ctx());
     c->g = *g;
     if (c->g.ny <= 0) c->g.ny = 1;
@@ -772,7 +959,13 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
         c->plan.gz = 8;  // RSG halo 5, rounded for float4 staging
         c->plan.stages = 1;
     }
-    if (g->scheme == SFD_ACOUSTIC_3D) return set_err(ctx, SFD_ERR_UNSUPPORTED, "3-D scheme is not built yet");
+    if (g->scheme == SFD_ACOUSTIC_3D) {
+        int b0[2], b1[2], b2[2];
+        if (!acoustic3d_boxes(R, b0, b1, b2))
+            return set_err(ctx, SFD_ERR_UNSUPPORTED, "the 3-D kernel is built for orders 8 and 4, not %d", g->order);
+        if (g->flags & SFD_EXACT)
+            return set_err(ctx, SFD_ERR_UNSUPPORTED, "SFD_EXACT applies to the reference's 2-D schemes");
+    }
     *out = c.release();
     return SFD_OK;
 }
@@ -806,8 +999,12 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     }
     const int cols = ctx->g.nx * ctx->g.ny;
     const int nz = ctx->g.nz;
-    const int nzt = (nz + kTileZ - 1) / kTileZ * kTileZ;  // tiles may read past nz
-    ctx->mpitch = round_up(2 * kModelGhostZ + nzt, 32);
+    const bool is3d = ctx->g.scheme == SFD_ACOUSTIC_3D;
+    // 2-D: kModelGhostZ replicated rows on both sides, tiles may read past nz; 3-D: the field
+    // layout of one shot ([x][y][pitch], no ghost rows)
+    const int ghost = is3d ? 0 : kModelGhostZ;
+    const int nzt = (nz + kTileZ - 1) / kTileZ * kTileZ;
+    ctx->mpitch = is3d ? round_up(nz, 4) : round_up(2 * kModelGhostZ + nzt, 32);
     const size_t mfloats = (size_t)cols * ctx->mpitch;
     // Buffers are allocated once per context and refilled in place, so a captured time loop
     // (which bakes these pointers and the density constant in) stays valid across model updates.
@@ -820,7 +1017,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
             const float* s = src + (size_t)c * nz;
             float* d = staged.data() + (size_t)c * ctx->mpitch;
             for (int k = 0; k < ctx->mpitch; k++) {
-                const int z = std::min(std::max(k - kModelGhostZ, 0), nz - 1);
+                const int z = std::min(std::max(k - ghost, 0), nz - 1);
                 d[k] = s[z];
             }
         }
@@ -858,7 +1055,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     // source scale factors depend on the model
     if (ctx->have_shots) {
         for (auto& s : ctx->h_shots) {
-            const size_t mi = (size_t)(s.x0 + s.sx) * ctx->g.nz + s.sz;
+            const size_t mi = ((size_t)(s.x0 + s.sx) * ctx->g.ny + s.sy) * ctx->g.nz + s.sz;
             const float d = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
             float sc = ctx->g.dt * d;
             sc = sc * ctx->h_vp[mi];
@@ -871,6 +1068,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
 
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     if (!ctx || nshot <= 0 || !shots) return SFD_ERR_ARG;
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D) return set_shots_3d(ctx, nshot, shots);
     const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
     if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d is not implemented", ctx->g.scheme);
@@ -968,6 +1166,8 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     ctx->nshot = nshot;
     ctx->nt_max = nt_max;
     ctx->order = order;
+    ctx->nrec_max = 0;
+    for (const auto& d : hs) ctx->nrec_max = std::max(ctx->nrec_max, d.nrec);
 
     auto up = [&](auto** dst, const auto& v) -> int {
         using E = typename std::remove_reference<decltype(v)>::type::value_type;
@@ -1070,9 +1270,9 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
     ctx->timing.loop_ms = ms;
     ctx->timing.launches = launches + 2;
     ctx->timing.graph = 0;
-    ctx->timing.kernel_variant = (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
+    ctx->timing.kernel_variant = kernel_variant(ctx);
     double pts = 0;
-    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.ny * ctx->g.nz * s.nt;
     ctx->timing.point_updates = pts;
     ctx->timing.h2d_bytes = 0;
     ctx->timing.d2h_bytes = records ? (long long)sizeof(float) * ctx->rec_total : 0;
@@ -1085,6 +1285,27 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
     if (!ctx->have_shots || shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
     CK(cudaSetDevice(ctx->device));
     const ShotDev& sd = ctx->h_shots[shot];
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D) {
+        // P is stored damped, the velocities before the sponge multiply (applied here)
+        const int fidx = field == SFD_FIELD_P ? 0 : field == SFD_FIELD_VX ? 2 : field == SFD_FIELD_VY ? 4
+                                                                          : field == SFD_FIELD_VZ ? 6 : -1;
+        if (fidx < 0) return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+        const Layout3D& L = ctx->L3;
+        const int buf = sd.nt & 1;
+        const long long fs = (long long)ctx->nshot * L.shot_stride;
+        const float* base = ctx->d_state + (fidx + buf) * fs + (long long)shot * L.shot_stride;
+        const int nz = ctx->g.nz;
+        CK(cudaMemcpy2D(out, sizeof(float) * nz, base, sizeof(float) * L.pitch, sizeof(float) * nz,
+                        (size_t)L.nx * L.ny, cudaMemcpyDeviceToHost));
+        if (fidx != 0)
+            for (int x = 0; x < L.nx; x++)
+                for (int y = 0; y < L.ny; y++)
+                    for (int z = 0; z < nz; z++) {
+                        float& v = out[((size_t)x * L.ny + y) * nz + z];
+                        v = v * sponge3(ctx->g, x, y, z);
+                    }
+        return SFD_OK;
+    }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
         // vx, vz, sigma = (sx + sz) + sr (QS strxx), r = (rx + rz) + rr (QS rxx)
         const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;

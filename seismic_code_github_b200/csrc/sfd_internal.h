@@ -182,4 +182,44 @@ cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const S
                                      int nrec_max, int nt_max, cudaStream_t st);
 cudaError_t launch_nan_scan(const float* rec, long long n, int* flag, cudaStream_t st);
 
+// ---- 3-D acoustic scheme (acoustic3d.cu) ----
+// Field storage: per shot a dense [x][y][pitch] block, z fastest, pitch = nz rounded up to a
+// multiple of 4 (16-byte rows for the TMA strides and float4 accesses).  No ghost cells: the
+// tensor maps have the exact grid extents, so halo boxes read zeros outside the grid.
+constexpr int kTile3Y = 32;
+constexpr int kTile3Z = 32;
+struct Layout3D {
+    int nx, ny, nz;
+    int pitch;
+    long long xstride;      // ny * pitch
+    long long shot_stride;  // nx * ny * pitch
+    int nty, ntz;           // tiles per x-plane
+};
+struct Acou3DArgs {
+    CUtensorMap tm_p, tm_vy, tm_vz;   // 4-D maps (z, y, x, shot) of this step's input P, Vy, Vz
+    int* err_flag;
+    Layout3D L;
+    const float* p_in; const float* vx_in;
+    float* p_out; float* vx_out; float* vy_out; float* vz_out;
+    const float* vp; const float* den;  // model in the field layout (one shot); den NULL = constant
+    float den_c, dt;
+    float rdx, rdy, rdz;                // 1/dx, 1/dy, 1/dz
+    float dtdx, dtdy, dtdz;             // dt/dx, dt/dy, dt/dz
+    float coef[kMaxRadius];
+    int pml;
+    float sponge[256];                  // taper value at distance index q into the sponge
+    const int* slot_to_shot;
+};
+// one time step of all active shots: velocities, then pressure, sponge (one launch)
+cudaError_t acoustic3d_launch_step(int radius, const Acou3DArgs& a, int active, bool varden, cudaStream_t st);
+// P_in[source] -= inj_scale * w[step] for the active shots (before the step)
+cudaError_t acoustic3d_launch_inject(float* p, const Layout3D& L, const ShotDev* shots, const int* slot_to_shot,
+                                     int active, const float* wavelets, int step, cudaStream_t st);
+// records[rec_base + step * nrec + r] = P_out at receiver r (after the step)
+cudaError_t acoustic3d_launch_gather(const float* p, const Layout3D& L, const ShotDev* shots,
+                                     const int* slot_to_shot, int active, const int* rec_x, const int* rec_y,
+                                     const int* rec_z, float* records, int nrec_max, int step, cudaStream_t st);
+// TMA box extents (z, y) of the P, Vy and Vz boxes at this radius; false if unsupported
+bool acoustic3d_boxes(int radius, int box_p[2], int box_vy[2], int box_vz[2]);
+
 }  // namespace sfd
