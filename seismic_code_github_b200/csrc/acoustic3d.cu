@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "sfd_internal.h"
 
@@ -41,29 +42,37 @@ struct K3 {
     static constexpr int HY = 2 * R;          // y halo of the staged pressure
     static constexpr int HZ = r4(RQ + R);     // z halo of the staged pressure
     static constexpr int PY = TY + 2 * HY, PZ = TZ + 2 * HZ;
-    static constexpr int VYR = TY + 2 * R;    // rows of the Vy region
-    static constexpr int VZW = TZ + 2 * RQ;   // width of the Vz region
-    static constexpr int NVY = VYR * (TZ / 4);  // float4 tasks of the Vy region
-    static constexpr int NVZ = TY * (VZW / 4);  // float4 tasks of the Vz region
+    static constexpr int VYR = TY + 2 * R;    // rows of the Vy region (y0-R .. y0+TY+R-1)
+    static constexpr int VZW = TZ + 2 * RQ;   // columns of the Vz region (z0-RQ .. z0+TZ+RQ-1)
+    static constexpr int NVY2 = (VYR / 2) * (TZ / 4);  // Vy tasks: two rows x one float4
+    static constexpr int NVZ = TY * (VZW / 4);         // Vz tasks: one float4
+    // Vz tasks: threads from NVY2 on take up to three, the rest go to the last Vy threads
+    static constexpr int HVZ = kThreads - NVY2;
+    static constexpr int RVZ = NVZ > 3 * HVZ ? NVZ - 3 * HVZ : 0;
     // Vz window: P columns 4u + B4 .. of the staged box, BR = first needed column - B4
     static constexpr int B = HZ - RQ + 1 - R, B4 = B & ~3, BR = B - B4, NFZ = cdiv4(BR + 2 * R + 3);
     // d/dz of the new Vz at the own points: columns zr + D4 .. of the Vz region
     static constexpr int D = RQ - R, D4 = D & ~3, DR = D - D4, NFD = cdiv4(DR + 2 * R + 3);
+    static constexpr int NQ = 2 * R;  // planes held in the P (registers) and Vx (shared) queues
+    // shared layout (floats): two TMA stages {P box, Vy box, Vz box}, two buffers of the new
+    // Vy / Vz regions, the per-thread Vx ring, the sponge tables and two mbarriers
     static constexpr int OFF_VY = r32(PY * PZ);
     static constexpr int OFF_VZ = OFF_VY + r32(VYR * TZ);
     static constexpr int STAGE = r32(OFF_VZ + TY * VZW);
-    static constexpr int OFF_NY = 2 * STAGE;              // new Vy on the Vy region
-    static constexpr int OFF_NZ = OFF_NY + r32(VYR * TZ);  // new Vz on the Vz region
-    static constexpr int OFF_TY = OFF_NZ + r32(TY * VZW);  // float2 per Vy-region row
-    static constexpr int OFF_TZ = OFF_TY + r32(2 * VYR);    // float2 per Vz-region column
-    static constexpr int OFF_BAR = OFF_TZ + r32(2 * VZW);
+    static constexpr int NB_NZ = r32(VYR * TZ);           // within a new-velocity buffer
+    static constexpr int NBUF = NB_NZ + r32(TY * VZW);
+    static constexpr int OFF_NB = 2 * STAGE;
+    static constexpr int OFF_VQ = OFF_NB + 2 * NBUF;           // [NQ][kThreads] float4
+    static constexpr int NTAB = VYR * VZW;                      // positions of the CTA's region
+    static constexpr int OFF_FA = OFF_VQ + NQ * kThreads * 4;  // y/z damping factor per position
+    static constexpr int OFF_FK = OFF_FA + r32(NTAB);          // 1 where y and z are updated, else 0
+    static constexpr int OFF_BAR = OFF_FK + r32(NTAB);
     static constexpr int SMEM_FLOATS = OFF_BAR + 4;
     static constexpr unsigned TX_BYTES = 4u * (PY * PZ + VYR * TZ + TY * VZW);
-    static constexpr int NQ = 2 * R;  // planes held in each register queue
     static_assert(TY * TZ / 4 == kThreads, "one float4 of own points per thread");
-    static_assert(NVY <= 2 * kThreads && NVZ <= 2 * kThreads, "at most two halo tasks per thread");
+    static_assert(VYR % 2 == 0 && NVY2 <= kThreads && RVZ <= NVY2, "halo task split");
     static_assert(B >= 0 && D >= 0, "halo windows start inside the staged boxes");
-    static_assert(VYR <= 64 && VZW <= kThreads - 64, "table fill: one thread per entry");
+    static_assert(SMEM_FLOATS * 4 <= 227 * 1024, "shared memory of one CTA");
 };
 
 __device__ __forceinline__ unsigned sptr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -93,22 +102,43 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-__device__ __forceinline__ float c4(const float4& v, int i) {
-    return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+// bounded wait on an mbarrier phase: about one second of wall time, then give up
+__device__ __forceinline__ bool bounded_wait(uint64_t* bar, unsigned parity) {
+    bool done = mbar_try_wait(bar, parity);
+    if (!done) {
+        const uint64_t t0 = global_ns();
+        while (!(done = mbar_try_wait(bar, parity)) && global_ns() - t0 < 1000000000ull) {
+        }
+    }
+    return done;
 }
-__device__ __forceinline__ float& r4f(float4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
+
 __device__ __forceinline__ float4 ld4s(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4s(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float4 cat4(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+__device__ __forceinline__ float2 bc2(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) {
+    return cat4(__fmul2_rn(lo2(a), lo2(b)), __fmul2_rn(hi2(a), hi2(b)));
+}
 
 // Every stencil sum is written with explicit roundings in one fixed order, so a halo value a CTA
 // recomputes is bit-identical to the value the owning CTA stores.
-// sum_m C_m (hi_m - lo_m), m = 1..R
-template <int R>
+// sum_m C_m (hi_m - lo_m), m = 1..R, one point (z stencils) ...
 struct Acc {
     float v;
     __device__ __forceinline__ void add(int m, float c, float hi, float lo) {
         const float d = __fsub_rn(hi, lo);
         v = (m == 1) ? __fmul_rn(c, d) : __fmaf_rn(c, d, v);
+    }
+};
+// ... and two neighbouring z points per paired FP32 instruction (x and y stencils); cc = (c, c)
+struct Acc2 {
+    float2 v;
+    __device__ __forceinline__ void add(int m, float2 cc, float2 hi, float2 lo) {
+        const float2 d = __ffma2_rn(lo, make_float2(-1.0f, -1.0f), hi);  // hi - lo, one rounding
+        v = (m == 1) ? __fmul2_rn(cc, d) : __ffma2_rn(cc, d, v);
     }
 };
 
@@ -118,16 +148,23 @@ __device__ __forceinline__ float axis_taper(const Acou3DArgs& a, int d, int n, b
     *in_pad = q >= 0;
     return (q >= 0 && q < a.pml) ? a.sponge[q] : 1.0f;
 }
-// y/z part of the sponge (the y factor wins over the z factor where the pads overlap)
-__device__ __forceinline__ float taper_yz(const Acou3DArgs& a, int y, int z) {
-    bool py, pz;
-    const float fy = axis_taper(a, y, a.L.ny, &py);
-    const float fz = axis_taper(a, z, a.L.nz, &pz);
-    return py ? fy : fz;
-}
-template <int R>
-__device__ __forceinline__ bool in_yz(const Acou3DArgs& a, int y, int z) {
-    return y >= R && y < a.L.ny - R && z >= R && z < a.L.nz - R;
+
+// new velocity on four points: (v_old * f - b * sum) * k, with f the damping factors of the old
+// value and k the rim mask (EDGE), else v_old - b * sum
+template <bool EDGE>
+__device__ __forceinline__ float4 vel_update(float4 vo, float4 b, float2 s01, float2 s23, float4 f, float4 k) {
+    float2 v01 = lo2(vo), v23 = hi2(vo);
+    if (EDGE) {
+        v01 = __fmul2_rn(v01, lo2(f));
+        v23 = __fmul2_rn(v23, hi2(f));
+    }
+    v01 = __ffma2_rn(make_float2(-b.x, -b.y), s01, v01);
+    v23 = __ffma2_rn(make_float2(-b.z, -b.w), s23, v23);
+    if (EDGE) {
+        v01 = __fmul2_rn(v01, lo2(k));
+        v23 = __fmul2_rn(v23, hi2(k));
+    }
+    return cat4(v01, v23);
 }
 
 template <int R, bool VARDEN>
@@ -141,8 +178,9 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
     const int ty_i = blockIdx.x / L.ntz;
     const int y0 = ty_i * TY, z0 = (blockIdx.x - ty_i * L.ntz) * TZ;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + K::OFF_BAR);
-    float* sNY = smem + K::OFF_NY;
-    float* sNZ = smem + K::OFF_NZ;
+    float4* sVq = reinterpret_cast<float4*>(smem + K::OFF_VQ) + tid;  // this thread's Vx ring
+    const float* sFA = smem + K::OFF_FA;
+    const float* sFK = smem + K::OFF_FK;
 
     // own points: one row y, four consecutive z
     const int yl = tid >> 3, zr = (tid & 7) * 4;
@@ -153,33 +191,23 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
     const float* p_in = a.p_in + shot_off;
     const float* vx_in = a.vx_in + shot_off;
 
-    // Per-CTA tables of the y / z sponge factors and rim masks (read on edge iterations only):
-    // tY[i] for y = y0 - R + i: (taper if y lies in a y pad else -1, 1 if R <= y < ny-R else 0),
-    // tZ[i] for z = z0 - RQ + i: (taper or 1, 1 if R <= z < nz-R else 0).
-    float2* tY = reinterpret_cast<float2*>(smem + K::OFF_TY);
-    float2* tZ = reinterpret_cast<float2*>(smem + K::OFF_TZ);
-    if (tid < K::VYR) {
-        const int y = y0 - R + tid;
-        bool py;
-        const float f = axis_taper(a, y, ny, &py);
-        tY[tid] = make_float2(py ? f : -1.0f, (y >= R && y < ny - R) ? 1.0f : 0.0f);
-    } else if (tid >= 64 && tid < 64 + K::VZW) {
-        const int z = z0 - K::RQ + (tid - 64);
-        bool pz;
-        const float f = axis_taper(a, z, nz, &pz);
-        tZ[tid - 64] = make_float2(f, (z >= R && z < nz - R) ? 1.0f : 0.0f);
+    // Damping factor (y pad wins over z pad; 1 outside the pads) and rim mask of every position
+    // (y0-R+i, z0-RQ+j) of the CTA's region; the x pad is applied per plane.
+    for (int i = tid; i < K::NTAB; i += kThreads) {
+        const int y = y0 - R + i / K::VZW, z = z0 - K::RQ + i % K::VZW;
+        bool py, pz;
+        const float fy = axis_taper(a, y, ny, &py);
+        const float fz = axis_taper(a, z, nz, &pz);
+        smem[K::OFF_FA + i] = py ? fy : fz;
+        smem[K::OFF_FK + i] = (y >= R && y < ny - R && z >= R && z < nz - R) ? 1.0f : 0.0f;
     }
     const int E = a.pml > R ? a.pml : R;
     const bool yz_int = y0 - R >= E && y0 + TY + R <= ny - E && z0 - K::RQ >= E && z0 + TZ + K::RQ <= nz - E;
     const float bxc = a.dtdx / a.den_c, byc = a.dtdy / a.den_c, bzc = a.dtdz / a.den_c, kc = a.den_c * a.dt;
+    float2 cc[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) cc[m] = bc2(a.coef[m]);
 
-    auto own_tables = [&](float2& fy, float2* fz) {
-        fy = tY[yl + R];
-        const float4 z01 = ld4s(reinterpret_cast<const float*>(tZ + K::RQ + zr));
-        const float4 z23 = ld4s(reinterpret_cast<const float*>(tZ + K::RQ + zr + 2));
-        fz[0] = make_float2(z01.x, z01.y); fz[1] = make_float2(z01.z, z01.w);
-        fz[2] = make_float2(z23.x, z23.y); fz[3] = make_float2(z23.z, z23.w);
-    };
     auto ld_own = [&](const float* base, int x) -> float4 {
         if (!own_ok || x >= nx) return make_float4(0.f, 0.f, 0.f, 0.f);
         return __ldg(reinterpret_cast<const float4*>(base + (long long)x * L.xstride + own_off));
@@ -189,7 +217,8 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
         z = min(max(z, 0), L.pitch - 4);
         return __ldg(reinterpret_cast<const float4*>(base + (long long)x * L.xstride + (long long)y * L.pitch + z));
     };
-    auto issue = [&](int s, int stg) {
+    auto issue = [&](int s) {
+        const int stg = s & 1;
         float* st = smem + stg * K::STAGE;
         uint64_t* bar = bars + stg;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -208,98 +237,91 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
     __syncthreads();
     // iteration s: new Vx on plane s+R-1 (own points), then, for s >= R, new Vy / Vz on plane s
     // (column + halo) and new P on plane s.  Planes below R and from nx-R on are the frozen rim.
+    // The boxes of plane s+2 are requested once every thread is done with those of plane s.
     const int s_begin = 1, s_end = nx - R;
-    if (tid == 0) issue(s_begin, s_begin & 1);
-
-    float4 Pq[K::NQ], Vq[K::NQ];
+    if (tid == 0) {
+        issue(s_begin);
+        if (s_begin + 1 < s_end) issue(s_begin + 1);
+    }
+    float4 Pq[K::NQ];
 #pragma unroll
     for (int j = 0; j < K::NQ; j++) {
         Pq[j] = ld_own(p_in, s_begin + j);
-        Vq[j] = make_float4(0.f, 0.f, 0.f, 0.f);  // planes s_begin - R .. R - 1: rim
+        sVq[j * kThreads] = make_float4(0.f, 0.f, 0.f, 0.f);  // planes below R: rim
     }
     float4 Pn = ld_own(p_in, s_begin + K::NQ);
     float4 Vxo = ld_own(vx_in, s_begin + R - 1);
-    float4 vpn = ld_own(a.vp - 0, s_begin);
+    float4 vpn = ld_own(a.vp, s_begin);
     unsigned phase = 0;
 
     for (int s = s_begin; s < s_end; s++) {
         const int stg = s & 1;
-        const unsigned par = (phase >> stg) & 1u;
-        bool done = mbar_try_wait(bars + stg, par);
-        if (!done) {
-            const uint64_t t0 = global_ns();
-            while (!(done = mbar_try_wait(bars + stg, par)) && global_ns() - t0 < 1000000000ull) {
-            }
-        }
-        if (__syncthreads_or(!done)) {  // also: every thread is done with iteration s-1
-            if (tid == 0) atomicExch(a.err_flag, 1);
-            return;
-        }
+        const bool got = bounded_wait(bars + stg, (phase >> stg) & 1u);
         phase ^= 1u << stg;
-        if (tid == 0 && s + 1 < s_end) issue(s + 1, stg ^ 1);
         const float* st = smem + stg * K::STAGE;
-        const float4 vxo = Vxo, vpc = vpn, pnext = Pn;
-        Pn = ld_own(p_in, s + K::NQ + 1);
-        Vxo = ld_own(vx_in, s + R);
-        vpn = ld_own(a.vp, s + 1);
-
+        float* nby = smem + K::OFF_NB + stg * K::NBUF;  // new Vy region of this plane
+        float* nbz = nby + K::NB_NZ;                     // new Vz region of this plane
+        // the loads of the next plane's own values are issued as soon as this plane's are used
         const int xv = s + R - 1;  // plane of this iteration's new Vx
         const bool edge = !yz_int || !(s >= E && xv < nx - E);
-        // x-plane factors (uniform): sponge value where the plane lies in an x pad, rim masks
         bool xpad_s, xpad_v;
         const float fx_s = axis_taper(a, s, nx, &xpad_s);
         const float fx_v = axis_taper(a, xv, nx, &xpad_v);
-        const bool xin_s = s >= R && s < nx - R, xin_v = xv >= R && xv < nx - R;
+        const float kx_s = (s >= R && s < nx - R) ? 1.0f : 0.0f, kx_v = (xv >= R && xv < nx - R) ? 1.0f : 0.0f;
+        // damping factors and masks of four points of the region at table index i, plane s
+        auto edge_f = [&](int i, bool xpad, float fx) {
+            return xpad ? make_float4(fx, fx, fx, fx) : ld4s(sFA + i);
+        };
+        auto edge_k = [&](int i, float kx) {
+            const float4 k = ld4s(sFK + i);
+            return make_float4(k.x * kx, k.y * kx, k.z * kx, k.w * kx);
+        };
 
         if (s >= R) {
-            // ---- new Vy on the Vy region: rows y0-R .. y0+TY+R-1, float4 along z ----
+            const long long plane_off = shot_off + (long long)s * L.xstride;
+            // ---- new Vy on the Vy region: rows y0-R .. y0+TY+R-1, two rows x float4 per task ----
+            if (tid < K::NVY2) {
+                const int r0 = (tid >> 3) * 2, zt = (tid & 7) * 4;
+                // P rows r0+R+1-m (lo, row r0) ... r0+R+1+m (hi, row r0+1), center row shared
+                const float* pc = st + K::HZ + zt;
+                Acc2 a01, a23, b01, b23;  // rows r0 and r0+1
+                float4 hi_a = ld4s(pc + (r0 + R + 1) * K::PZ), lo_b = hi_a;
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int t = tid + k * kThreads;
-                if (k == 1 && t >= K::NVY) break;
-                const int row = t >> 3, zt = (t & 7) * 4;
-                float4 sum;
-                {
-                    Acc<R> acc[4];
+                for (int m = 1; m <= R; m++) {
+                    const float4 lo_a = ld4s(pc + (r0 + R + 1 - m) * K::PZ);
+                    const float4 hi_b = ld4s(pc + (r0 + R + 1 + m) * K::PZ);
+                    a01.add(m, cc[m - 1], lo2(hi_a), lo2(lo_a));
+                    a23.add(m, cc[m - 1], hi2(hi_a), hi2(lo_a));
+                    b01.add(m, cc[m - 1], lo2(hi_b), lo2(lo_b));
+                    b23.add(m, cc[m - 1], hi2(hi_b), hi2(lo_b));
+                    hi_a = hi_b;
+                    lo_b = lo_a;
+                }
 #pragma unroll
-                    for (int m = 1; m <= R; m++) {
-                        const float4 hi = ld4s(st + (row + R + m) * K::PZ + K::HZ + zt);
-                        const float4 lo = ld4s(st + (row + R - m + 1) * K::PZ + K::HZ + zt);
-#pragma unroll
-                        for (int c = 0; c < 4; c++) acc[c].add(m, a.coef[m - 1], c4(hi, c), c4(lo, c));
+                for (int h = 0; h < 2; h++) {
+                    const int row = r0 + h;
+                    float4 b = make_float4(byc, byc, byc, byc);
+                    if (VARDEN) {
+                        const float4 d = ld_model(a.den, s, y0 - R + row, z0 + zt);
+                        b = make_float4(a.dtdy / d.x, a.dtdy / d.y, a.dtdy / d.z, a.dtdy / d.w);
                     }
-                    sum = make_float4(acc[0].v, acc[1].v, acc[2].v, acc[3].v);
+                    const float4 vo = ld4s(st + K::OFF_VY + row * TZ + zt);
+                    const float2 s01 = h ? b01.v : a01.v, s23 = h ? b23.v : a23.v;
+                    float4 vn;
+                    if (edge) {
+                        const int i = row * K::VZW + K::RQ + zt;
+                        vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                    } else {
+                        vn = vel_update<false>(vo, b, s01, s23, vo, vo);
+                    }
+                    st4s(nby + row * TZ + zt, vn);
+                    const int y = y0 - R + row;
+                    if (row >= R && row < R + TY && y < ny && z0 + zt < L.pitch)
+                        st4s(a.vy_out + plane_off + (long long)y * L.pitch + z0 + zt, vn);
                 }
-                float4 vo = ld4s(st + K::OFF_VY + row * TZ + zt);
-                float4 b = make_float4(byc, byc, byc, byc);
-                if (VARDEN) {
-                    const float4 d = ld_model(a.den, s, y0 - R + row, z0 + zt);
-                    b = make_float4(a.dtdy / d.x, a.dtdy / d.y, a.dtdy / d.z, a.dtdy / d.w);
-                }
-                float4 vn;
-                float2 fy, fz[4];
-                if (edge) {
-                    fy = tY[row];
-                    const float4 z01 = ld4s(reinterpret_cast<const float*>(tZ + K::RQ + zt));
-                    const float4 z23 = ld4s(reinterpret_cast<const float*>(tZ + K::RQ + zt + 2));
-                    fz[0] = make_float2(z01.x, z01.y); fz[1] = make_float2(z01.z, z01.w);
-                    fz[2] = make_float2(z23.x, z23.y); fz[3] = make_float2(z23.z, z23.w);
-                }
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    float v = c4(vo, c);
-                    if (edge) v = __fmul_rn(v, xpad_s ? fx_s : (fy.x >= 0.0f ? fy.x : fz[c].x));
-                    v = __fmaf_rn(-c4(b, c), c4(sum, c), v);
-                    if (edge) v = (xin_s && fy.y != 0.0f && fz[c].y != 0.0f) ? v : 0.0f;
-                    r4f(vn, c) = v;
-                }
-                st4s(sNY + row * TZ + zt, vn);
             }
             // ---- new Vz on the Vz region: rows y0 .. y0+TY-1, z0-RQ .. z0+TZ+RQ-1 ----
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int t = tid + k * kThreads;
-                if (k == 1 && t >= K::NVZ) break;
+            auto vz_task = [&](int t) {
                 const int row = t / (K::VZW / 4), u = t % (K::VZW / 4);
                 float w[4 * K::NFZ];
 #pragma unroll
@@ -307,79 +329,105 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
                     const float4 v = ld4s(st + (row + K::HY) * K::PZ + 4 * u + K::B4 + 4 * f);
                     w[4 * f] = v.x; w[4 * f + 1] = v.y; w[4 * f + 2] = v.z; w[4 * f + 3] = v.w;
                 }
-                float4 vo = ld4s(st + K::OFF_VZ + row * K::VZW + 4 * u);
+                Acc acc[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+#pragma unroll
+                    for (int m = 1; m <= R; m++)
+                        acc[c].add(m, a.coef[m - 1], w[K::BR + R - 1 + c + m], w[K::BR + R + c - m]);
                 float4 b = make_float4(bzc, bzc, bzc, bzc);
                 if (VARDEN) {
                     const float4 d = ld_model(a.den, s, y0 + row, z0 - K::RQ + 4 * u);
                     b = make_float4(a.dtdz / d.x, a.dtdz / d.y, a.dtdz / d.z, a.dtdz / d.w);
                 }
+                const float4 vo = ld4s(st + K::OFF_VZ + row * K::VZW + 4 * u);
+                const float2 s01 = make_float2(acc[0].v, acc[1].v), s23 = make_float2(acc[2].v, acc[3].v);
                 float4 vn;
-                float2 fy, fz[4];
                 if (edge) {
-                    fy = tY[row + R];
-                    const float4 z01 = ld4s(reinterpret_cast<const float*>(tZ + 4 * u));
-                    const float4 z23 = ld4s(reinterpret_cast<const float*>(tZ + 4 * u + 2));
-                    fz[0] = make_float2(z01.x, z01.y); fz[1] = make_float2(z01.z, z01.w);
-                    fz[2] = make_float2(z23.x, z23.y); fz[3] = make_float2(z23.z, z23.w);
+                    const int i = (row + R) * K::VZW + 4 * u;
+                    vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                } else {
+                    vn = vel_update<false>(vo, b, s01, s23, vo, vo);
                 }
+                st4s(nbz + row * K::VZW + 4 * u, vn);
+                const int y = y0 + row, z = z0 - K::RQ + 4 * u;
+                if (4 * u >= K::RQ && 4 * u < K::RQ + TZ && y < ny && z < L.pitch)
+                    st4s(a.vz_out + plane_off + (long long)y * L.pitch + z, vn);
+            };
+            if (tid >= K::NVY2) {
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    Acc<R> acc;
-#pragma unroll
-                    for (int m = 1; m <= R; m++)
-                        acc.add(m, a.coef[m - 1], w[K::BR + R - 1 + c + m], w[K::BR + R + c - m]);
-                    float v = c4(vo, c);
-                    if (edge) v = __fmul_rn(v, xpad_s ? fx_s : (fy.x >= 0.0f ? fy.x : fz[c].x));
-                    v = __fmaf_rn(-c4(b, c), acc.v, v);
-                    if (edge) v = (xin_s && fy.y != 0.0f && fz[c].y != 0.0f) ? v : 0.0f;
-                    r4f(vn, c) = v;
+                for (int k = 0; k < 3; k++) {
+                    const int j = (tid - K::NVY2) + k * K::HVZ;
+                    if (j < K::NVZ) vz_task(j);
                 }
-                st4s(sNZ + row * K::VZW + 4 * u, vn);
+            } else if (K::RVZ > 0 && tid >= K::NVY2 - K::RVZ) {
+                vz_task(3 * K::HVZ + tid - (K::NVY2 - K::RVZ));
             }
         }
-        // ---- new Vx on plane xv (own points, register queue) ----
+        const int io = (yl + R) * K::VZW + K::RQ + zr;  // table index of the own points
+        // ---- new Vx on plane xv (own points, P from the register queue) ----
         {
+            Acc2 s01, s23;
+#pragma unroll
+            for (int m = 1; m <= R; m++) {
+                s01.add(m, cc[m - 1], lo2(Pq[R - 1 + m]), lo2(Pq[R - m]));
+                s23.add(m, cc[m - 1], hi2(Pq[R - 1 + m]), hi2(Pq[R - m]));
+            }
             float4 b = make_float4(bxc, bxc, bxc, bxc);
             if (VARDEN) {
                 const float4 d = ld_model(a.den, xv, yo, zo);
                 b = make_float4(a.dtdx / d.x, a.dtdx / d.y, a.dtdx / d.z, a.dtdx / d.w);
             }
-            float4 vn;
-            float2 fy, fz[4];
-            if (edge) own_tables(fy, fz);
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                Acc<R> acc;
-#pragma unroll
-                for (int m = 1; m <= R; m++) acc.add(m, a.coef[m - 1], c4(Pq[R - 1 + m], c), c4(Pq[R - m], c));
-                float v = c4(vxo, c);
-                if (edge) v = __fmul_rn(v, xpad_v ? fx_v : (fy.x >= 0.0f ? fy.x : fz[c].x));
-                v = __fmaf_rn(-c4(b, c), acc.v, v);
-                if (edge) v = (xin_v && fy.y != 0.0f && fz[c].y != 0.0f) ? v : 0.0f;
-                r4f(vn, c) = v;
-            }
+            const float4 vn = edge ? vel_update<true>(Vxo, b, s01.v, s23.v, edge_f(io, xpad_v, fx_v), edge_k(io, kx_v))
+                                   : vel_update<false>(Vxo, b, s01.v, s23.v, Vxo, Vxo);
+            Vxo = ld_own(vx_in, s + R);
             if (own_ok) st4s(a.vx_out + shot_off + (long long)xv * L.xstride + own_off, vn);
-#pragma unroll
-            for (int j = 0; j + 1 < K::NQ; j++) Vq[j] = Vq[j + 1];
-            Vq[K::NQ - 1] = vn;
+            sVq[((unsigned)xv % K::NQ) * kThreads] = vn;
         }
-        __syncthreads();  // new Vy / Vz of the column and its halo are in shared memory
+        // every thread is done with this stage and with the new-velocity buffer of plane s-1
+        if (__syncthreads_or(!got)) {
+            if (tid == 0) {
+                atomicExch(a.err_flag, 1);
+                // let the copies still in flight land before the CTA's shared memory is released
+                bounded_wait(bars + stg, ((phase >> stg) & 1u) ^ 1u);
+                if (s + 1 < s_end) bounded_wait(bars + (stg ^ 1), (phase >> (stg ^ 1)) & 1u);
+            }
+            return;
+        }
+        if (tid == 0 && s + 2 < s_end) issue(s + 2);
         if (s >= R) {
             // ---- new P on plane s (own points) ----
             float wz[4 * K::NFD];
 #pragma unroll
             for (int f = 0; f < K::NFD; f++) {
-                const float4 v = ld4s(sNZ + yl * K::VZW + zr + K::D4 + 4 * f);
+                const float4 v = ld4s(nbz + yl * K::VZW + zr + K::D4 + 4 * f);
                 wz[4 * f] = v.x; wz[4 * f + 1] = v.y; wz[4 * f + 2] = v.z; wz[4 * f + 3] = v.w;
             }
-            Acc<R> ay_acc[4];
+            Acc2 ax01, ax23, ay01, ay23;
 #pragma unroll
             for (int m = 1; m <= R; m++) {
-                const float4 hi = ld4s(sNY + (yl + R + m - 1) * TZ + zr);
-                const float4 lo = ld4s(sNY + (yl + R - m) * TZ + zr);
-#pragma unroll
-                for (int c = 0; c < 4; c++) ay_acc[c].add(m, a.coef[m - 1], c4(hi, c), c4(lo, c));
+                const float4 xhi = sVq[((unsigned)(s + m - 1) % K::NQ) * kThreads];
+                const float4 xlo = sVq[((unsigned)(s - m) % K::NQ) * kThreads];
+                ax01.add(m, cc[m - 1], lo2(xhi), lo2(xlo));
+                ax23.add(m, cc[m - 1], hi2(xhi), hi2(xlo));
+                const float4 yhi = ld4s(nby + (yl + R + m - 1) * TZ + zr);
+                const float4 ylo = ld4s(nby + (yl + R - m) * TZ + zr);
+                ay01.add(m, cc[m - 1], lo2(yhi), lo2(ylo));
+                ay23.add(m, cc[m - 1], hi2(yhi), hi2(ylo));
             }
+            Acc az[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+#pragma unroll
+                for (int m = 1; m <= R; m++)
+                    az[c].add(m, a.coef[m - 1], wz[K::DR + R + c + m - 1], wz[K::DR + R + c - m]);
+            // div = ((Sx / dx) + Sy / dy) + Sz / dz, then P = P - (den dt vp vp) div
+            const float2 rdx = bc2(a.rdx), rdy = bc2(a.rdy), rdz = bc2(a.rdz);
+            float2 d01 = __fmul2_rn(ax01.v, rdx), d23 = __fmul2_rn(ax23.v, rdx);
+            d01 = __ffma2_rn(ay01.v, rdy, d01);
+            d23 = __ffma2_rn(ay23.v, rdy, d23);
+            d01 = __ffma2_rn(make_float2(az[0].v, az[1].v), rdz, d01);
+            d23 = __ffma2_rn(make_float2(az[2].v, az[3].v), rdz, d23);
             float4 kk;
             if (VARDEN) {
                 const float4 d = ld_model(a.den, s, yo, zo);
@@ -387,40 +435,18 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
             } else {
                 kk = make_float4(kc, kc, kc, kc);
             }
-            const float4 pold = Pq[0];
-            float4 pn;
-            float2 fy, fz[4];
-            if (edge) own_tables(fy, fz);
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                Acc<R> ax, az_;
-#pragma unroll
-                for (int m = 1; m <= R; m++) {
-                    ax.add(m, a.coef[m - 1], c4(Vq[R + m - 1], c), c4(Vq[R - m], c));
-                    az_.add(m, a.coef[m - 1], wz[K::DR + R + c + m - 1], wz[K::DR + R + c - m]);
-                }
-                float div = __fmul_rn(ax.v, a.rdx);
-                div = __fmaf_rn(ay_acc[c].v, a.rdy, div);
-                div = __fmaf_rn(az_.v, a.rdz, div);
-                const float v = c4(vpc, c);
-                const float k = __fmul_rn(__fmul_rn(c4(kk, c), v), v);
-                float p = __fmaf_rn(-k, div, c4(pold, c));
-                if (edge)
-                    p = (xin_s && fy.y != 0.0f && fz[c].y != 0.0f)
-                            ? __fmul_rn(p, xpad_s ? fx_s : (fy.x >= 0.0f ? fy.x : fz[c].x))
-                            : 0.0f;
-                r4f(pn, c) = p;
-            }
-            if (own_ok) {
-                const long long o = shot_off + (long long)s * L.xstride + own_off;
-                st4s(a.p_out + o, pn);
-                st4s(a.vy_out + o, ld4s(sNY + (yl + R) * TZ + zr));
-                st4s(a.vz_out + o, ld4s(sNZ + yl * K::VZW + zr + K::RQ));
-            }
+            const float2 k01 = __fmul2_rn(__fmul2_rn(lo2(kk), lo2(vpn)), lo2(vpn));
+            const float2 k23 = __fmul2_rn(__fmul2_rn(hi2(kk), hi2(vpn)), hi2(vpn));
+            float4 pn = cat4(__ffma2_rn(make_float2(-k01.x, -k01.y), d01, lo2(Pq[0])),
+                             __ffma2_rn(make_float2(-k23.x, -k23.y), d23, hi2(Pq[0])));
+            if (edge) pn = mul4(mul4(pn, edge_f(io, xpad_s, fx_s)), edge_k(io, kx_s));
+            if (own_ok) st4s(a.p_out + shot_off + (long long)s * L.xstride + own_off, pn);
         }
+        vpn = ld_own(a.vp, s + 1);
 #pragma unroll
         for (int j = 0; j + 1 < K::NQ; j++) Pq[j] = Pq[j + 1];
-        Pq[K::NQ - 1] = pnext;
+        Pq[K::NQ - 1] = Pn;
+        Pn = ld_own(p_in, s + K::NQ + 1);
     }
 }
 
