@@ -279,6 +279,55 @@ def measure_viscoacoustic(args, dev):
     return out
 
 
+def measure_3d(args, dev):
+    """Config 5: 3-D acoustic, 16 shots of 612^3 padded cells in one batched time loop.  The
+    record lengths are scaled by --d3-nt-scale so the section stays short; the per-step cost does
+    not depend on nt.  No 3-D reference exists: the CPU figure is the restated scheme
+    (oracle/afd3d_oracle.cpp, OpenMP, FP32) on one shot for a few steps."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config5(nshot=args.d3_nshot, nt_scale=args.d3_nt_scale)
+    n, d = c["n"], c["d"]
+    vp = np.empty((n, n, n), np.float32)
+    for x0 in range(0, n, 64):
+        vp[x0:x0 + 64] = c["vp_slab"](x0, min(n, x0 + 64))
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_RIC, nt, c["dt"], c["f0"], 80), sy=sy, rec_y=ry)
+             for (sx, sy, sz), (rx, ry, rz), nt in zip(c["src"], c["rec"], c["nt"])]
+    with S.Engine(S.ACOUSTIC_3D, n, n, d, d, c["dt"], c["PML"], order=8, ny=n, dy=d, device=dev) as e:
+        e.set_model(vp)
+        e.set_shots(shots)
+        e.forward_device(0)
+        ms = []
+        for _ in range(args.d3_steps):
+            e.forward_device(0)
+            t = e.timing()
+            ms.append(t["loop_ms"])
+    pts = float(n) ** 3 * sum(c["nt"])
+    gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    out = {"workload": f"config 5: 3-D acoustic order 8, {c['N']}^3 interior ({n}^3 padded), {len(shots)} shots, "
+                       f"256x256 receivers each, record lengths 1500-2500 scaled by {args.d3_nt_scale} "
+                       f"(nt {min(c['nt'])}-{max(c['nt'])})",
+           "gpts_per_s": gpts, "loop_ms": float(np.median(ms)), "launches": t["launches"], "bytes_per_point": 36,
+           "hbm_frac_of_measured": 36 * gpts / read_peaks()[0], "parity": "relL2 <= 1e-5 vs FP64 restatement"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        steps = args.d3_cpu_steps
+        r = np.zeros(1, np.int32) + c["PML"]
+        w = shots[0].wavelet[:steps + 1]
+        t0 = time.perf_counter()
+        ol.afd3d_forward(vp, None, w[:1], c["src"][0], r, r, r, c["PML"], d, d, d, c["dt"], fp64=False)
+        t1 = time.perf_counter()
+        ol.afd3d_forward(vp, None, w[:steps + 1], c["src"][0], r, r, r, c["PML"], d, d, d, c["dt"], fp64=False)
+        wall = (time.perf_counter() - t1) - (t1 - t0)
+        out["cpu_baseline"] = {"value": n ** 3 * steps / max(wall, 1e-9) / 1e9, "unit": "Gpts/s",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"restated 3-D step (oracle/afd3d_oracle.cpp, OpenMP, FP32) on one shot: the "
+                                         f"difference of a {steps + 1}- and a 1-step run on the {n}^3 grid"}
+    del vp
+    return out
+
+
 def config_dict(case, args):
     return {"workload": f"batched 2-D acoustic forward, {case.NZ}x{case.NX} interior "
                         f"({case.Nz}x{case.Nx} padded, {case.PML}-cell sponge), {case.nshot} shots, nt={case.nt}, "
@@ -409,6 +458,8 @@ def run_ours(args, world, rank, local):
         line["gradient"] = measure_gradient(args, dev)
     if world == 1 and args.q_steps > 0:
         line["viscoacoustic"] = measure_viscoacoustic(args, dev)
+    if world == 1 and args.d3_steps > 0:
+        line["acoustic3d"] = measure_3d(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_reference_sample(case, args.ref_steps).items() if k != "wall_s"}
     print(json.dumps(line), flush=True)
@@ -434,6 +485,10 @@ def main():
     ap.add_argument("--q-steps", type=int, default=2, help="timed viscoacoustic forwards (0 = skip)")
     ap.add_argument("--q-nshot", type=int, default=16)
     ap.add_argument("--q-cpu-steps", type=int, default=120)
+    ap.add_argument("--d3-steps", type=int, default=2, help="timed 3-D forwards (0 = skip)")
+    ap.add_argument("--d3-nshot", type=int, default=16)
+    ap.add_argument("--d3-nt-scale", type=float, default=0.05)
+    ap.add_argument("--d3-cpu-steps", type=int, default=3)
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

@@ -157,6 +157,46 @@ def config3(nshot: int = 16):
             "interior": (vp, rho, q)}
 
 
+def config5(nshot: int = 16, nt_scale: float = 1.0):
+    """3-D acoustic, 8th order: 512^3 interior, dx = dy = dz = 10 m, dt = 1 ms, 50-cell sponge
+    (612^3 padded), smooth layered vp 1500-4000 m/s (6 layers, Gaussian-smoothed with sigma = 6
+    cells, +-3% smooth lateral variation), 16 shots on a 4 x 4 grid at interior depth 2, record
+    lengths drawn uniformly from 1500-2500 steps (times nt_scale), a 256 x 256 receiver patch per
+    shot at interior depth 2 with seeded offsets, 15 Hz Ricker (RIC formula).  Returns a dict; the
+    velocity is built per x-slab (the grid holds 229M cells)."""
+    from scipy.ndimage import gaussian_filter1d
+    N, PML = 512, 50
+    n = N + 2 * PML
+    rng = np.random.default_rng(20261207)
+    bounds = np.sort(rng.uniform(0.1, 0.9, 5)) * N
+    z = np.arange(N)
+    col = np.linspace(1500.0, 4000.0, 6)[np.searchsorted(bounds, z, side="right")]
+    col = gaussian_filter1d(col, 6.0, mode="nearest")
+    col = np.pad(col, (PML, PML), mode="edge").astype(np.float32)
+    kx, ky = rng.uniform(1.0, 3.0, 2) * 2 * np.pi / n
+    px, py = rng.uniform(0, 2 * np.pi, 2)
+    yy = np.arange(n)
+
+    def vp_slab(x0: int, x1: int) -> np.ndarray:
+        xs = np.arange(x0, x1)
+        lat = 1.0 + 0.03 * np.cos(kx * xs[:, None] + px) * np.cos(ky * yy[None, :] + py)
+        return (lat[:, :, None] * col[None, None, :]).astype(np.float32)
+
+    nts = [max(1, int(round(v * nt_scale))) for v in rng.integers(1500, 2501, nshot)]
+    g = [PML + int(round((i + 0.5) * N / 4)) for i in range(4)]
+    src = [(g[i % 4], g[i // 4], PML + 2) for i in range(nshot)]
+    rec = []
+    for s in src:
+        ox, oy = rng.integers(-64, 65, 2)
+        x0 = int(np.clip(s[0] - 128 + ox, PML, PML + N - 256))
+        y0 = int(np.clip(s[1] - 128 + oy, PML, PML + N - 256))
+        ry, rx = np.meshgrid(np.arange(y0, y0 + 256), np.arange(x0, x0 + 256), indexing="ij")
+        rec.append((rx.ravel().astype(np.int32), ry.ravel().astype(np.int32),
+                    np.full(256 * 256, PML + 2, np.int32)))
+    return {"name": "config5_3d_512cube", "N": N, "PML": PML, "n": n, "d": 10.0, "dt": 1e-3, "f0": 15.0,
+            "vp_slab": vp_slab, "src": src, "rec": rec, "nt": nts}
+
+
 def small_varden(seed: int = 7) -> AcousticCase:
     """Non-square, variable-density case used to pin the restatement against the reference
     build: 80 (x) x 60 (z) interior, 15-cell sponge, 300 steps, off-centre source."""
