@@ -166,6 +166,17 @@ int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps);
 
 int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);
 
+/* Wavefield snapshots taken inside the forward time loop.  Replaces the Snap.dat / Pall.dat
+ * writes of AFD:343-373 and the snapshot files of QM:462-481.  Stream id (0..3) records, after
+ * every step k (0-based) with k >= first and (k - first) % every == 0, at most `count` times per
+ * shot, the interior (pml <= x < nx_shot - pml, pml <= z < nz - pml) of `field` as the reference
+ * holds it after the step: SFD_FIELD_P (AFD P1 / QS strxx), SFD_FIELD_VX, SFD_FIELD_VZ, and
+ * SFD_FIELD_R for the viscoacoustic scheme.  count = 0 removes the stream.  2-D schemes only. */
+int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int count);
+/* The snapshots of stream id for one shot from the last forward: n x (nx_shot - 2 pml) x
+ * (nz - 2 pml) floats, x-major, z fastest; *n_out receives n.  out may be NULL to query n. */
+int sfd_get_snapshots(sfd_ctx* ctx, int id, int shot, float* out, int* n_out);
+
 /* Single-shot 2-D acoustic forward that allocates no device memory.  No counterpart in the
  * reference: it is for callers that cannot allocate device memory when they model a shot (a
  * framework that has reserved the device memory for its own allocator, a process at its
@@ -192,6 +203,38 @@ int sfd_fd_coeffs(int order, float* coeffs);
 /* Edge-replicated padding of an interior model (QS:340-372): in (nx_in, nz_in) ->
  * out (nx_in + pxn + pxp, nz_in + pzn + pzp). */
 int sfd_pad_model(const float* in, int nx_in, int nz_in, int pxn, int pxp, int pzn, int pzp, float* out);
+
+/* ---- the reference programs' file contract (host only) ---- */
+/* Q_forward parameter card (QS:121-234): pairs of a label line and a value line, in this order.
+ * fdo2 / fdo1 are read and unused, as in the reference (the scheme is 10th order). */
+typedef struct {
+    char vp[256], vs[256], rho[256], qp[256], qs[256];     /* model files (nz x nx Fortran arrays) */
+    char shot1[256], shot2[256], shot3[256], shot4[256];   /* per-shot / merged record prefixes  */
+    int nshot;
+    float offset_min, offset_max;                          /* metres, relative to the source     */
+    float sx0, sz0, rz0;                                   /* first source x, source and receiver depth (m) */
+    float dsx;                                             /* shot spacing (m)                   */
+    int nx, nz;                                            /* model size (cells)                 */
+    float dx, dz;
+    int nt;                                                /* record length (samples)            */
+    float dt, f0;
+    float pml_xn, pml_xp, pml_zn, pml_zp;                  /* sponge thickness (m)               */
+    int fdo2, fdo1;
+} sfd_qpar;
+int sfd_qpar_read(const char* path, sfd_qpar* out);
+/* Raw little-endian float32 files: models (x-major, z fastest: QS:238-284, tools/get_vel_model.cpp:
+ * 50-58), AFD's record / snapshot outputs (AFD:343-393).  append = 1 opens for appending. */
+int sfd_read_floats(const char* path, long long n, float* out);
+int sfd_write_floats(const char* path, const float* data, long long n, int append);
+/* One shot's SU file (QS:1476-1546): per trace a 240-byte SEG-Y header with fldr = shot_no,
+ * trid = 1, sx = (isx - 1) dx, gx = (ixmin - 2 + i) dx for trace i = 1..ntr, offset = gx - sx,
+ * cdp = nint((gx + sx) / dx) + 1, ns = nt, dt in microseconds (integer conversions as in the
+ * Fortran), followed by the trace's nt float32 samples.  traces: [ntr][nt]. */
+int sfd_su_write(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
+                 float dt);
+/* Concatenate per-shot SU files in order (QS:1550-1624); delete_inputs = 1 removes them as the
+ * reference does. */
+int sfd_su_merge(const char* out_path, const char* const* in_paths, int n, int delete_inputs);
 
 #ifdef __cplusplus
 }

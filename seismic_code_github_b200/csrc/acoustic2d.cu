@@ -222,6 +222,7 @@ acoustic2d_step_kernel(const __grid_constant__ Acou2DArgs a) {
         if (gx < nx && gz < nz) {
             float pw = pn;
             if (gx == sd.sx && gz == sd.sz && step + 1 < sd.nt) {
+                if (a.src_pre) a.src_pre[shot] = pn;
                 const float w = __ldg(a.wavelets + sd.wav_off + step + 1);
                 pw = EXACT ? __fsub_rn(pn, __fmul_rn(sd.inj_scale, w)) : pn - sd.inj_scale * w;
             }

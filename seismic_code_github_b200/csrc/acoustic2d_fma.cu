@@ -389,7 +389,10 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                     const float inj = sd.inj_scale * __ldg(a.wavelets + sd.wav_off + step + 1);
 #pragma unroll
                     for (int c = 0; c < 4; c++)
-                        if (sd.sz == gz + c) pn[c] -= inj;
+                        if (sd.sz == gz + c) {
+                            if (a.src_pre) a.src_pre[shot] = pn[c];
+                            pn[c] -= inj;
+                        }
                 }
                 const long long c = cell(gx, gz);
                 const float4 vzc = make_float4(cmp2(vz[T::OFFC], h), cmp2(vz[T::OFFC + 1], h),

@@ -83,11 +83,27 @@ struct sfd_ctx {
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
 
+    // wavefield snapshot streams (sfd_set_snapshots)
+    struct Snap {
+        int field = 0, first = 0, every = 1, count = 0;
+        float* d_buf = nullptr;
+        long long* d_off = nullptr;       // per shot offset (floats) into d_buf
+        std::vector<long long> off;
+        std::vector<int> taken;           // snapshots per shot
+        long long total = 0;
+        bool ready = false;               // filled by the last forward
+    };
+    Snap snaps[4];
+    float* d_src_pre = nullptr;           // per shot: P at the source before the next injection
+
     // viscoacoustic scheme: prepared model (QS:434-551), sponge tables, source stamps
     float* q_busg = nullptr;
     float* q_p1 = nullptr;
     float* q_p2 = nullptr;
     float q_rtau = 0.0f;
+    std::vector<float> h_q;        // quality factors as given (empty: Q = 1e5)
+    std::vector<int> h_ap_x0;      // each shot's aperture start in the model as given
+    int q_width = 0;               // columns of the prepared model (one block per shot window)
     float* d_spg = nullptr;
     int spg_stride = 0;
     float* d_stamps = nullptr;
@@ -201,7 +217,13 @@ float sponge3(const sfd_grid& g, int x, int y, int z) {
 void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
     dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri); dfree(c->d_rec_y);
-    dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps);
+    dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps); dfree(c->d_src_pre);
+    for (auto& sn : c->snaps) {
+        dfree(sn.d_buf);
+        dfree(sn.d_off);
+        sn.ready = false;
+        sn.total = 0;
+    }
     if (c->graph) cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
     c->graph_valid = false;
@@ -277,6 +299,8 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.tm_vz = c->tmaps[4 + i];
     a.err_flag = c->d_err;
     a.step = step;
+    for (const auto& sn : c->snaps)
+        if (sn.count > 0 && sn.field == SFD_FIELD_P) a.src_pre = c->d_src_pre;
     return a;
 }
 
@@ -329,7 +353,7 @@ QArgs make_qargs(const sfd_ctx* c, int step) {
     a.p1 = c->q_p1 + kModelGhostZ;
     a.p2 = c->q_p2 + kModelGhostZ;
     a.mpitch = c->mpitch;
-    a.nx_model = c->g.nx;
+    a.nx_model = c->q_width;
     a.dt = c->g.dt;
     a.f_mem = c->g.dt * (-1.0f * c->q_rtau);  // QS:1160 dt*(-1.0*rtaustss)
     a.hx = 0.5f / c->g.dx;
@@ -351,6 +375,83 @@ QArgs make_qargs(const sfd_ctx* c, int step) {
     a.records = c->d_rec_tn;
     a.step = step;
     return a;
+}
+
+// Size the snapshot buffers for the current shot set; returns true if a buffer moved (the
+// captured time loop holds their addresses).
+bool snap_prepare(sfd_ctx* ctx, int* rc) {
+    *rc = SFD_OK;
+    bool moved = false;
+    const int pml = ctx->g.pml, nzi = ctx->g.nz - 2 * pml;
+    for (auto& sn : ctx->snaps) {
+        sn.ready = false;
+        if (sn.count <= 0) continue;
+        sn.off.assign(ctx->nshot, 0);
+        sn.taken.assign(ctx->nshot, 0);
+        long long total = 0;
+        for (int s = 0; s < ctx->nshot; s++) {
+            const ShotDev& d = ctx->h_shots[s];
+            const int t = d.nt > sn.first ? std::min(sn.count, (d.nt - 1 - sn.first) / sn.every + 1) : 0;
+            sn.taken[s] = t;
+            sn.off[s] = total;
+            total += (long long)t * (d.nx - 2 * pml) * nzi;
+        }
+        if (!sn.d_buf || total != sn.total) {
+            dfree(sn.d_buf);
+            dfree(sn.d_off);
+            if (cudaMalloc(&sn.d_buf, sizeof(float) * std::max<long long>(total, 1)) != cudaSuccess ||
+                cudaMalloc(&sn.d_off, sizeof(long long) * ctx->nshot) != cudaSuccess) {
+                cudaGetLastError();
+                *rc = set_err(ctx, SFD_ERR_NOMEM, "snapshot buffer of %lld floats", total);
+                return true;
+            }
+            moved = true;
+        }
+        sn.total = total;
+        if (cudaMemcpy(sn.d_off, sn.off.data(), sizeof(long long) * ctx->nshot, cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+            *rc = set_err(ctx, SFD_ERR_CUDA, "snapshot offsets upload");
+            return true;
+        }
+    }
+    return moved;
+}
+
+// Snapshots due after step k for the shots in slots[0 .. act).
+int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* launches) {
+    for (auto& sn : ctx->snaps) {
+        if (sn.count <= 0 || k < sn.first || (k - sn.first) % sn.every != 0) continue;
+        const int j = (k - sn.first) / sn.every;
+        if (j >= sn.count) continue;
+        SnapArgs s{};
+        const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+        const float* F = ctx->d_state;
+        if (ctx->g.scheme == SFD_VISCOAC_2D) {
+            const int f0 = sn.field == SFD_FIELD_VX ? 0 : sn.field == SFD_FIELD_VZ ? 1 : sn.field == SFD_FIELD_P ? 2 : 5;
+            s.nsum = (sn.field == SFD_FIELD_P || sn.field == SFD_FIELD_R) ? 3 : 1;
+            for (int i = 0; i < s.nsum; i++) s.f[i] = F + (f0 + i) * fs;
+        } else {
+            const int o = (k + 1) & 1;  // buffer written by step k
+            const int f0 = sn.field == SFD_FIELD_P ? 0 : sn.field == SFD_FIELD_VX ? 2 : 4;
+            s.nsum = 1;
+            s.f[0] = F + (f0 + o) * fs;
+            if (sn.field == SFD_FIELD_P) s.src_pre = ctx->d_src_pre;
+        }
+        s.L = ctx->L;
+        s.nz = ctx->g.nz;
+        s.pml = ctx->g.pml;
+        s.shots = ctx->d_shots;
+        s.slot_to_shot = slots;
+        s.step = k;
+        s.index = j;
+        s.out = sn.d_buf;
+        s.shot_off = sn.d_off;
+        int nx_max = 0;
+        for (const auto& d : ctx->h_shots) nx_max = std::max(nx_max, d.nx);
+        CK(launch_snapshot(s, act, nx_max, ctx->stream));
+        *launches += 1;
+    }
+    return SFD_OK;
 }
 
 int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* launches) {
@@ -395,8 +496,8 @@ int enqueue_loop(sfd_ctx* ctx, long long* launches) {
     for (int k = 0; k < ctx->nt_max; k++) {
         const int act = active_shots(ctx, k);
         if (act == 0) break;
-        const int rc = launch_one_step(ctx, k, ctx->d_slot, act, launches);
-        if (rc) return rc;
+        int rc = launch_one_step(ctx, k, ctx->d_slot, act, launches);
+        if (rc || (rc = snap_after_step(ctx, k, ctx->d_slot, act, launches))) return rc;
     }
     return SFD_OK;
 }
@@ -474,6 +575,8 @@ int kernel_variant(const sfd_ctx* ctx) {
 int run_forward(sfd_ctx* ctx, float* out_dev) {
     int rc;
     long long launches = 0;
+    if (snap_prepare(ctx, &rc)) ctx->graph_valid = false;
+    if (rc) return rc;
     if (!ctx->graph_valid) {
         if ((rc = tune_schedule(ctx)) != SFD_OK) return rc;
         cudaGraph_t g = nullptr;
@@ -492,6 +595,10 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
         ctx->graph_valid = true;
     } else {
         for (int k = 0; k < ctx->nt_max && active_shots(ctx, k) > 0; k++) launches++;
+        for (const auto& sn : ctx->snaps)
+            for (int k = sn.first; sn.count > 0 && k < ctx->nt_max && (k - sn.first) / sn.every < sn.count;
+                 k += sn.every)
+                launches++;
     }
     CK(cudaEventRecord(ctx->evs, ctx->stream));
     if ((rc = prologue(ctx)) != SFD_OK) return rc;
@@ -508,6 +615,7 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
     ctx->timing.device_ms = dms;
     ctx->timing.launches = launches + 2 + ((ctx->g.flags & SFD_NAN_CHECK) ? 1 : 0);
     ctx->timing.graph = 1;
+    for (auto& sn : ctx->snaps) sn.ready = sn.count > 0;
     ctx->timing.kernel_variant = kernel_variant(ctx);
     double pts = 0;
     for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.ny * ctx->g.nz * s.nt;
@@ -779,6 +887,69 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     return SFD_OK;
 }
 
+// Viscoacoustic model preparation, QS:434-551 (averaged density -> buoyancy, Lame and Blanch
+// tau), done per shot window as QS does for each shot's padded grid: the 2 x 2 density average
+// and its edge rule stop at the window's last row and column.  Every distinct window (aperture
+// start and width) gets its own block of the prepared arrays; shot x0 becomes that block's start.
+// Without shots the whole grid is one window.
+int q_prepare(sfd_ctx* ctx) {
+    if (ctx->g.scheme != SFD_VISCOAC_2D || !ctx->have_model) return SFD_OK;
+    const int nz = ctx->g.nz;
+    std::vector<std::pair<int, int>> wins;  // (x0, nx)
+    std::vector<int> blk(ctx->have_shots ? ctx->nshot : 0);
+    if (ctx->have_shots) {
+        for (int s = 0; s < ctx->nshot; s++) {
+            const std::pair<int, int> w(ctx->h_ap_x0[s], ctx->h_shots[s].nx);
+            auto it = std::find(wins.begin(), wins.end(), w);
+            blk[s] = (int)(it - wins.begin());
+            if (it == wins.end()) wins.push_back(w);
+        }
+    } else {
+        wins.emplace_back(0, ctx->g.nx);
+    }
+    int width = 0;
+    std::vector<int> start(wins.size());
+    for (size_t b = 0; b < wins.size(); b++) {
+        start[b] = width;
+        width += wins[b].second;
+    }
+    std::vector<float> busg((size_t)width * nz), p1((size_t)width * nz), p2((size_t)width * nz);
+    for (size_t b = 0; b < wins.size(); b++) {
+        const size_t off = (size_t)wins[b].first * nz, len = (size_t)wins[b].second * nz;
+        std::vector<float> rho(len, ctx->den_c);
+        if (!ctx->h_den.empty()) rho.assign(ctx->h_den.begin() + off, ctx->h_den.begin() + off + len);
+        const float* qw = ctx->h_q.empty() ? nullptr : ctx->h_q.data() + off;
+        viscoac2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, rho.data(), qw, ctx->g.f0,
+                          busg.data() + (size_t)start[b] * nz, p1.data() + (size_t)start[b] * nz,
+                          p2.data() + (size_t)start[b] * nz, &ctx->q_rtau);
+    }
+    // upload with kModelGhostZ replicated rows (the layout of the other model arrays)
+    const size_t mfloats = (size_t)width * ctx->mpitch;
+    auto upload = [&](float** dst, const std::vector<float>& src) -> int {
+        std::vector<float> staged(mfloats);
+        for (int c = 0; c < width; c++)
+            for (int k = 0; k < ctx->mpitch; k++)
+                staged[(size_t)c * ctx->mpitch + k] = src[(size_t)c * nz + std::min(std::max(k - kModelGhostZ, 0), nz - 1)];
+        if (width != ctx->q_width) {
+            dfree(*dst);
+            ctx->graph_valid = false;
+        }
+        if (!*dst) CK(cudaMalloc(dst, mfloats * sizeof(float)));
+        CK(cudaMemcpy(*dst, staged.data(), mfloats * sizeof(float), cudaMemcpyHostToDevice));
+        return SFD_OK;
+    };
+    int rc;
+    if ((rc = upload(&ctx->q_busg, busg)) || (rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2)))
+        return rc;
+    if (width != ctx->q_width) ctx->graph_valid = false;
+    ctx->q_width = width;
+    if (ctx->have_shots) {
+        for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
+        CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
+    }
+    return SFD_OK;
+}
+
 // sfd_set_shots for the 3-D scheme: every shot covers the whole grid (no aperture windows);
 // sources must lie where the step updates P (R <= coordinate < n - R on every axis).
 int set_shots_3d(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
@@ -1039,21 +1210,18 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
                 if (!(q[i] > 0.0f) || !std::isfinite(q[i]))
                     return set_err(ctx, SFD_ERR_ARG, "q[%zu] = %g is not a positive finite quality factor", i,
                                    (double)q[i]);
-        std::vector<float> rho(n, 2400.0f), busg(n), p1(n), p2(n);
-        if (den) rho.assign(den, den + n);
-        viscoac2d_prepare(ctx->g.nx, nz, vp, rho.data(), q, ctx->g.f0, busg.data(), p1.data(), p2.data(),
-                          &ctx->q_rtau);
-        if ((urc = upload(&ctx->q_busg, busg.data())) || (urc = upload(&ctx->q_p1, p1.data())) ||
-            (urc = upload(&ctx->q_p2, p2.data())))
-            return urc;
+        if (q) ctx->h_q.assign(q, q + n);
+        else ctx->h_q.clear();
+        ctx->have_model = true;
+        if ((urc = q_prepare(ctx))) return urc;
     }
     if (ctx->varden != varden_old || (!ctx->varden && ctx->den_c != den_c_old)) {
         ctx->graph_valid = false;
         ctx->grad_valid = false;
     }
     ctx->have_model = true;
-    // source scale factors depend on the model
-    if (ctx->have_shots) {
+    // source scale factors depend on the model (the viscoacoustic source is a stamp)
+    if (ctx->have_shots && ctx->g.scheme != SFD_VISCOAC_2D) {
         for (auto& s : ctx->h_shots) {
             const size_t mi = ((size_t)(s.x0 + s.sx) * ctx->g.ny + s.sy) * ctx->g.nz + s.sz;
             const float d = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
@@ -1186,6 +1354,7 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
     ctx->state_floats = (visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
+    CK(cudaMalloc(&ctx->d_src_pre, sizeof(float) * nshot));
     if (visco) {
         // Gaussian source stamps (QS:1340-1444) and the split cosine sponge tables (QS:555-605)
         std::vector<float> stamps;
@@ -1216,8 +1385,11 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
             if (rc2) return rc2;
         }
     }
+    ctx->h_ap_x0.resize(nshot);
+    for (int s = 0; s < nshot; s++) ctx->h_ap_x0[s] = shots[s].ap_x0;
     ctx->have_shots = true;
     ctx->graph_valid = false;
+    if (visco) return q_prepare(ctx);
     return SFD_OK;
 }
 
@@ -1254,9 +1426,14 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
     if ((rc = prologue(ctx)) != SFD_OK) return rc;
     long long launches = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    snap_prepare(ctx, &rc);
+    if (rc) return rc;
     for (int s = 0; s < ctx->nshot; s++)
         for (int k = 0; k < ctx->h_shots[s].nt; k++)
-            if ((rc = launch_one_step(ctx, k, ctx->d_ident + s, 1, &launches))) return rc;
+            if ((rc = launch_one_step(ctx, k, ctx->d_ident + s, 1, &launches)) ||
+                (rc = snap_after_step(ctx, k, ctx->d_ident + s, 1, &launches)))
+                return rc;
+    for (auto& sn : ctx->snaps) sn.ready = sn.count > 0;
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     if ((rc = epilogue(ctx, ctx->d_rec_nt)) != SFD_OK) return rc;
     CK(cudaEventRecord(ctx->eve, ctx->stream));
@@ -1370,6 +1547,39 @@ int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out) {
     const ShotDev& sd = ctx->h_shots[shot];
     CK(cudaMemcpy(out, ctx->d_lam + (size_t)shot * ctx->nt_max, sizeof(float) * sd.nt, cudaMemcpyDeviceToHost));
     for (int j = 0; j < sd.nt; j++) out[j] = -sd.inj_scale * out[j];  // d misfit / d w[j] = -s lambda_j[src]
+    return SFD_OK;
+}
+
+int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int count) {
+    if (!ctx || id < 0 || id >= 4 || count < 0 || first < 0 || (count > 0 && every < 1)) return SFD_ERR_ARG;
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D && count > 0)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "snapshots are taken for the 2-D schemes");
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    if (count > 0 && field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ &&
+        !(visco && field == SFD_FIELD_R))
+        return set_err(ctx, SFD_ERR_ARG, "field %d cannot be recorded for this scheme", field);
+    auto& sn = ctx->snaps[id];
+    sn.field = field;
+    sn.first = first;
+    sn.every = every < 1 ? 1 : every;
+    sn.count = count;
+    sn.ready = false;
+    ctx->graph_valid = false;
+    return SFD_OK;
+}
+
+int sfd_get_snapshots(sfd_ctx* ctx, int id, int shot, float* out, int* n_out) {
+    if (!ctx || id < 0 || id >= 4) return SFD_ERR_ARG;
+    const auto& sn = ctx->snaps[id];
+    if (!sn.ready) return set_err(ctx, SFD_ERR_STATE, "snapshot stream %d has not been filled by a forward", id);
+    if (shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
+    if (n_out) *n_out = sn.taken[shot];
+    if (out && sn.taken[shot] > 0) {
+        CK(cudaSetDevice(ctx->device));
+        const long long n =
+            (long long)sn.taken[shot] * (ctx->h_shots[shot].nx - 2 * ctx->g.pml) * (ctx->g.nz - 2 * ctx->g.pml);
+        CK(cudaMemcpy(out, sn.d_buf + sn.off[shot], sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
     return SFD_OK;
 }
 

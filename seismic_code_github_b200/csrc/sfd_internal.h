@@ -114,6 +114,8 @@ struct Acou2DArgs {
     float* records;            // [nt][nrec] per shot at ShotDev::rec_base
     int step;
     float* div_out;            // optional: D = rdx S-x Vx + rdz S-z Vz of this step (field layout)
+    float* src_pre;            // optional, per shot: P at the source cell before the next step's
+                               // injection (the value AFD holds there after the sponge)
 };
 
 // Arguments of the adjoint step kernel (adjoint2d.cu); field buffers share Layout2D.
@@ -181,6 +183,21 @@ cudaError_t acoustic2d_launch_inject0(const Acou2DArgs& a, int nshot, bool exact
 cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const ShotDev* shots, int nshot,
                                      int nrec_max, int nt_max, cudaStream_t st);
 cudaError_t launch_nan_scan(const float* rec, long long n, int* flag, cudaStream_t st);
+
+// ---- wavefield snapshots (snapshots.cu) ----
+struct SnapArgs {
+    const float* f[3];          // field slabs (nsum = 3: summed in order, the viscoacoustic sigma / r)
+    int nsum;
+    Layout2D L;
+    int nz, pml;
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* src_pre;       // acoustic P: value at the source cell before the next injection
+    int step, index;            // step just completed, snapshot number
+    float* out;                 // per shot at shot_off[shot]: [snapshot][nx_shot - 2 pml][nz - 2 pml]
+    const long long* shot_off;
+};
+cudaError_t launch_snapshot(const SnapArgs& a, int active, int nx_max, cudaStream_t st);
 
 // ---- 3-D acoustic scheme (acoustic3d.cu) ----
 // Field storage: per shot a dense [x][y][pitch] block, z fastest, pitch = nz rounded up to a

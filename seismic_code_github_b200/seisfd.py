@@ -33,6 +33,39 @@ class Shot(ctypes.Structure):
                 ("wavelet", _F32P), ("ap_x0", ctypes.c_int), ("ap_nx", ctypes.c_int)]
 
 
+class QPar(ctypes.Structure):
+    """sfd_qpar: the Q_forward parameter card."""
+    _fields_ = [(n, ctypes.c_char * 256) for n in ("vp", "vs", "rho", "qp", "qs", "shot1", "shot2", "shot3", "shot4")] + \
+               [("nshot", ctypes.c_int), ("offset_min", ctypes.c_float), ("offset_max", ctypes.c_float),
+                ("sx0", ctypes.c_float), ("sz0", ctypes.c_float), ("rz0", ctypes.c_float), ("dsx", ctypes.c_float),
+                ("nx", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
+                ("nt", ctypes.c_int), ("dt", ctypes.c_float), ("f0", ctypes.c_float),
+                ("pml_xn", ctypes.c_float), ("pml_xp", ctypes.c_float), ("pml_zn", ctypes.c_float),
+                ("pml_zp", ctypes.c_float), ("fdo2", ctypes.c_int), ("fdo1", ctypes.c_int)]
+
+
+def read_qpar(path: str) -> QPar:
+    p = QPar()
+    rc = load().sfd_qpar_read(path.encode(), ctypes.byref(p))
+    if rc:
+        raise SfdError(rc, f"sfd_qpar_read({path})")
+    return p
+
+
+def su_write(path: str, traces: np.ndarray, shot_no: int, isx: int, ixmin: int, dx: float, dt: float):
+    tr = np.ascontiguousarray(traces, np.float32)
+    rc = load().sfd_su_write(path.encode(), _fp(tr), tr.shape[0], tr.shape[1], shot_no, isx, ixmin, dx, dt)
+    if rc:
+        raise SfdError(rc, f"sfd_su_write({path})")
+
+
+def su_merge(out_path: str, parts: Sequence[str], delete_inputs: bool = True):
+    arr = (ctypes.c_char_p * len(parts))(*[p.encode() for p in parts])
+    rc = load().sfd_su_merge(out_path.encode(), arr, len(parts), 1 if delete_inputs else 0)
+    if rc:
+        raise SfdError(rc, f"sfd_su_merge({out_path})")
+
+
 class Timing(ctypes.Structure):
     _fields_ = [("loop_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("point_updates", ctypes.c_double),
                 ("launches", ctypes.c_longlong), ("h2d_bytes", ctypes.c_longlong), ("d2h_bytes", ctypes.c_longlong),
@@ -57,9 +90,19 @@ SIGNATURES = {
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
+    "sfd_set_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int]),
+    "sfd_get_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _F32P,
+                                         ctypes.POINTER(ctypes.c_int)]),
     "sfd_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(Grid), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I32P, _I32P,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "sfd_qpar_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p]),
+    "sfd_read_floats": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong, _F32P]),
+    "sfd_write_floats": (ctypes.c_int, [ctypes.c_char_p, _F32P, ctypes.c_longlong, ctypes.c_int]),
+    "sfd_su_write": (ctypes.c_int, [ctypes.c_char_p, _F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_float, ctypes.c_float]),
+    "sfd_su_merge": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int]),
     "sfd_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _F32P]),
     "sfd_afd_sponge": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P]),
     "sfd_fd_coeffs": (ctypes.c_int, [ctypes.c_int, _F32P]),
@@ -263,6 +306,19 @@ class Engine:
 
     def set_checkpoint_interval(self, steps: int):
         self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
+
+    def set_snapshots(self, stream: int, field: int, first: int, every: int, count: int):
+        self._check(self._lib.sfd_set_snapshots(self._h, stream, field, first, every, count), "sfd_set_snapshots")
+
+    def snapshots(self, stream: int, shot: int) -> np.ndarray:
+        """(n, nx_shot - 2 pml, nz - 2 pml) interior snapshots of one shot from the last forward."""
+        n = ctypes.c_int()
+        self._check(self._lib.sfd_get_snapshots(self._h, stream, shot, None, ctypes.byref(n)), "sfd_get_snapshots")
+        s = self._shots[shot]
+        nx = (s.ap_nx if s.ap_nx > 0 else self.grid.nx) - 2 * self.grid.pml
+        out = np.empty((n.value, nx, self.grid.nz - 2 * self.grid.pml), np.float32)
+        self._check(self._lib.sfd_get_snapshots(self._h, stream, shot, _fp(out), ctypes.byref(n)), "sfd_get_snapshots")
+        return out
 
     def timing(self) -> dict:
         t = Timing()

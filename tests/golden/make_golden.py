@@ -11,6 +11,9 @@ reference tree and the builds of oracle/ref_build.py; the GPU tests only read th
         seismic_code_github_b200.workloads.config1(): 251 traces x 1000 samples.
   small_varden_record.f32  same for workloads.small_varden(): non-square grid, variable
         density, off-centre source (80 traces x 300 samples).
+  afd_small/{record,Snap,Model,Pall}.dat  the patched reference with its own constant model and
+        28 Hz wavelet on NX=NZ=40, PML=10, Nt=150, dt=1 ms, Snapshot at step 100 and the
+        every-10-steps Pall.dat switched on: the outputs of the afd_fd program are pinned to it.
   manifest.json      sizes and sha256 of the above.
 
 Usage: python tests/golden/make_golden.py [--reference /root/reference]
@@ -80,6 +83,18 @@ def main():
         res = ref_runner.run(ref_config(case, w))
         res["record"].astype(np.float32).tofile(os.path.join(HERE, fn))
         out[fn] = {"case": case.name, "wall_s": round(res["wall_s"], 3)}
+
+    small = ref_runner.AfdRefConfig(NX=40, NZ=40, PML=10, Nt=150, dt=0.001, snap=100, pall=True)
+    d = os.path.join(HERE, "afd_small")
+    os.makedirs(d, exist_ok=True)
+    work = tempfile.mkdtemp()
+    try:
+        ref_runner.run(small, keep=work)
+        for f in ("record.dat", "Snap.dat", "Model.dat", "Pall.dat"):
+            shutil.copyfile(os.path.join(work, "file", f), os.path.join(d, f))
+            out[f"afd_small/{f}"] = {"case": "NX=NZ=40 PML=10 Nt=150 dt=1ms snap=100 pall"}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
 
     manifest = {}
     for k, meta in out.items():

@@ -1,0 +1,163 @@
+"""GPU checks of the file-contract programs and of the in-loop snapshots.
+
+  * afd_fd with no options writes the reference's own record.dat / Snap.dat / Model.dat
+    (forward/Acoustic_FD_by_ss/file/) bit for bit; on a reduced grid with Pall.dat switched on
+    it matches the patched reference build (fixture tests/golden/afd_small) file for file.
+  * q_forward on a parameter card of three aperture shots writes merged SU files whose traces
+    equal the FP32 restatement of Q_forward per shot (bit for bit) and whose headers follow
+    QS:1502-1533; the per-shot parts are deleted as in QS:1582.
+  * sfd_set_snapshots: each recorded interior equals the wavefield of a run stopped after that
+    step (both schemes, batched and per-shot paths).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from conftest import GOLDEN, ROOT, bits_equal, rel_l2
+from seismic_code_github_b200 import seisfd as S
+from seismic_code_github_b200 import workloads as W
+from test_fileio import CARD, expected_header
+
+pytestmark = pytest.mark.gpu
+BIN = os.path.join(ROOT, "seismic_code_github_b200", "bin")
+
+
+def run(cmd, cwd):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+def read(path, shape=None):
+    a = np.fromfile(path, np.float32)
+    return a if shape is None else a.reshape(shape)
+
+
+def test_afd_fd_default_reproduces_the_shipped_outputs(tmp_path):
+    (tmp_path / "file").mkdir()
+    (tmp_path / "bin").mkdir()
+    run([os.path.join(BIN, "afd_fd")], cwd=tmp_path / "bin")  # writes ../file like the reference
+    for f in ("record.dat", "Snap.dat", "Model.dat"):
+        got, ref = read(tmp_path / "file" / f), read(os.path.join(GOLDEN, "afd_default", f))
+        assert bits_equal(got, ref), f
+    assert read(tmp_path / "file" / "Pall.dat").size == 200 * 100 * 100
+
+
+def test_afd_fd_small_case_with_pall_matches_the_reference_build(tmp_path):
+    run([os.path.join(BIN, "afd_fd"), "--nx", "40", "--nz", "40", "--pml", "10", "--nt", "150", "--dt", "0.001",
+         "--snap", "100", "--out", str(tmp_path)], cwd=tmp_path)
+    for f in ("record.dat", "Snap.dat", "Model.dat", "Pall.dat"):
+        got, ref = read(tmp_path / f), read(os.path.join(GOLDEN, "afd_small", f))
+        assert got.shape == ref.shape and bits_equal(got, ref), f
+
+
+def test_afd_fd_fast_path_within_tolerance(tmp_path):
+    run([os.path.join(BIN, "afd_fd"), "--fast", "--out", str(tmp_path), "--pall-every", "0"], cwd=tmp_path)
+    got, ref = read(tmp_path / "record.dat"), read(os.path.join(GOLDEN, "afd_default", "record.dat"))
+    assert rel_l2(got, ref) <= 1e-5
+    assert not (tmp_path / "Pall.dat").exists()
+
+
+def qcard_case(tmp_path):
+    nx, nz = 120, 80
+    rng = np.random.default_rng(11)
+    z = np.arange(nz)
+    vp = np.tile(np.where(z < 40, 2000.0, 2600.0), (nx, 1)).astype(np.float32)
+    vp += rng.uniform(-50, 50, vp.shape).astype(np.float32)
+    rho = (2000.0 + 300.0 * rng.random((nx, nz))).astype(np.float32)
+    qp = (30.0 + 150.0 * rng.random((nx, nz))).astype(np.float32)
+    for name, a in (("vp", vp), ("vs", vp * 0), ("rho", rho), ("qp", qp), ("qs", qp)):
+        a.tofile(tmp_path / f"{name}.bin")
+    card = CARD.format(d=str(tmp_path)).replace("0.001\n", "0.0005\n").replace("500\n!*dt", "400\n!*dt")
+    (tmp_path / "card.par").write_text(card)
+    return S.read_qpar(str(tmp_path / "card.par")), vp, rho, qp
+
+
+@pytest.mark.parametrize("use_q", [False, True])
+def test_q_forward_program_against_restatement(tmp_path, use_q):
+    p, vp, rho, qp = qcard_case(tmp_path)
+    assert p.nt == 400 and np.float32(p.dt) == np.float32(0.0005)
+    cmd = [os.path.join(BIN, "q_forward"), str(tmp_path / "card.par")] + (["--use-q"] if use_q else [])
+    run(cmd, cwd=tmp_path)
+    nint = lambda v: int(np.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
+    np_ = nint(p.pml_xn / p.dx) + 1
+    isx0, nsz0, nrz0 = nint(p.sx0 / p.dx) + 1, nint(p.sz0 / p.dz) + 1, nint(p.rz0 / p.dz) + 1
+    for stem in ("pz", "px"):
+        assert not (tmp_path / f"{stem}_tmp1.su").exists()
+        raw = open(tmp_path / f"shot_{stem}.su", "rb").read()
+        off = 0
+        for i in range(1, p.nshot + 1):
+            isx = isx0 + nint((i - 1) * p.dsx / p.dx)
+            ixmine, ixmaxe = isx + nint(p.offset_min / p.dx), isx + nint(p.offset_max / p.dx)
+            nxe = ixmaxe - ixmine + 1
+            r1, r2, _ = ol.q_forward(vp, vp * 0, rho, qp, qp, p.dx, p.dz, p.dt, p.f0, p.nt, np_, np_,
+                                     isx - ixmine + np_ + 1, nsz0 + np_ + 1, nrz0=nrz0, ixmine=ixmine,
+                                     ixmaxe=ixmaxe, q_override=not use_q)
+            ref = r1 if stem == "pz" else r2
+            for t in range(nxe):
+                rec = raw[off:off + 240 + 4 * p.nt]
+                off += 240 + 4 * p.nt
+                assert rec[:240] == expected_header(i, isx, ixmine, p.dx, p.dt, p.nt, t + 1)
+                assert bits_equal(np.frombuffer(rec[240:], np.float32), ref[t]), (stem, i, t)
+        assert off == len(raw)
+
+
+def test_snapshots_equal_truncated_runs_acoustic():
+    case = W.small_varden()
+    rx, rz = case.receivers()
+    w = S.wavelet(S.WAVELET_RIC, 60, case.dt, 20.0, 20)
+    shots = [S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w),
+             S.ShotSpec(case.src_x[0] + 9, case.src_z[0] - 5, rx, rz, w[:45])]
+    pml = case.PML
+    with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, pml, flags=S.EXACT) as e:
+        e.set_model(case.vp, case.den)
+        e.set_shots(shots)
+        e.set_snapshots(0, S.FIELD_P, 3, 7, 6)
+        e.set_snapshots(1, S.FIELD_VX, 10, 20, 3)
+        e.forward()
+        got = [[e.snapshots(sid, s) for s in range(2)] for sid in range(2)]
+        e.forward_per_shot()
+        per = [[e.snapshots(sid, s) for s in range(2)] for sid in range(2)]
+    assert [g.shape[0] for g in got[0]] == [6, 6] and [g.shape[0] for g in got[1]] == [3, 2]
+    for a, b in zip(sum(got, []), sum(per, [])):
+        assert bits_equal(a, b)
+    for sid, field, first, every in ((0, S.FIELD_P, 3, 7), (1, S.FIELD_VX, 10, 20)):
+        for s in range(2):
+            for j, snap in enumerate(got[sid][s]):
+                k = first + j * every
+                with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, pml, flags=S.EXACT) as e:
+                    e.set_model(case.vp, case.den)
+                    sh = shots[s]
+                    e.set_shots([S.ShotSpec(sh.sx, sh.sz, rx, rz, sh.wavelet[:k + 1])])
+                    e.forward()
+                    full = e.wavefield(0, field)
+                assert bits_equal(snap, full[pml:-pml, pml:-pml]), (sid, s, k)
+
+
+def test_snapshots_equal_truncated_runs_viscoacoustic():
+    rng = np.random.default_rng(3)
+    npx, f0, dt, dx = 8, 20.0, 5e-4, 10.0
+    vp = S.pad_model((2000 + 300 * rng.random((40, 36))).astype(np.float32), npx, npx, npx, npx)
+    rho = np.full_like(vp, 2100.0)
+    q = S.pad_model((40 + 100 * rng.random((40, 36))).astype(np.float32), npx, npx, npx, npx)
+    r = np.arange(npx, vp.shape[0] - npx, dtype=np.int32)
+    w = S.wavelet(S.WAVELET_Q, 90, dt, f0)
+    with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0) as e:
+        e.set_model(vp, rho, q)
+        e.set_shots([S.ShotSpec(20, 12, r, np.full_like(r, 10), w)])
+        e.set_snapshots(2, S.FIELD_P, 9, 40, 3)
+        e.set_snapshots(3, S.FIELD_R, 49, 50, 1)
+        e.forward()
+        snaps = e.snapshots(2, 0), e.snapshots(3, 0)
+    for (sid, field, first, every), got in zip(((2, S.FIELD_P, 9, 40), (3, S.FIELD_R, 49, 50)), snaps):
+        for j, snap in enumerate(got):
+            k = first + j * every
+            with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0) as e:
+                e.set_model(vp, rho, q)
+                e.set_shots([S.ShotSpec(20, 12, r, np.full_like(r, 10), w[:k + 1])])
+                e.forward()
+                full = e.wavefield(0, field)
+            assert bits_equal(snap, full[npx:-npx, npx:-npx]), (field, k)
