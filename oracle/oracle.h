@@ -64,6 +64,19 @@ int oracle_afd3d_f32(const OracleAfd3Cfg* g, const float* vp, const float* den, 
                      float* final_p);
 int oracle_afd3d_f64(const OracleAfd3Cfg* g, const float* vp, const float* den, const float* wavelet, double* record,
                      double* final_p);
+// FP64 misfit gradient of the viscoacoustic (vs = 0) scheme on a padded grid (np sponge cells per
+// side, arrays x-major): records [nrec][nt], d/dvp and d/d(1/Q) per cell, d/dw per sample.
+typedef struct {
+    int nx, nz, np;
+    float dx, dz, dt, f0;
+    int nt, sx, sz;        // steps, source cell (0-based)
+    int nrec;
+    const int* rec_x;
+    const int* rec_z;
+} OracleQGradCfg;
+int oracle_q_gradient_f64(const OracleQGradCfg* c, const float* vp, const float* rho, const float* q,
+                          const float* wavelet, const float* obs, double* misfit, double* grad_vp,
+                          double* grad_invq, double* dw, double* records);
 void oracle_wavelet_afd(int nt, float dt, float freq, float* out);
 void oracle_wavelet_ric(int nt, float dt, int f0, int delay, float* out);
 

@@ -218,3 +218,41 @@ def afd3d_forward(vp, den, wavelet, src, rec_x, rec_y, rec_z, pml, dx, dy, dz, d
     if rc != 0:
         raise ValueError("oracle_afd3d rejected the configuration")
     return rec, fin
+
+
+class OracleQGradCfg(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("np", ctypes.c_int), ("dx", ctypes.c_float),
+                ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int),
+                ("sx", ctypes.c_int), ("sz", ctypes.c_int), ("nrec", ctypes.c_int), ("rec_x", _I32P),
+                ("rec_z", _I32P)]
+
+
+def q_gradient_f64(vp, rho, q, wavelet, src, rec_x, rec_z, np_, dx, dz, dt, f0, obs=None):
+    """FP64 viscoacoustic forward (+ gradient when obs is given) on the padded grid
+    (oracle/q_adj_oracle.cpp).  Returns dict(records, misfit, grad_vp, grad_invq, dw)."""
+    L = lib()
+    if not hasattr(L, "_qg_sig"):
+        L.oracle_q_gradient_f64.argtypes = [ctypes.POINTER(OracleQGradCfg), _F32P, _F32P, _F32P, _F32P, _F32P,
+                                            _F64P, _F64P, _F64P, _F64P, _F64P]
+        L._qg_sig = True
+    vp = np.ascontiguousarray(vp, np.float32)
+    nx, nz = vp.shape
+    rho = np.ascontiguousarray(rho, np.float32)
+    q = None if q is None else np.ascontiguousarray(q, np.float32)
+    w = np.ascontiguousarray(wavelet, np.float32)
+    rx, rz = np.ascontiguousarray(rec_x, np.int32), np.ascontiguousarray(rec_z, np.int32)
+    cfg = OracleQGradCfg(nx, nz, np_, dx, dz, dt, f0, len(w), src[0], src[1], len(rx), rx.ctypes.data_as(_I32P),
+                         rz.ctypes.data_as(_I32P))
+    rec = np.zeros((len(rx), len(w)), np.float64)
+    mis = np.zeros(1, np.float64)
+    g1 = np.zeros((nx, nz), np.float64) if obs is not None else None
+    g2 = np.zeros((nx, nz), np.float64) if obs is not None else None
+    dw = np.zeros(len(w), np.float64) if obs is not None else None
+    o = None if obs is None else np.ascontiguousarray(obs, np.float32)
+    rc = L.oracle_q_gradient_f64(ctypes.byref(cfg), _p(vp), _p(rho), None if q is None else _p(q), _p(w),
+                                 None if o is None else _p(o), _p(mis, _F64P), None if g1 is None else _p(g1, _F64P),
+                                 None if g2 is None else _p(g2, _F64P), None if dw is None else _p(dw, _F64P),
+                                 _p(rec, _F64P))
+    if rc:
+        raise ValueError(f"oracle_q_gradient_f64 rejected the configuration (rc={rc})")
+    return {"records": rec, "misfit": float(mis[0]), "grad_vp": g1, "grad_invq": g2, "dw": dw}
