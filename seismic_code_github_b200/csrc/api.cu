@@ -122,6 +122,8 @@ struct sfd_ctx {
     float* d_lam = nullptr;     // [nshot][nt_max] adjoint of P at the source cell
     double* d_misfit = nullptr;
     double* d_grad = nullptr;   // gradient on the model grid (double)
+    double* d_grad2 = nullptr;  // viscoacoustic: d misfit / d (1/Q) on the model grid
+    int* d_apx0 = nullptr;      // viscoacoustic: each shot's aperture start in the model
     cudaGraphExec_t grad_graph = nullptr;
     bool grad_valid = false;
     bool have_grad = false;
@@ -229,7 +231,7 @@ void free_shot_buffers(sfd_ctx* c) {
     c->graph_valid = false;
     dfree(c->d_ckpt); dfree(c->d_div); dfree(c->d_adj); dfree(c->d_gseg); dfree(c->d_gacc);
     dfree(c->d_obs_nt); dfree(c->d_obs_tn); dfree(c->d_res); dfree(c->d_lam); dfree(c->d_misfit);
-    dfree(c->d_grad);
+    dfree(c->d_grad); dfree(c->d_grad2); dfree(c->d_apx0);
     if (c->grad_graph) cudaGraphExecDestroy(c->grad_graph);
     c->grad_graph = nullptr;
     c->grad_valid = false;
@@ -623,11 +625,33 @@ int run_forward(sfd_ctx* ctx, float* out_dev) {
     return finish_nan(ctx);
 }
 
+// d tau_eps/tau_sigma / d (1/Q) of QS:473-551 (Blanch's tau: tau_p = (1/(0.9 Q)) (ln-ratio)
+// / (atan-ratio)), in double, for the chain rule of the viscoacoustic gradient.
+double q_kappa(float f0) {
+    const double pi = 3.1415926, flow = 2.0 * 2.0 * pi, fup = 2.5 * (double)f0 * 2.0 * pi;
+    const double tss = 1.0 / ((fup - flow) / 2.0);
+    const double nlow = std::log(tss * tss * flow * flow + 1.0), nup = std::log(tss * tss * fup * fup + 1.0);
+    const double dlow = std::atan(flow * tss) - flow * tss / (1.0 + tss * tss * flow * flow);
+    const double dup = std::atan(fup * tss) - fup * tss / (1.0 + tss * tss * fup * fup);
+    return (20.0 / 18.0) * (nup - nlow) / (dup - dlow);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Gradient: forward with checkpoints every C steps, residuals and misfit, then for each segment
 // (last to first) restore its checkpoint, recompute its C forward steps keeping D_k, and run
 // the C adjoint steps backwards accumulating the zero-lag imaging sum.
 // ---------------------------------------------------------------------------------------------
+// Per scheme: fields kept in a checkpoint, forward derivatives kept per recomputed step,
+// adjoint fields, imaging sums.  Acoustic: P, Vx, Vz (one parity) / D / Q, X, Z ping-pong /
+// g.  Viscoacoustic: the eight in-place fields / Dx1 vx, Dz1 vz / eight adjoints + Qx, Qz /
+// g1, g2.
+struct GradShape {
+    int ckpt, div, adj, img;
+};
+GradShape grad_shape(const sfd_ctx* c) {
+    return c->g.scheme == SFD_VISCOAC_2D ? GradShape{8, 2, 10, 2} : GradShape{3, 1, 6, 1};
+}
+
 int grad_alloc(sfd_ctx* ctx) {
     const int C = ctx->ckpt_interval > 0 ? std::min(ctx->ckpt_interval, ctx->nt_max)
                                          : (int)std::ceil(std::sqrt((double)ctx->nt_max));
@@ -637,14 +661,20 @@ int grad_alloc(sfd_ctx* ctx) {
     if (ctx->grad_graph) cudaGraphExecDestroy(ctx->grad_graph);
     ctx->grad_graph = nullptr;
     ctx->grad_valid = false;
+    const GradShape gs = grad_shape(ctx);
     const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
     const size_t nrec = std::max<long long>(1, ctx->rec_total);
-    CK(cudaMalloc(&ctx->d_ckpt, sizeof(float) * fs * 3 * ncp));
-    CK(cudaMalloc(&ctx->d_div, sizeof(float) * fs * C));
+    CK(cudaMalloc(&ctx->d_ckpt, sizeof(float) * fs * gs.ckpt * ncp));
+    CK(cudaMalloc(&ctx->d_div, sizeof(float) * fs * gs.div * C));
     if (!ctx->d_adj) {
-        CK(cudaMalloc(&ctx->d_adj, sizeof(float) * fs * 6));
-        CK(cudaMalloc(&ctx->d_gseg, sizeof(float) * fs));
-        CK(cudaMalloc(&ctx->d_gacc, sizeof(double) * fs));
+        CK(cudaMalloc(&ctx->d_adj, sizeof(float) * fs * gs.adj));
+        CK(cudaMalloc(&ctx->d_gseg, sizeof(float) * fs * gs.img));
+        CK(cudaMalloc(&ctx->d_gacc, sizeof(double) * fs * gs.img));
+        if (ctx->g.scheme == SFD_VISCOAC_2D) {
+            CK(cudaMalloc(&ctx->d_grad2, sizeof(double) * (size_t)ctx->g.nx * ctx->g.nz));
+            CK(cudaMalloc(&ctx->d_apx0, sizeof(int) * ctx->nshot));
+            CK(cudaMemcpy(ctx->d_apx0, ctx->h_ap_x0.data(), sizeof(int) * ctx->nshot, cudaMemcpyHostToDevice));
+        }
         CK(cudaMalloc(&ctx->d_obs_nt, sizeof(float) * nrec));
         CK(cudaMalloc(&ctx->d_obs_tn, sizeof(float) * nrec));
         CK(cudaMalloc(&ctx->d_res, sizeof(float) * nrec));
@@ -670,6 +700,16 @@ int range_active(const sfd_ctx* ctx, const GradRange& r, int k) {
 }
 
 int grad_fwd_step(sfd_ctx* ctx, const GradRange& r, int k, int act, float* div_out) {
+    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        QArgs q = make_qargs(ctx, k);
+        q.slot_to_shot = r.slots;
+        if (div_out) {
+            q.d1_out = div_out;
+            q.d4_out = div_out + (size_t)ctx->nshot * ctx->L.shot_stride;
+        }
+        CK(viscoac2d_launch_step(q, act, ctx->stream));
+        return SFD_OK;
+    }
     Acou2DArgs a = make_args(ctx, k);
     a.slot_to_shot = r.slots;
     a.div_out = div_out;
@@ -677,7 +717,44 @@ int grad_fwd_step(sfd_ctx* ctx, const GradRange& r, int k, int act, float* div_o
     return SFD_OK;
 }
 
+// arguments of the viscoacoustic adjoint kernels (q_adjoint2d.cu) for forward step k
+QAdjArgs make_qadj(const sfd_ctx* ctx, const GradRange& r, int k, const float* div) {
+    const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+    const QArgs f = make_qargs(ctx, k);
+    QAdjArgs a{};
+    float* A = ctx->d_adj;
+    a.avx = A; a.avz = A + fs; a.asx = A + 2 * fs; a.asz = A + 3 * fs; a.asr = A + 4 * fs;
+    a.arx = A + 5 * fs; a.arz = A + 6 * fs; a.arr = A + 7 * fs; a.qx = A + 8 * fs; a.qz = A + 9 * fs;
+    a.d1 = div;
+    a.d4 = div ? div + fs : nullptr;
+    a.g1 = ctx->d_gseg;
+    a.g2 = ctx->d_gseg + fs;
+    a.L = ctx->L;
+    a.nz = f.nz; a.npx = f.npx; a.npz = f.npz;
+    a.busg = f.busg; a.p1 = f.p1; a.p2 = f.p2;
+    a.mpitch = f.mpitch; a.nx_model = f.nx_model;
+    a.dt = f.dt; a.f_mem = f.f_mem; a.hx = f.hx; a.hz = f.hz; a.dz2 = f.dz2;
+    std::memcpy(a.a, f.a, sizeof(a.a));
+    a.spg = f.spg; a.spg_stride = f.spg_stride;
+    a.shots = ctx->d_shots;
+    a.slot_to_shot = r.slots;
+    a.stamps = f.stamps;
+    a.res = ctx->d_res;
+    a.rec_x = ctx->d_rec_x; a.rec_z = ctx->d_rec_z;
+    a.tile_rec_ptr = ctx->d_trp; a.tile_rec_idx = ctx->d_tri;
+    a.lam_src = ctx->d_lam;
+    a.nt_max = ctx->nt_max;
+    a.step = k;
+    return a;
+}
+
+int grad_adj_step_q(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
+    CK(q_adjoint_launch_step(make_qadj(ctx, r, k, div), act, ctx->stream));
+    return SFD_OK;
+}
+
 int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return grad_adj_step_q(ctx, r, k, act, div);
     const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
     float* Q[2] = {ctx->d_adj, ctx->d_adj + fs};
     float* X[2] = {ctx->d_adj + 2 * fs, ctx->d_adj + 3 * fs};
@@ -724,9 +801,11 @@ int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float*
 int grad_copy_state(sfd_ctx* ctx, const GradRange& r, int slot, int b, bool to_ckpt) {
     const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
     const size_t off = (size_t)r.first * ctx->L.shot_stride, len = (size_t)r.count * ctx->L.shot_stride;
-    for (int f = 0; f < 3; f++) {
-        float* st = ctx->d_state + (2 * f + b) * fs + off;
-        float* ck = ctx->d_ckpt + ((size_t)slot * 3 + f) * fs + off;
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;  // eight in-place fields, no parity
+    const int nf = grad_shape(ctx).ckpt;
+    for (int f = 0; f < nf; f++) {
+        float* st = ctx->d_state + (visco ? f : 2 * f + b) * fs + off;
+        float* ck = ctx->d_ckpt + ((size_t)slot * nf + f) * fs + off;
         CK(cudaMemcpyAsync(to_ckpt ? ck : st, to_ckpt ? st : ck, len * sizeof(float), cudaMemcpyDeviceToDevice,
                            ctx->stream));
     }
@@ -738,6 +817,9 @@ int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches
     const int C = ctx->grad_C, ncp = ctx->grad_ncp;
     const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
     const size_t off = (size_t)r.first * ctx->L.shot_stride, len = (size_t)r.count * ctx->L.shot_stride;
+    const GradShape gs = grad_shape(ctx);
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    const int per_step = visco ? 2 : 1;  // launches per forward or adjoint step
     int nrec_max = 0;
     for (int s = r.first; s < r.first + r.count; s++) nrec_max = std::max(nrec_max, ctx->h_shots[s].nrec);
     // forward with checkpoints
@@ -746,36 +828,43 @@ int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches
         if (act == 0) break;
         if (k % C == 0 && (rc = grad_copy_state(ctx, r, k / C, k & 1, true))) return rc;
         if ((rc = grad_fwd_step(ctx, r, k, act, nullptr))) return rc;
-        (*launches)++;
+        *launches += per_step;
     }
     // residuals of this range and the misfit
     const ShotDev& s0 = ctx->h_shots[r.first];
     const ShotDev& s1 = ctx->h_shots[r.first + r.count - 1];
     const long long rb = s0.rec_base, re = s1.rec_base + (long long)s1.nrec * s1.nt;
     CK(launch_residual(ctx->d_rec_tn + rb, ctx->d_obs_tn + rb, ctx->d_res + rb, re - rb, ctx->d_misfit, ctx->stream));
-    CK(launch_adjoint_init(ctx->d_adj, ctx->d_adj + fs, ctx->L, ctx->d_shots, r.first, r.count, ctx->d_res,
-                           ctx->d_rec_x, ctx->d_rec_z, nrec_max, ctx->stream));
+    if (visco) {
+        CK(q_adjoint_launch_init(make_qadj(ctx, r, 0, nullptr), r.first, r.count, nrec_max, ctx->stream));
+    } else {
+        CK(launch_adjoint_init(ctx->d_adj, ctx->d_adj + fs, ctx->L, ctx->d_shots, r.first, r.count, ctx->d_res,
+                               ctx->d_rec_x, ctx->d_rec_z, nrec_max, ctx->stream));
+    }
     *launches += 2;
     // segments, last to first
     for (int j = ncp - 1; j >= 0; j--) {
         const int k0 = j * C, k1 = std::min(k0 + C, ctx->nt_max);
         if (range_active(ctx, r, k0) == 0) continue;
         if ((rc = grad_copy_state(ctx, r, j, k0 & 1, false))) return rc;
-        CK(cudaMemsetAsync(ctx->d_gseg + off, 0, len * sizeof(float), ctx->stream));
+        for (int i = 0; i < gs.img; i++)
+            CK(cudaMemsetAsync(ctx->d_gseg + i * fs + off, 0, len * sizeof(float), ctx->stream));
         for (int k = k0; k < k1; k++) {
             const int act = range_active(ctx, r, k);
             if (act == 0) break;
-            if ((rc = grad_fwd_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * fs))) return rc;
-            (*launches)++;
+            if ((rc = grad_fwd_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * gs.div * fs))) return rc;
+            *launches += per_step;
         }
         for (int k = k1 - 1; k >= k0; k--) {
             const int act = range_active(ctx, r, k);
             if (act == 0) continue;
-            if ((rc = grad_adj_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * fs))) return rc;
+            if ((rc = grad_adj_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * gs.div * fs))) return rc;
+            *launches += per_step;
+        }
+        for (int i = 0; i < gs.img; i++) {
+            CK(launch_accumulate(ctx->d_gacc + i * fs + off, ctx->d_gseg + i * fs + off, (long long)len, ctx->stream));
             (*launches)++;
         }
-        CK(launch_accumulate(ctx->d_gacc + off, ctx->d_gseg + off, (long long)len, ctx->stream));
-        (*launches)++;
     }
     return SFD_OK;
 }
@@ -785,8 +874,9 @@ int enqueue_gradient(sfd_ctx* ctx, bool batched, long long* launches) {
     const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
     if ((rc = prologue(ctx))) return rc;
     CK(cudaMemsetAsync(ctx->d_misfit, 0, sizeof(double), ctx->stream));
-    CK(cudaMemsetAsync(ctx->d_adj, 0, 6 * fs * sizeof(float), ctx->stream));
-    CK(cudaMemsetAsync(ctx->d_gacc, 0, fs * sizeof(double), ctx->stream));
+    const GradShape gs = grad_shape(ctx);
+    CK(cudaMemsetAsync(ctx->d_adj, 0, gs.adj * fs * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_gacc, 0, gs.img * fs * sizeof(double), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_lam, 0, sizeof(float) * (size_t)ctx->nshot * ctx->nt_max, ctx->stream));
     int nrec_max = 0;
     for (const auto& s : ctx->h_shots) nrec_max = std::max(nrec_max, s.nrec);
@@ -802,6 +892,15 @@ int enqueue_gradient(sfd_ctx* ctx, bool batched, long long* launches) {
             if ((rc = enqueue_gradient_range(ctx, r, launches))) return rc;
         }
     }
+    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        const QArgs q = make_qargs(ctx, 0);
+        CK(q_launch_gradient_reduce(ctx->d_gacc, ctx->d_gacc + fs, ctx->L, ctx->d_shots, ctx->d_apx0, ctx->nshot,
+                                    ctx->d_vp + kModelGhostZ, q.p1, q.p2, ctx->mpitch, ctx->g.nx, ctx->g.nz,
+                                    (double)q.dt, (double)q.f_mem, q_kappa(ctx->g.f0), ctx->d_grad, ctx->d_grad2,
+                                    ctx->stream));
+        (*launches)++;
+        return SFD_OK;
+    }
     const Acou2DArgs f = make_args(ctx, 0);
     CK(launch_gradient_reduce(ctx->d_gacc, ctx->L, ctx->d_shots, ctx->nshot, f.vp, f.den, ctx->den_c, ctx->mpitch,
                               ctx->g.nx, ctx->g.nz, ctx->g.dt, ctx->d_grad, ctx->stream));
@@ -813,9 +912,10 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (!obs) return set_err(ctx, SFD_ERR_ARG, "observed records are required");
-    if (ctx->g.scheme != SFD_ACOUSTIC_2D)
-        return set_err(ctx, SFD_ERR_UNSUPPORTED, "the gradient is implemented for the acoustic scheme");
-    if (grad_invq) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "the gradient is implemented for the 2-D schemes");
+    if (grad_invq && !visco) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = grad_alloc(ctx))) return rc;
     if (!ctx->graph_valid && (rc = tune_schedule(ctx))) return rc;
@@ -856,7 +956,7 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     ctx->timing.loop_ms = ms;
     ctx->timing.device_ms = ms;
     ctx->timing.graph = batched ? 1 : 0;
-    ctx->timing.kernel_variant = 20 + ctx->plan.stages;
+    ctx->timing.kernel_variant = visco ? 50 : 20 + ctx->plan.stages;
     double pts = 0;
     for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
     ctx->timing.point_updates = 3 * pts;  // forward, recomputation, adjoint
@@ -864,7 +964,18 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
     if (misfit) *misfit = (float)mis;
     ctx->have_grad = true;
-    if (grad_vp) {
+    const size_t nm = (size_t)ctx->g.nx * ctx->g.nz;
+    if (visco) {
+        std::vector<double> g(nm);
+        if (grad_vp) {
+            CK(cudaMemcpy(g.data(), ctx->d_grad, nm * sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < nm; i++) grad_vp[i] = (float)g[i];
+        }
+        if (grad_invq) {
+            CK(cudaMemcpy(g.data(), ctx->d_grad2, nm * sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < nm; i++) grad_invq[i] = (float)g[i];
+        }
+    } else if (grad_vp) {
         const size_t n = (size_t)ctx->g.nx * ctx->g.nz;
         std::vector<double> g(n);
         CK(cudaMemcpy(g.data(), ctx->d_grad, n * sizeof(double), cudaMemcpyDeviceToHost));
@@ -882,7 +993,7 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
         for (size_t i = 0; i < n; i++) grad_vp[i] = (float)g[i];
     }
     ctx->timing.h2d_bytes = (long long)sizeof(float) * ctx->rec_total;
-    ctx->timing.d2h_bytes = grad_vp ? (long long)sizeof(float) * ctx->g.nx * ctx->g.nz : 0;
+    ctx->timing.d2h_bytes = (long long)sizeof(float) * nm * ((grad_vp ? 1 : 0) + (grad_invq ? 1 : 0));
     ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SFD_OK;
 }
@@ -941,7 +1052,7 @@ int q_prepare(sfd_ctx* ctx) {
     int rc;
     if ((rc = upload(&ctx->q_busg, busg)) || (rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2)))
         return rc;
-    if (width != ctx->q_width) ctx->graph_valid = false;
+    if (width != ctx->q_width) ctx->graph_valid = ctx->grad_valid = false;
     ctx->q_width = width;
     if (ctx->have_shots) {
         for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
@@ -1546,7 +1657,10 @@ int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out) {
     if (shot < 0 || shot >= ctx->nshot) return set_err(ctx, SFD_ERR_ARG, "bad shot %d", shot);
     const ShotDev& sd = ctx->h_shots[shot];
     CK(cudaMemcpy(out, ctx->d_lam + (size_t)shot * ctx->nt_max, sizeof(float) * sd.nt, cudaMemcpyDeviceToHost));
-    for (int j = 0; j < sd.nt; j++) out[j] = -sd.inj_scale * out[j];  // d misfit / d w[j] = -s lambda_j[src]
+    // acoustic: d misfit / d w[j] = -s lambda_j[src]; viscoacoustic: the kernels store the
+    // stamp-weighted sum itself
+    if (ctx->g.scheme != SFD_VISCOAC_2D)
+        for (int j = 0; j < sd.nt; j++) out[j] = -sd.inj_scale * out[j];
     return SFD_OK;
 }
 

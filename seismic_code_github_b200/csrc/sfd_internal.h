@@ -70,8 +70,46 @@ struct QArgs {
     const int* tile_rec_ptr; const int* tile_rec_idx;
     float* records;                       // [nt][nrec] per shot: strzz (= strxx) at the receivers
     int step;
+    float* d1_out;                        // optional: Dx1 vx of this step (field layout), for the gradient
+    float* d4_out;                        // optional: Dz1 vz of this step
 };
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
+
+// Arguments of the viscoacoustic adjoint kernels (q_adjoint2d.cu): adjoint fields in place.
+struct QAdjArgs {
+    float* avx; float* avz;               // adjoints of vx, vz
+    float* asx; float* asz; float* asr;   // adjoints of sx, sz, sr
+    float* arx; float* arz; float* arr;   // adjoints of rx, rz, rr
+    float* qx; float* qz;                 // dt b vx^, dt b vz^ of the current step (halo exchange)
+    const float* d1; const float* d4;     // Dx1 vx, Dz1 vz of the forward step being transposed
+    float* g1; float* g2;                 // per-shot imaging sums for p1 and p2 (field layout)
+    Layout2D L;
+    int nz, npx, npz;
+    const float* busg; const float* p1; const float* p2;  // prepared model (row z = 0 of column 0)
+    int mpitch, nx_model;
+    float dt, f_mem, hx, hz, dz2;
+    float a[5];
+    const float* spg;
+    int spg_stride;
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* stamps;
+    const float* res;                     // residuals, [nt][nrec] per shot at ShotDev::rec_base
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr; const int* tile_rec_idx;
+    float* lam_src;                       // [shot][nt_max]: d misfit / d wavelet sample
+    int nt_max;
+    int step;
+};
+// adjoint of forward step a.step for the active shots (two launches)
+cudaError_t q_adjoint_launch_step(const QAdjArgs& a, int active, cudaStream_t st);
+// adjoint initial state: sx^, sz^, sr^ += residual of each shot's last step at its receivers
+cudaError_t q_adjoint_launch_init(const QAdjArgs& a, int first_shot, int nshot, int nrec_max, cudaStream_t st);
+// model-grid d misfit / d vp and d misfit / d (1/Q) from the per-shot double imaging sums
+cudaError_t q_launch_gradient_reduce(const double* acc1, const double* acc2, const Layout2D& L, const ShotDev* shots,
+                                     const int* ap_x0, int nshot, const float* vp, const float* p1, const float* p2,
+                                     int mpitch, int nx_model, int nz, double dt, double f, double kappa,
+                                     double* grad_vp, double* grad_invq, cudaStream_t st);
 // host preparation, QS:434-551: busg, p1, p2 on the padded grid and rtaustss
 void viscoac2d_prepare(int nx, int nz, const float* vp, const float* rho, const float* q, float f0, float* busg,
                        float* p1, float* p2, float* rtau);

@@ -173,6 +173,10 @@ __global__ void __launch_bounds__(kThreads) q_stress_kernel(const __grid_constan
         rz = xs(rz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
         a.sx[c] = sx; a.sz[c] = sz; a.sr[c] = sr;
         a.rx[c] = rx; a.rz[c] = rz; a.rr[c] = rr;
+        if (a.d1_out) {  // gradient recomputation keeps the derivatives for the imaging condition
+            a.d1_out[c] = d1;
+            a.d4_out[c] = d4;
+        }
     }
     // receivers: strzz (= strxx) = (sx + sz) + sr (QM:452-459)
     const int* trp = a.tile_rec_ptr + sd.tile_rec_base + t.tile;
