@@ -15,6 +15,12 @@
 //   * tiles whose working set is inside the sponge-free, fully updated interior skip the
 //     sponge and mask multiplies (a CTA-uniform branch).
 // Two CTAs share an SM, so one CTA's loads overlap the other's arithmetic.
+//
+// The same kernel runs the adjoint step (ADJ = true; the recurrence is stated in adjoint2d.cu):
+// the P, Vx, Vz slots then hold the adjoint state nu = M K a Q (halo 2R), X and Z; phase A forms
+// X' = X + rdx S+x nu, phase B Z' = Z + rdz S+z nu, phase C the new nu from S-x and S-z of the
+// density-scaled, masked X' and Z', plus the imaging sum g += nu_old D_k.  Every model factor is
+// needed at the tile's own cells only, which is why the adjoint carries nu rather than Q.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -120,7 +126,7 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // One tile.  EDGE = some point of the tile's working set lies in the sponge or the frozen rim.
-template <int R, int NST, bool VARDEN, bool EDGE>
+template <int R, int NST, bool VARDEN, bool EDGE, bool ADJ>
 __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, float* stage, const ShotDev& sd, int shot,
                                           int tile, int x0, int z0) {
     using T = TP<R, NST>;
@@ -214,7 +220,19 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                     bh = make_float2(-a.dtdx / d.z, -a.dtdx / d.w);
                 }
                 float2 vl = lo(vo), vh = hi(vo);
-                if (EDGE) {
+                if (ADJ) {  // staged X'' = B M (X + rdx S+x nu), B = dt/(dx den) (1 here for constant density)
+                    vl = fma2(bc(a.rdx_f), sl, vl);
+                    vh = fma2(bc(a.rdx_f), sh, vh);
+                    if (EDGE) {
+                        const float mx = sMx[row];
+                        vl = mul2(vl, mul2(bc(mx), lo(mz)));
+                        vh = mul2(vh, mul2(bc(mx), hi(mz)));
+                    }
+                    if (VARDEN) {
+                        vl = mul2(vl, make_float2(-bl.x, -bl.y));
+                        vh = mul2(vh, make_float2(-bh.x, -bh.y));
+                    }
+                } else if (EDGE) {
                     const float ax = sAx[row], mx = sMx[row];
                     const float4 sa = ax >= 0.0f ? make_float4(ax, ax, ax, ax) : az;
                     vl = mul2(vl, lo(sa));
@@ -275,7 +293,12 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                         b0 = a.dtdz / __ldg(a.den + (long long)g0 * a.mpitch + zg);
                         b1 = a.dtdz / __ldg(a.den + (long long)g1 * a.mpitch + zg);
                     }
-                    if (EDGE) {
+                    if (ADJ) {  // staged Z'' = B M (Z + rdz S+z nu)
+                        const float mz = EDGE ? sMz[zi + kk] : 1.0f;
+                        const float c0 = VARDEN ? b0 : 1.0f, c1 = VARDEN ? b1 : 1.0f;
+                        outz[kq] = make_float2(fmaf(a.rdz_f, s.x, vo0) * (mx0 * mz) * c0,
+                                               fmaf(a.rdz_f, s.y, vo1) * (mx1 * mz) * c1);
+                    } else if (EDGE) {
                         const float az = sAz[zi + kk], mz = sMz[zi + kk];
                         vo0 *= (ax0 >= 0.0f ? ax0 : az);
                         vo1 *= (ax1 >= 0.0f ? ax1 : az);
@@ -316,10 +339,11 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                 sl = fma2(bc(C[m]), sub2(lo(vw[o + R + m]), lo(vw[o + R - m - 1])), sl);
                 sh = fma2(bc(C[m]), sub2(hi(vw[o + R + m]), hi(vw[o + R - m - 1])), sh);
             }
-            sx[o] = cat(mul2(sl, bc(a.rdx_f)), mul2(sh, bc(a.rdx_f)));
+            const float cx = ADJ ? a.adj_cx : a.rdx_f;
+            sx[o] = cat(mul2(sl, bc(cx)), mul2(sh, bc(cx)));
         }
         const int gz = z0 + zo;
-        if (gz < nz) {
+        if (!ADJ && gz < nz) {
             float* vxo = a.vx_out + cell(x0 + r0, gz);
 #pragma unroll
             for (int o = 0; o < 4; o++) {
@@ -354,7 +378,7 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             float2 s = mul2(bc(C[0]), sub2(vz[c + T::OFFC], vz[c + T::OFFC - 1]));
 #pragma unroll
             for (int m = 1; m < R; m++) s = fma2(bc(C[m]), sub2(vz[c + T::OFFC + m], vz[c + T::OFFC - m - 1]), s);
-            sz[c] = mul2(s, bc(a.rdz_f));
+            sz[c] = mul2(s, bc(ADJ ? a.adj_cz : a.rdz_f));
         }
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -363,6 +387,63 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             const float4 po = ld4(pc);
             const float4 vp4 = vpre[o];
             const float4 dn4 = dpre[o];
+            if (ADJ) {
+                // bracket = nu_old / K + S-x(B M X') + S-z(B M Z') (= M a Q_old + ...), nu_new = M a K bracket
+                const float2 kl = mul2(mul2(mul2(lo(dn4), lo(vp4)), lo(vp4)), bc(a.dt));
+                const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(a.dt));
+                const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
+                const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
+                const float2 bl = __fadd2_rn(__fadd2_rn(lo(sx[o]), dl),
+                                             make_float2(__fdividef(po.x, kl.x), __fdividef(po.y, kl.y)));
+                const float2 bh = __fadd2_rn(__fadd2_rn(hi(sx[o]), dh),
+                                             make_float2(__fdividef(po.z, kh.x), __fdividef(po.w, kh.y)));
+                float4 fa4 = make_float4(1.f, 1.f, 1.f, 1.f), fm4 = fa4;  // sponge a and mask M of the own cells
+                if (EDGE) {
+                    const float ax = sAx[row + R], mx = sMx[row + R];
+                    fa4 = ax >= 0.0f ? make_float4(ax, ax, ax, ax) : az;
+                    fm4 = make_float4(mx * mz.x, mx * mz.y, mx * mz.z, mx * mz.w);
+                }
+                const float2 nl = mul2(mul2(bl, kl), mul2(lo(fa4), lo(fm4)));
+                const float2 nh = mul2(mul2(bh, kh), mul2(hi(fa4), hi(fm4)));
+                if (gx < nx && gz < nz) {
+                    const long long c = cell(gx, gz);
+                    // X = a M X' and Z = a M Z' from the staged B M X', B M Z'
+                    float4 xf = fa4, zf = fa4;
+                    if (VARDEN) {
+                        xf = make_float4(fa4.x * dn4.x * a.adj_xs, fa4.y * dn4.y * a.adj_xs, fa4.z * dn4.z * a.adj_xs,
+                                         fa4.w * dn4.w * a.adj_xs);
+                        zf = make_float4(fa4.x * dn4.x * a.adj_zs, fa4.y * dn4.y * a.adj_zs, fa4.z * dn4.z * a.adj_zs,
+                                         fa4.w * dn4.w * a.adj_zs);
+                    }
+                    const float4 xs = ld4(sVx + (row + R) * T::SVX_P + zo);
+                    const float4 xo = make_float4(xs.x * xf.x, xs.y * xf.y, xs.z * xf.z, xs.w * xf.w);
+                    const float4 zo4 = make_float4(cmp2(vz[T::OFFC], h) * zf.x, cmp2(vz[T::OFFC + 1], h) * zf.y,
+                                                   cmp2(vz[T::OFFC + 2], h) * zf.z, cmp2(vz[T::OFFC + 3], h) * zf.w);
+                    const float bq[4] = {bl.x, bl.y, bh.x, bh.y};
+                    if (gx == sd.sx && sd.sz >= gz && sd.sz < gz + 4)
+                        for (int cc = 0; cc < 4; cc++)
+                            if (sd.sz == gz + cc) a.adj_lam[(long long)shot * a.nt_max + step] = bq[cc];
+                    const float4 nn = cat(nl, nh);
+                    if (gz + 3 < nz) {
+                        const float4 d4 = __ldg(reinterpret_cast<const float4*>(a.adj_div + c));
+                        float4 g4 = *reinterpret_cast<const float4*>(a.adj_g + c);
+                        g4 = make_float4(fmaf(po.x, d4.x, g4.x), fmaf(po.y, d4.y, g4.y), fmaf(po.z, d4.z, g4.z),
+                                         fmaf(po.w, d4.w, g4.w));
+                        *reinterpret_cast<float4*>(a.adj_g + c) = g4;
+                        *reinterpret_cast<float4*>(a.p_out + c) = nn;
+                        *reinterpret_cast<float4*>(a.vx_out + c) = xo;
+                        *reinterpret_cast<float4*>(a.vz_out + c) = zo4;
+                    } else {
+                        for (int qq = 0; qq < 4 && gz + qq < nz; qq++) {
+                            a.adj_g[c + qq] = fmaf(comp(po, qq), __ldg(a.adj_div + c + qq), a.adj_g[c + qq]);
+                            a.p_out[c + qq] = comp(nn, qq);
+                            a.vx_out[c + qq] = comp(xo, qq);
+                            a.vz_out[c + qq] = comp(zo4, qq);
+                        }
+                    }
+                }
+                continue;
+            }
             // -kk = -DEN * Vp * Vp * dt (AFD:293)
             const float2 kl = mul2(mul2(mul2(lo(dn4), lo(vp4)), lo(vp4)), bc(-a.dt));
             const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(-a.dt));
@@ -408,6 +489,28 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                 }
             }
         }
+    }
+    // ---- adjoint: residual of step k-1 at the receivers of this tile (AFD:376-377 transposed),
+    // nu += M a K res; several receivers may share a cell, so the adds are atomic ----
+    if (ADJ) {
+        if (step >= 1 && re > rb) {
+            __syncthreads();
+            for (int j = rb + tid; j < re; j += kThreads) {
+                const int ridx = a.tile_rec_idx[j];
+                const int rx = a.rec_x[sd.rec_list + ridx], rz = a.rec_z[sd.rec_list + ridx];
+                if (rx < R || rx >= nx - R || rz < R || rz >= nz - R) continue;  // M = 0
+                const long long mi = (long long)min(sd.x0 + rx, a.nx_model - 1) * a.mpitch + rz;
+                const float vpv = __ldg(a.vp + mi), dnv = VARDEN ? __ldg(a.den + mi) : a.den_c;
+                float sa = 1.0f;
+                if (rx < a.pml) sa = a.sponge[a.pml - 1 - rx];
+                else if (rx >= nx - a.pml) sa = a.sponge[rx - (nx - a.pml)];
+                else if (rz < a.pml) sa = a.sponge[a.pml - 1 - rz];
+                else if (rz >= nz - a.pml) sa = a.sponge[rz - (nz - a.pml)];
+                const float v = a.adj_res[sd.rec_base + (long long)(step - 1) * sd.nrec + ridx];
+                atomicAdd(a.p_out + cell(rx, rz), dnv * vpv * vpv * a.dt * sa * v);
+            }
+        }
+        return;
     }
     // ---- receivers (AFD:376-377) ----
     if (re > rb) {
@@ -457,7 +560,7 @@ __device__ __forceinline__ void build_tables(const Acou2DArgs& a, float* smem, i
 // Persistent kernel: CTA b processes tiles b, b+G, b+2G, ... of all active shots.  While a tile
 // is computed out of one shared-memory stage, the TMA unit fills the other stage with the next
 // tile's P, Vx and Vz boxes (one mbarrier per stage, expect_tx accounting).
-template <int R, int NST, bool VARDEN>
+template <int R, int NST, bool VARDEN, bool ADJ>
 __global__ void __launch_bounds__(kThreads, NST == 1 ? 2 : 1)
 acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
     using T = TP<R, NST>;
@@ -532,8 +635,8 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
         }
         phase ^= 1u << stg;
         float* st = smem + stg * T::STAGE;
-        if (edge) tile_body<R, NST, VARDEN, true>(a, smem, st, sd, shot, tile, x0, z0);
-        else tile_body<R, NST, VARDEN, false>(a, smem, st, sd, shot, tile, x0, z0);
+        if (edge) tile_body<R, NST, VARDEN, true, ADJ>(a, smem, st, sd, shot, tile, x0, z0);
+        else tile_body<R, NST, VARDEN, false, ADJ>(a, smem, st, sd, shot, tile, x0, z0);
         __syncthreads();  // stage, interleave buffer and tables are free again
     }
 }
@@ -548,10 +651,10 @@ int sm_count() {
     return n;
 }
 
-template <int R, int NST, bool VARDEN>
+template <int R, int NST, bool VARDEN, bool ADJ>
 cudaError_t launch_t(const Acou2DArgs& a, int active, cudaStream_t st) {
     const size_t smem = sizeof(float) * TP<R, NST>::SMEM_FLOATS;
-    auto k = acoustic2d_step_fma_kernel<R, NST, VARDEN>;
+    auto k = acoustic2d_step_fma_kernel<R, NST, VARDEN, ADJ>;
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -565,10 +668,11 @@ cudaError_t launch_t(const Acou2DArgs& a, int active, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int R>
+template <int R, bool ADJ>
 cudaError_t launch_r(const Acou2DArgs& a, int active, bool varden, int stages, cudaStream_t st) {
-    if (stages == 2) return varden ? launch_t<R, 2, true>(a, active, st) : launch_t<R, 2, false>(a, active, st);
-    return varden ? launch_t<R, 1, true>(a, active, st) : launch_t<R, 1, false>(a, active, st);
+    if (stages == 2)
+        return varden ? launch_t<R, 2, true, ADJ>(a, active, st) : launch_t<R, 2, false, ADJ>(a, active, st);
+    return varden ? launch_t<R, 1, true, ADJ>(a, active, st) : launch_t<R, 1, false, ADJ>(a, active, st);
 }
 
 template <int R>
@@ -582,10 +686,11 @@ void boxes_t(int bp[2], int bvx[2], int bvz[2]) {
 }  // namespace
 
 cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, bool varden, int stages,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, bool adj) {
     switch (radius) {
 #define SFD_CASE(RR) \
-    case RR: return launch_r<RR>(a, active, varden, stages, st);
+    case RR: return adj ? launch_r<RR, true>(a, active, varden, stages, st) \
+                        : launch_r<RR, false>(a, active, varden, stages, st);
         SFD_CASE(1) SFD_CASE(2) SFD_CASE(4) SFD_CASE(5) SFD_CASE(8)
 #undef SFD_CASE
     default: return cudaErrorInvalidValue;

@@ -113,7 +113,8 @@ struct sfd_ctx {
     int grad_C = 0, grad_ncp = 0;
     float* d_ckpt = nullptr;    // [ncp][3 fields][nshot * shot_stride]
     float* d_div = nullptr;     // [C][nshot * shot_stride]: D_k of the segment being recomputed
-    float* d_adj = nullptr;     // adjoint state: q0 q1 x0 x1 z0 z1
+    float* d_adj = nullptr;     // adjoint state: nu0 nu1 x0 x1 z0 z1 (viscoacoustic: 8 adjoints + Qx Qz)
+    CUtensorMap adj_tmaps[6];   // TMA descriptors of the acoustic adjoint buffers
     float* d_gseg = nullptr;    // per-segment imaging sum (float)
     double* d_gacc = nullptr;   // imaging sum over all segments (double)
     float* d_obs_nt = nullptr;  // observed records as given ([nrec][nt] per shot)
@@ -670,6 +671,16 @@ int grad_alloc(sfd_ctx* ctx) {
         CK(cudaMalloc(&ctx->d_adj, sizeof(float) * fs * gs.adj));
         CK(cudaMalloc(&ctx->d_gseg, sizeof(float) * fs * gs.img));
         CK(cudaMalloc(&ctx->d_gacc, sizeof(double) * fs * gs.img));
+        if (ctx->g.scheme == SFD_ACOUSTIC_2D) {
+            int bp[2], bvx[2], bvz[2];
+            acoustic2d_fma_boxes(ctx->radius, bp, bvx, bvz);
+            const int* boxes[3] = {bp, bvx, bvz};
+            for (int b = 0; b < 6; b++) {
+                const int rc = encode_field_map(ctx, &ctx->adj_tmaps[b], ctx->d_adj + b * fs, ctx->L, ctx->nshot,
+                                                boxes[b / 2]);
+                if (rc) return rc;
+            }
+        }
         if (ctx->g.scheme == SFD_VISCOAC_2D) {
             CK(cudaMalloc(&ctx->d_grad2, sizeof(double) * (size_t)ctx->g.nx * ctx->g.nz));
             CK(cudaMalloc(&ctx->d_apx0, sizeof(int) * ctx->nshot));
@@ -753,46 +764,39 @@ int grad_adj_step_q(sfd_ctx* ctx, const GradRange& r, int k, int act, const floa
     return SFD_OK;
 }
 
+// Arguments of the FMA kernel in adjoint mode for forward step k: reads buffer (k+1) & 1 of
+// nu, X, Z and writes buffer k & 1.
+Acou2DArgs make_adj_args(const sfd_ctx* ctx, const GradRange& r, int k, const float* div) {
+    const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+    Acou2DArgs a = make_args(ctx, k);
+    const int i = (k + 1) & 1, o = k & 1;
+    float* A = ctx->d_adj;
+    a.p_in = A + i * fs; a.p_out = A + o * fs;
+    a.vx_in = A + (2 + i) * fs; a.vx_out = A + (2 + o) * fs;
+    a.vz_in = A + (4 + i) * fs; a.vz_out = A + (4 + o) * fs;
+    a.tm_p = ctx->adj_tmaps[i];
+    a.tm_vx = ctx->adj_tmaps[2 + i];
+    a.tm_vz = ctx->adj_tmaps[4 + i];
+    a.slot_to_shot = r.slots;
+    a.records = nullptr;
+    a.src_pre = nullptr;
+    a.div_out = nullptr;
+    a.adj_div = div;
+    a.adj_g = ctx->d_gseg;
+    a.adj_res = ctx->d_res;
+    a.adj_lam = ctx->d_lam;
+    a.nt_max = ctx->nt_max;
+    a.adj_cx = ctx->varden ? 1.0f : a.dtdx / ctx->den_c;
+    a.adj_cz = ctx->varden ? 1.0f : a.dtdz / ctx->den_c;
+    a.adj_xs = ctx->g.dx / ctx->g.dt;
+    a.adj_zs = ctx->g.dz / ctx->g.dt;
+    return a;
+}
+
 int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
     if (ctx->g.scheme == SFD_VISCOAC_2D) return grad_adj_step_q(ctx, r, k, act, div);
-    const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
-    float* Q[2] = {ctx->d_adj, ctx->d_adj + fs};
-    float* X[2] = {ctx->d_adj + 2 * fs, ctx->d_adj + 3 * fs};
-    float* Z[2] = {ctx->d_adj + 4 * fs, ctx->d_adj + 5 * fs};
-    const int i = (k + 1) & 1, o = k & 1;
-    const Acou2DArgs f = make_args(ctx, k);
-    Adj2DArgs a{};
-    a.q_in = Q[i]; a.q_out = Q[o];
-    a.x_in = X[i]; a.x_out = X[o];
-    a.z_in = Z[i]; a.z_out = Z[o];
-    a.div = div;
-    a.g_seg = ctx->d_gseg;
-    a.L = ctx->L;
-    a.nz = ctx->g.nz;
-    a.pml = ctx->g.pml;
-    a.vp = f.vp;
-    a.den = f.den;
-    a.mpitch = ctx->mpitch;
-    a.nx_model = ctx->g.nx;
-    a.den_c = ctx->den_c;
-    a.dt = ctx->g.dt;
-    a.dtdx = f.dtdx;
-    a.dtdz = f.dtdz;
-    a.rdx = f.rdx_f;
-    a.rdz = f.rdz_f;
-    std::memcpy(a.coef, f.coef, sizeof(a.coef));
-    std::memcpy(a.sponge, f.sponge, sizeof(a.sponge));
-    a.shots = ctx->d_shots;
-    a.slot_to_shot = r.slots;
-    a.res = ctx->d_res;
-    a.rec_x = ctx->d_rec_x;
-    a.rec_z = ctx->d_rec_z;
-    a.tile_rec_ptr = ctx->d_trp;
-    a.tile_rec_idx = ctx->d_tri;
-    a.lam_src = ctx->d_lam;
-    a.nt_max = ctx->nt_max;
-    a.step = k;
-    CK(adjoint2d_launch_step(ctx->radius, a, act, ctx->varden, ctx->stream));
+    CK(acoustic2d_fma_launch(ctx->radius, make_adj_args(ctx, r, k, div), act, ctx->varden, ctx->plan.stages,
+                             ctx->stream, true));
     return SFD_OK;
 }
 
@@ -838,8 +842,8 @@ int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches
     if (visco) {
         CK(q_adjoint_launch_init(make_qadj(ctx, r, 0, nullptr), r.first, r.count, nrec_max, ctx->stream));
     } else {
-        CK(launch_adjoint_init(ctx->d_adj, ctx->d_adj + fs, ctx->L, ctx->d_shots, r.first, r.count, ctx->d_res,
-                               ctx->d_rec_x, ctx->d_rec_z, nrec_max, ctx->stream));
+        CK(launch_adjoint_init(ctx->d_adj, ctx->d_adj + fs, make_adj_args(ctx, r, 0, nullptr), ctx->radius, r.first,
+                               r.count, nrec_max, ctx->stream));
     }
     *launches += 2;
     // segments, last to first
@@ -901,9 +905,8 @@ int enqueue_gradient(sfd_ctx* ctx, bool batched, long long* launches) {
         (*launches)++;
         return SFD_OK;
     }
-    const Acou2DArgs f = make_args(ctx, 0);
-    CK(launch_gradient_reduce(ctx->d_gacc, ctx->L, ctx->d_shots, ctx->nshot, f.vp, f.den, ctx->den_c, ctx->mpitch,
-                              ctx->g.nx, ctx->g.nz, ctx->g.dt, ctx->d_grad, ctx->stream));
+    CK(launch_gradient_reduce(ctx->d_gacc, ctx->L, ctx->d_shots, ctx->nshot, ctx->d_vp + kModelGhostZ, ctx->mpitch,
+                              ctx->g.nx, ctx->g.nz, ctx->d_grad, ctx->stream));
     (*launches)++;
     return SFD_OK;
 }

@@ -154,48 +154,33 @@ struct Acou2DArgs {
     float* div_out;            // optional: D = rdx S-x Vx + rdz S-z Vz of this step (field layout)
     float* src_pre;            // optional, per shot: P at the source cell before the next step's
                                // injection (the value AFD holds there after the sponge)
+    // Adjoint mode of the FMA kernel (acoustic2d_fma_launch with adj = true): the P, Vx, Vz slots
+    // hold the adjoint state nu = M K a Q (K = DEN Vp^2 dt, a the sponge, M the update mask),
+    // X = a M X' and Z = a M Z' of adjoint step `step` (adjoint2d.cu states the recurrence).
+    const float* adj_div;      // D_k of the forward step being transposed (field layout)
+    float* adj_g;              // imaging sum, field layout: g += nu_old D_k
+    const float* adj_res;      // residuals [nt][nrec] per shot at ShotDev::rec_base
+    float* adj_lam;            // [shot][nt_max]: adjoint of P at the source cell
+    int nt_max;
+    float adj_cx, adj_cz;      // dtdx/den_c, dtdz/den_c (constant density), 1 with variable density
+    float adj_xs, adj_zs;      // dx/dt, dz/dt: X = a den (dx/dt) (staged value) with variable density
 };
 
-// Arguments of the adjoint step kernel (adjoint2d.cu); field buffers share Layout2D.
-struct Adj2DArgs {
-    const float* q_in;  float* q_out;   // adjoint of P
-    const float* x_in;  float* x_out;   // adjoint of the unsponged Vx
-    const float* z_in;  float* z_out;   // adjoint of the unsponged Vz
-    const float* div;                   // D_k of the forward step being transposed
-    float* g_seg;                       // per-shot imaging accumulator (field layout)
-    Layout2D L;
-    int nz, pml;
-    const float* vp; const float* den;  // model (row z = 0 of column 0), den NULL = constant
-    int mpitch, nx_model;
-    float den_c, dt, dtdx, dtdz, rdx, rdz;
-    float coef[kMaxRadius];
-    float sponge[256];
-    const ShotDev* shots;
-    const int* slot_to_shot;
-    const float* res;                   // residuals, [nt][nrec] per shot at ShotDev::rec_base
-    const int* rec_x; const int* rec_z;
-    const int* tile_rec_ptr; const int* tile_rec_idx;
-    float* lam_src;                     // [shot][nt_max]: adjoint of P at the source cell
-    int nt_max;
-    int step;
-};
-cudaError_t adjoint2d_launch_step(int radius, const Adj2DArgs& a, int active, bool varden, cudaStream_t st);
 // residual = pred - obs (both [nt][nrec] per shot), misfit += 0.5 sum residual^2 (double)
 cudaError_t launch_residual(const float* pred, const float* obs, float* res, long long n, double* misfit,
                             cudaStream_t st);
 // records [nrec][nt] per shot -> [nt][nrec] per shot
 cudaError_t launch_records_transpose_in(const float* rec_nt, float* rec_tn, const ShotDev* shots, int nshot,
                                         int nrec_max, int nt_max, cudaStream_t st);
-// adjoint initial state: Q(shot, buffer nt & 1) = R^T res[nt-1]
-cudaError_t launch_adjoint_init(float* q0, float* q1, const Layout2D& L, const ShotDev* shots, int first_shot,
-                                int nshot, const float* res, const int* rec_x, const int* rec_z, int nrec_max,
-                                cudaStream_t st);
+// adjoint initial state: nu(shot, buffer nt & 1) += M a K res[nt-1] at the receivers
+cudaError_t launch_adjoint_init(float* q0, float* q1, const Acou2DArgs& a, int radius, int first_shot, int nshot,
+                                int nrec_max, cudaStream_t st);
 // acc (double) += seg (float) over n values
 cudaError_t launch_accumulate(double* acc, const float* seg, long long n, cudaStream_t st);
-// grad_model[x][z] = scale(x, z) * sum over shots of acc_s(x - ap_x0_s, z), scale = -2 den vp dt
+// grad_model[x][z] = -(2 / vp) * sum over shots of acc_s(x - ap_x0_s, z)
 cudaError_t launch_gradient_reduce(const double* acc, const Layout2D& L, const ShotDev* shots, int nshot,
-                                   const float* vp, const float* den, float den_c, int mpitch, int nx_model,
-                                   int nz, float dt, double* grad_model, cudaStream_t st);
+                                   const float* vp, int mpitch, int nx_model, int nz, double* grad_model,
+                                   cudaStream_t st);
 
 // Host-side launchers (acoustic2d.cu).
 struct Acou2DPlan {
@@ -211,9 +196,10 @@ constexpr int kModelGhostZ = 16;
 bool acoustic2d_plan(int radius, Acou2DPlan* plan);
 cudaError_t acoustic2d_launch_step(const Acou2DPlan& plan, const Acou2DArgs& a, int active_shots,
                                    bool exact, bool varden, cudaStream_t st);
-// stages: 1 = one tile per CTA, two CTAs per SM; 2 = persistent CTAs with double-buffered TMA
+// stages: 1 = one tile per CTA, two CTAs per SM; 2 = persistent CTAs with double-buffered TMA.
+// adj: run the adjoint of step a.step instead (the adj_* arguments).
 cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, bool varden, int stages,
-                                 cudaStream_t st);
+                                 cudaStream_t st, bool adj = false);
 int acoustic2d_fma_gz(int radius);
 // TMA box extents (z, x) the FMA kernel loads for P, Vx and Vz at this radius.
 void acoustic2d_fma_boxes(int radius, int box_p[2], int box_vx[2], int box_vz[2]);
