@@ -3,6 +3,7 @@
     python -m seismic_code_github_b200.cases acoustic3d --n 384 --nshot 2 --nt 3
     python -m seismic_code_github_b200.cases viscoac --nshot 4 --nt 200
     python -m seismic_code_github_b200.cases gradient --nshot 4 --nt 300
+    python -m seismic_code_github_b200.cases forward2d --nshot 16 --nt 40
 
 Each run builds a seeded synthetic model, runs one warm-up call and one timed call of the
 batched path and prints the engine's timing record.  Sizes are chosen on the command line so
@@ -49,6 +50,19 @@ def viscoac(args):
         return e.timing()
 
 
+def forward2d(args):
+    case = W.config2(nshot=args.nshot, nt=args.nt)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    shots = [S.ShotSpec(sx, sz, rx, rz, w) for sx, sz in zip(case.src_x, case.src_z)]
+    with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16) as e:
+        e.set_model(case.vp, case.den)
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
 def gradient(args):
     case, vp_true = W.config4(nshot=args.nshot, nt=args.nt)
     w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
@@ -67,12 +81,12 @@ def gradient(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient"])
+    ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient", "forward2d"])
     ap.add_argument("--n", type=int, default=384, help="3-D padded grid size per axis")
     ap.add_argument("--nshot", type=int, default=2)
     ap.add_argument("--nt", type=int, default=3)
     args = ap.parse_args()
-    t = {"acoustic3d": acoustic3d, "viscoac": viscoac, "gradient": gradient}[args.case](args)
+    t = {"acoustic3d": acoustic3d, "viscoac": viscoac, "gradient": gradient, "forward2d": forward2d}[args.case](args)
     print(json.dumps(t))
 
 

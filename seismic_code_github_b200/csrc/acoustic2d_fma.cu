@@ -49,7 +49,9 @@ struct TP {
     static constexpr int HX = 2 * R;         // x halo of the staged pressure
     // TMA boxes land densely: row pitch = box width
     static constexpr int SP_ROWS = TX + 2 * HX, SP_W = TZ + 2 * HZ, SP_P = SP_W;
-    static constexpr int SVX_ROWS = TX + 2 * R, SVX_P = TZ;
+    // Vx rows are padded to TZ + 4 floats (the TMA box is 4 floats wider than the tile) so that
+    // rows four apart fall on different shared-memory banks in phase C
+    static constexpr int SVX_ROWS = TX + 2 * R, SVX_P = TZ + 4;
     static constexpr int NZV = TZ + 2 * RQ, SVZ_P = pitch8(NZV);
     static constexpr int NXV = TX + 2 * R;
     static constexpr int NPAIR = TX / 2;
@@ -79,7 +81,7 @@ struct TP {
     static constexpr int OFF_MZ = OFF_AZ + r4(NZV);
     static constexpr int OFF_BAR = r4(OFF_MZ + r4(NZV));  // two mbarriers (8 bytes each)
     static constexpr int SMEM_FLOATS = OFF_BAR + 4;
-    static constexpr unsigned TX_BYTES = 4u * (SP_ROWS * SP_W + SVX_ROWS * TZ + TX * SVZ_P);
+    static constexpr unsigned TX_BYTES = 4u * (SP_ROWS * SP_W + SVX_ROWS * SVX_P + TX * SVZ_P);
     static_assert(NPAIR * NZB == kThreads, "phase B covers the block");
     static_assert(TX * TZ == 16 * kThreads, "phase C: 16 points per thread");
     static_assert(NZB * KZB >= NZV, "phase B covers the velocity region");
@@ -152,7 +154,7 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
     // loads are issued now so that their latency is covered by phases A and B.
     float4 vpre[4], dpre[4];
     {
-        const int zgv = (tid & 7) + 8 * (warp & 1), xbv = (lane >> 3) + 4 * (warp >> 1);
+        const int zgv = (lane & 3) + 4 * (lane >> 3), xbv = ((lane >> 2) & 1) + 2 * warp;  // phase C's mapping
         const int gz = z0 + 4 * zgv;
 #pragma unroll
         for (int o = 0; o < 4; o++) {
@@ -166,17 +168,18 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
     const int rb = __ldg(trp), re = __ldg(trp + 1);
 
     // ---- interleave the tile's P rows in x pairs: sI[(p*IW + z)*2 + {0,1}] = P[x0+2p+{0,1}][z] ----
+    // (each item moves two z of a pair: 8-byte loads and 16-byte stores, both contiguous across
+    // consecutive lanes, so neither side has bank conflicts)
     {
-        constexpr int Q = T::SP_W / 4, N = T::NPAIR * Q, IT = (N + kThreads - 1) / kThreads;
+        constexpr int Q = T::SP_W / 2, N = T::NPAIR * Q, IT = (N + kThreads - 1) / kThreads;
 #pragma unroll
         for (int it = 0; it < IT; it++) {
             const int i = tid + it * kThreads;
             if (i < N) {
                 const int p = i / Q, q = i - p * Q;
-                const float4 u = ld4(sP + (2 * p + T::HX) * T::SP_P + 4 * q);
-                const float4 v = ld4(sP + (2 * p + 1 + T::HX) * T::SP_P + 4 * q);
-                st4(sI + (p * T::IW + 4 * q) * 2, make_float4(u.x, v.x, u.y, v.y));
-                st4(sI + (p * T::IW + 4 * q + 2) * 2, make_float4(u.z, v.z, u.w, v.w));
+                const float2 u = ld2(sP + (2 * p + T::HX) * T::SP_P + 2 * q);
+                const float2 v = ld2(sP + (2 * p + 1 + T::HX) * T::SP_P + 2 * q);
+                st4(sI + (p * T::IW + 2 * q) * 2, make_float4(u.x, v.x, u.y, v.y));
             }
         }
     }
@@ -312,17 +315,22 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
     }
     __syncthreads();  // everyone is done reading interleaved P
     {
+        // interleaved new Vz, two z per 16-byte store: the eight lanes of a quarter warp share
+        // one x pair and start 2*KZB entries apart, which spreads them over all banks
         float* dst = sI + (pB * T::IW + zbB * T::KZB) * 2;
 #pragma unroll
-        for (int k = 0; k < T::KZB; k++)
-            if (zbB * T::KZB + k < T::NZV) st2(dst + 2 * k, outz[k]);  // interleaved new Vz
+        for (int k = 0; k < T::KZB; k += 2)
+            if (zbB * T::KZB + k < T::NZV) st4(dst + 2 * k, cat(outz[k], outz[k + 1]));
     }
     __syncthreads();
 
     // ---- phase C: P(t) on the tile, 4 rows x one z-vector per thread (AFD:289-314, 337-338) ----
     const int step = a.step;
-    const int zgv = (tid & 7) + 8 * (warp & 1);
-    const int xbv = (lane >> 3) + 4 * (warp >> 1);
+    // a quarter warp = 4 consecutive z-vectors x 2 consecutive x blocks: with the padded Vx rows
+    // and odd x blocks taking their two x pairs in reverse order, the Vx and interleaved-Vz
+    // window loads of the eight lanes fall on distinct banks
+    const int zgv = (lane & 3) + 4 * (lane >> 3);
+    const int xbv = ((lane >> 2) & 1) + 2 * warp;
     const int zo = 4 * zgv, r0 = 4 * xbv;
     float4 sx[4];
     {
@@ -362,8 +370,24 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
     }
     const int gz = z0 + zo;
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
+    for (int qi = 0; qi < 2; qi++) {
+        const int q = (xbv & 1) ? 1 - qi : qi;
         const int p = 2 * xbv + q;  // x pair: tile rows 2p, 2p+1 = r0 + 2q, r0 + 2q + 1
+        // adjoint: D_k and the imaging sum of the pair's cells, loaded before the z-stencil so
+        // that their latency is covered
+        float4 dpf[2], gpf[2];
+        if (ADJ) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gx = x0 + r0 + 2 * q + h;
+                dpf[h] = gpf[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gx < nx && gz + 3 < nz) {
+                    const long long c = cell(gx, gz);
+                    dpf[h] = __ldg(reinterpret_cast<const float4*>(a.adj_div + c));
+                    gpf[h] = *reinterpret_cast<const float4*>(a.adj_g + c);
+                }
+            }
+        }
         const float* zsrc = sI + (p * T::IW + zo + T::RQ - T::OFFC) * 2;
         float2 vz[T::NWC];
 #pragma unroll
@@ -385,17 +409,19 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             const int o = 2 * q + h, row = r0 + o, gx = x0 + row;
             float* pc = sP + (row + T::HX) * T::SP_P + T::HZ + zo;
             const float4 po = ld4(pc);
-            const float4 vp4 = vpre[o];
-            const float4 dn4 = dpre[o];
+            // q depends on the thread: pick the register arrays' entries by selects
+            const float4 vp4 = q ? vpre[2 + h] : vpre[h];
+            const float4 dn4 = q ? dpre[2 + h] : dpre[h];
+            const float4 sxo = q ? sx[2 + h] : sx[h];
             if (ADJ) {
                 // bracket = nu_old / K + S-x(B M X') + S-z(B M Z') (= M a Q_old + ...), nu_new = M a K bracket
                 const float2 kl = mul2(mul2(mul2(lo(dn4), lo(vp4)), lo(vp4)), bc(a.dt));
                 const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(a.dt));
                 const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
                 const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
-                const float2 bl = __fadd2_rn(__fadd2_rn(lo(sx[o]), dl),
+                const float2 bl = __fadd2_rn(__fadd2_rn(lo(sxo), dl),
                                              make_float2(__fdividef(po.x, kl.x), __fdividef(po.y, kl.y)));
-                const float2 bh = __fadd2_rn(__fadd2_rn(hi(sx[o]), dh),
+                const float2 bh = __fadd2_rn(__fadd2_rn(hi(sxo), dh),
                                              make_float2(__fdividef(po.z, kh.x), __fdividef(po.w, kh.y)));
                 float4 fa4 = make_float4(1.f, 1.f, 1.f, 1.f), fm4 = fa4;  // sponge a and mask M of the own cells
                 if (EDGE) {
@@ -425,8 +451,8 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                             if (sd.sz == gz + cc) a.adj_lam[(long long)shot * a.nt_max + step] = bq[cc];
                     const float4 nn = cat(nl, nh);
                     if (gz + 3 < nz) {
-                        const float4 d4 = __ldg(reinterpret_cast<const float4*>(a.adj_div + c));
-                        float4 g4 = *reinterpret_cast<const float4*>(a.adj_g + c);
+                        const float4 d4 = dpf[h];
+                        float4 g4 = gpf[h];
                         g4 = make_float4(fmaf(po.x, d4.x, g4.x), fmaf(po.y, d4.y, g4.y), fmaf(po.z, d4.z, g4.z),
                                          fmaf(po.w, d4.w, g4.w));
                         *reinterpret_cast<float4*>(a.adj_g + c) = g4;
@@ -449,7 +475,7 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(-a.dt));
             const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
             const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
-            const float2 divl = __fadd2_rn(lo(sx[o]), dl), divh = __fadd2_rn(hi(sx[o]), dh);
+            const float2 divl = __fadd2_rn(lo(sxo), dl), divh = __fadd2_rn(hi(sxo), dh);
             float2 pl = fma2(kl, divl, lo(po));
             float2 ph = fma2(kh, divh, hi(po));
             if (a.div_out != nullptr && gx < nx && gz < nz) {  // recomputation for the adjoint
@@ -621,18 +647,32 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
             !(x0 - R >= E && x0 + T::TX + R <= nx - E && z0 - T::RQ >= E && z0 + T::TZ + T::RQ <= nz - E);
         if (edge) build_tables<R, NST>(a, smem, x0, z0, nx);
         __syncthreads();  // tables written
-        // bounded wait for this tile's boxes (about one second of wall time, then give up)
+        // bounded wait for this tile's boxes (about one second of wall time, then give up).  One
+        // thread polls while the others sleep in the barrier, so that a waiting CTA takes no issue
+        // slots from the CTA computing beside it; after the barrier every thread observes the
+        // completed phase itself, which orders the TMA writes before its shared-memory reads.
         const unsigned par = (phase >> stg) & 1u;
-        bool done = mbar_try_wait(bars + stg, par);
-        if (!done) {
-            const uint64_t t0 = global_ns();
-            while (!(done = mbar_try_wait(bars + stg, par)) && global_ns() - t0 < 1000000000ull) {
+        auto bounded_wait = [&](int b, unsigned pa) {
+            bool ok = mbar_try_wait(bars + b, pa);
+            if (!ok) {
+                const uint64_t t0 = global_ns();
+                while (!(ok = mbar_try_wait(bars + b, pa)) && global_ns() - t0 < 1000000000ull) {
+                }
             }
-        }
+            return ok;
+        };
+        bool done = true;
+        if (tid == 0) done = bounded_wait(stg, par);
         if (__syncthreads_or(!done)) {
-            if (tid == 0) atomicExch(a.err_flag, 1);
+            if (tid == 0) {
+                atomicExch(a.err_flag, 1);
+                // let copies still in flight land before the CTA's shared memory is released
+                bounded_wait(stg, par);
+                if (NST == 2 && t + G < total) bounded_wait(stg ^ 1, (phase >> (stg ^ 1)) & 1u);
+            }
             return;
         }
+        if (tid != 0) mbar_try_wait(bars + stg, par);  // completed: returns at once
         phase ^= 1u << stg;
         float* st = smem + stg * T::STAGE;
         if (edge) tile_body<R, NST, VARDEN, true, ADJ>(a, smem, st, sd, shot, tile, x0, z0);
@@ -679,7 +719,7 @@ template <int R>
 void boxes_t(int bp[2], int bvx[2], int bvz[2]) {
     using T = TP<R, 1>;
     bp[0] = T::SP_W; bp[1] = T::SP_ROWS;
-    bvx[0] = T::TZ; bvx[1] = T::SVX_ROWS;
+    bvx[0] = T::SVX_P; bvx[1] = T::SVX_ROWS;
     bvz[0] = T::SVZ_P; bvz[1] = T::TX;
 }
 
