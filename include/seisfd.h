@@ -144,8 +144,8 @@ int sfd_forward_per_shot(sfd_ctx* ctx, float* records);
 int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out);
 
 /* Full-waveform gradient: forward with checkpoints, adjoint of the discrete time loop,
- * zero-lag cross-correlation imaging.  obs: observed records in the sfd_forward layout.
- * misfit = 0.5 * sum (pred - obs)^2.  grad_vp: d misfit / d vp on the padded grid.
+ * zero-lag cross-correlation imaging (2-D acoustic, viscoacoustic and 3-D acoustic schemes).
+ * obs: observed records in the sfd_forward layout.  misfit = 0.5 * sum (pred - obs)^2.  grad_vp: d misfit / d vp on the padded grid.
  * grad_invq: d misfit / d (1/Q) (SFD_VISCOAC_2D only; may be NULL).  No reference
  * counterpart (the reference has no adjoint). */
 int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);
@@ -163,6 +163,13 @@ int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out);
  * every shot is kept every `steps` steps; each segment is recomputed once during the
  * backward pass, so memory is O(nt/steps + steps) wavefields per shot. */
 int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps);
+
+/* Device-memory budget of sfd_gradient in bytes (0 = the free device memory).  The 3-D gradient
+ * sizes its shot groups and checkpoint levels to the budget: every shot group keeps its
+ * wavefields, adjoint fields and outer checkpoints; when one level of checkpoints does not fit,
+ * segments are recomputed from inner checkpoints (two levels, four passes instead of three).
+ * No reference counterpart (the reference has no adjoint). */
+int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes);
 
 int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);
 

@@ -64,6 +64,10 @@ int oracle_afd3d_f32(const OracleAfd3Cfg* g, const float* vp, const float* den, 
                      float* final_p);
 int oracle_afd3d_f64(const OracleAfd3Cfg* g, const float* vp, const float* den, const float* wavelet, double* record,
                      double* final_p);
+// FP64 misfit, d misfit / d vp and d misfit / d wavelet of the 3-D scheme and its FP64 records
+// ([nrec][nt]); obs NULL computes the records only.
+int oracle_afd3d_gradient_f64(const OracleAfd3Cfg* g, const float* vp, const float* den, const float* wavelet,
+                              const float* obs, double* misfit, double* grad_vp, double* dw, double* records);
 // FP64 misfit gradient of the viscoacoustic (vs = 0) scheme on a padded grid (np sponge cells per
 // side, arrays x-major): records [nrec][nt], d/dvp and d/d(1/Q) per cell, d/dw per sample.
 typedef struct {

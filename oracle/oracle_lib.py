@@ -191,6 +191,35 @@ def afd3d_sponge(nx: int, ny: int, nz: int, pml: int) -> np.ndarray:
     return a
 
 
+def afd3d_gradient_f64(vp, den, wavelet, src, rec_x, rec_y, rec_z, pml, dx, dy, dz, dt, obs=None, radius=4,
+                       den_c=2400.0):
+    """FP64 3-D records, misfit, d misfit/d vp and d misfit/d wavelet (oracle/adj3d_oracle.cpp).
+    Returns dict(records, misfit, grad_vp, dw); the gradients are None without obs."""
+    L = lib()
+    if not hasattr(L, "_a3g_sig"):
+        L.oracle_afd3d_gradient_f64.argtypes = [ctypes.POINTER(OracleAfd3Cfg), _F32P, _F32P, _F32P, _F32P, _F64P,
+                                                _F64P, _F64P, _F64P]
+        L._a3g_sig = True
+    vp = np.ascontiguousarray(vp, np.float32)
+    nx, ny, nz = vp.shape
+    den = None if den is None else np.ascontiguousarray(den, np.float32)
+    w = np.ascontiguousarray(wavelet, np.float32)
+    rx, ry, rz = (np.ascontiguousarray(a, np.int32) for a in (rec_x, rec_y, rec_z))
+    cfg = OracleAfd3Cfg(nx, ny, nz, pml, len(w), radius, dx, dy, dz, dt, src[0], src[1], src[2], len(rx),
+                        rx.ctypes.data_as(_I32P), ry.ctypes.data_as(_I32P), rz.ctypes.data_as(_I32P), den_c)
+    rec = np.zeros((len(rx), len(w)), np.float64)
+    mis = np.zeros(1, np.float64)
+    g = np.zeros((nx, ny, nz), np.float64) if obs is not None else None
+    dw = np.zeros(len(w), np.float64) if obs is not None else None
+    o = None if obs is None else np.ascontiguousarray(obs, np.float32)
+    rc = L.oracle_afd3d_gradient_f64(ctypes.byref(cfg), _p(vp), None if den is None else _p(den), _p(w),
+                                     None if o is None else _p(o), _p(mis, _F64P), None if g is None else _p(g, _F64P),
+                                     None if dw is None else _p(dw, _F64P), _p(rec, _F64P))
+    if rc != 0:
+        raise ValueError("oracle_afd3d_gradient_f64 rejected the configuration")
+    return {"records": rec, "misfit": float(mis[0]), "grad_vp": g, "dw": dw}
+
+
 def afd3d_forward(vp, den, wavelet, src, rec_x, rec_y, rec_z, pml, dx, dy, dz, dt, radius=4, fp64=True,
                   den_c=2400.0, want_final=False):
     """Restated 3-D scheme (oracle/afd3d_oracle.cpp) for one shot on the padded (nx, ny, nz) grid.

@@ -18,10 +18,17 @@
 // pressure update uses the undamped new velocities and P is stored damped -- the order of
 // AFD:289-340.  The source (before the step) and the receivers (after it) are separate small
 // launches.
+//
+// The same kernel runs the adjoint step (ADJ = true), the 2-D recurrence of adjoint2d.cu with a
+// y axis: the P slot holds nu = M K a Q, the velocity slots X, Y, Z; the velocity phases form
+// X' = X + rd S+ nu and stage B M X' (B = dt / (d den)) for the pressure phase, which forms
+// nu' = M a K (nu / K + sum_a S-a(B M X_a')) and the imaging sum g += nu D_k; the velocity
+// outputs are a M X'.  Every model factor is needed at the updated point only.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <type_traits>
 
 #include "sfd_internal.h"
@@ -167,7 +174,27 @@ __device__ __forceinline__ float4 vel_update(float4 vo, float4 b, float2 s01, fl
     return cat4(v01, v23);
 }
 
-template <int R, bool VARDEN>
+// adjoint velocity update on four points: staged B M (X + rd sum), output a M (X + rd sum)
+template <bool EDGE, bool VARDEN>
+__device__ __forceinline__ float4 adj_vel(float4 xo, float rd, float2 s01, float2 s23, float4 f, float4 k, float4 b,
+                                          float4* out) {
+    float2 v01 = __ffma2_rn(make_float2(rd, rd), s01, lo2(xo));
+    float2 v23 = __ffma2_rn(make_float2(rd, rd), s23, hi2(xo));
+    if (EDGE) {
+        v01 = __fmul2_rn(v01, lo2(k));
+        v23 = __fmul2_rn(v23, hi2(k));
+        *out = cat4(__fmul2_rn(v01, lo2(f)), __fmul2_rn(v23, hi2(f)));
+    } else {
+        *out = cat4(v01, v23);
+    }
+    if (VARDEN) {
+        v01 = __fmul2_rn(v01, lo2(b));
+        v23 = __fmul2_rn(v23, hi2(b));
+    }
+    return cat4(v01, v23);
+}
+
+template <int R, bool VARDEN, bool ADJ>
 __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __grid_constant__ Acou3DArgs a) {
     using K = K3<R>;
     extern __shared__ __align__(128) float smem[];
@@ -187,7 +214,8 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
     const int yo = y0 + yl, zo = z0 + zr;
     const bool own_ok = yo < ny && zo < L.pitch;  // the float4 lies inside the allocation
     const long long own_off = (long long)min(yo, ny - 1) * L.pitch + min(zo, L.pitch - 4);
-    const long long shot_off = (long long)shot * L.shot_stride;
+    const int slab = a.slab_by_slot ? (int)blockIdx.y : shot;
+    const long long shot_off = (long long)slab * L.shot_stride;
     const float* p_in = a.p_in + shot_off;
     const float* vx_in = a.vx_in + shot_off;
 
@@ -224,9 +252,9 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sptr(bar)), "r"(K::TX_BYTES)
                      : "memory");
-        tma_load_4d(st, &a.tm_p, z0 - K::HZ, y0 - K::HY, s, shot, bar);
-        tma_load_4d(st + K::OFF_VY, &a.tm_vy, z0, y0 - R, s, shot, bar);
-        tma_load_4d(st + K::OFF_VZ, &a.tm_vz, z0 - K::RQ, y0, s, shot, bar);
+        tma_load_4d(st, &a.tm_p, z0 - K::HZ, y0 - K::HY, s, slab, bar);
+        tma_load_4d(st + K::OFF_VY, &a.tm_vy, z0, y0 - R, s, slab, bar);
+        tma_load_4d(st + K::OFF_VZ, &a.tm_vz, z0 - K::RQ, y0, s, slab, bar);
     };
 
     if (tid == 0) {
@@ -307,17 +335,25 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
                     }
                     const float4 vo = ld4s(st + K::OFF_VY + row * TZ + zt);
                     const float2 s01 = h ? b01.v : a01.v, s23 = h ? b23.v : a23.v;
-                    float4 vn;
-                    if (edge) {
-                        const int i = row * K::VZW + K::RQ + zt;
-                        vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                    float4 vn, vout;
+                    const int i = row * K::VZW + K::RQ + zt;
+                    if (ADJ) {
+                        if (edge)
+                            vn = adj_vel<true, VARDEN>(vo, a.rdy, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s), b,
+                                                       &vout);
+                        else
+                            vn = adj_vel<false, VARDEN>(vo, a.rdy, s01, s23, vo, vo, b, &vout);
                     } else {
-                        vn = vel_update<false>(vo, b, s01, s23, vo, vo);
+                        if (edge)
+                            vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                        else
+                            vn = vel_update<false>(vo, b, s01, s23, vo, vo);
+                        vout = vn;
                     }
                     st4s(nby + row * TZ + zt, vn);
                     const int y = y0 - R + row;
                     if (row >= R && row < R + TY && y < ny && z0 + zt < L.pitch)
-                        st4s(a.vy_out + plane_off + (long long)y * L.pitch + z0 + zt, vn);
+                        st4s(a.vy_out + plane_off + (long long)y * L.pitch + z0 + zt, vout);
                 }
             }
             // ---- new Vz on the Vz region: rows y0 .. y0+TY-1, z0-RQ .. z0+TZ+RQ-1 ----
@@ -342,17 +378,25 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
                 }
                 const float4 vo = ld4s(st + K::OFF_VZ + row * K::VZW + 4 * u);
                 const float2 s01 = make_float2(acc[0].v, acc[1].v), s23 = make_float2(acc[2].v, acc[3].v);
-                float4 vn;
-                if (edge) {
-                    const int i = (row + R) * K::VZW + 4 * u;
-                    vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                float4 vn, vout;
+                const int i = (row + R) * K::VZW + 4 * u;
+                if (ADJ) {
+                    if (edge)
+                        vn = adj_vel<true, VARDEN>(vo, a.rdz, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s), b,
+                                                   &vout);
+                    else
+                        vn = adj_vel<false, VARDEN>(vo, a.rdz, s01, s23, vo, vo, b, &vout);
                 } else {
-                    vn = vel_update<false>(vo, b, s01, s23, vo, vo);
+                    if (edge)
+                        vn = vel_update<true>(vo, b, s01, s23, edge_f(i, xpad_s, fx_s), edge_k(i, kx_s));
+                    else
+                        vn = vel_update<false>(vo, b, s01, s23, vo, vo);
+                    vout = vn;
                 }
                 st4s(nbz + row * K::VZW + 4 * u, vn);
                 const int y = y0 + row, z = z0 - K::RQ + 4 * u;
                 if (4 * u >= K::RQ && 4 * u < K::RQ + TZ && y < ny && z < L.pitch)
-                    st4s(a.vz_out + plane_off + (long long)y * L.pitch + z, vn);
+                    st4s(a.vz_out + plane_off + (long long)y * L.pitch + z, vout);
             };
             if (tid >= K::NVY2) {
 #pragma unroll
@@ -378,10 +422,18 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
                 const float4 d = ld_model(a.den, xv, yo, zo);
                 b = make_float4(a.dtdx / d.x, a.dtdx / d.y, a.dtdx / d.z, a.dtdx / d.w);
             }
-            const float4 vn = edge ? vel_update<true>(Vxo, b, s01.v, s23.v, edge_f(io, xpad_v, fx_v), edge_k(io, kx_v))
-                                   : vel_update<false>(Vxo, b, s01.v, s23.v, Vxo, Vxo);
+            float4 vn, vout;
+            if (ADJ) {
+                vn = edge ? adj_vel<true, VARDEN>(Vxo, a.rdx, s01.v, s23.v, edge_f(io, xpad_v, fx_v), edge_k(io, kx_v),
+                                                  b, &vout)
+                          : adj_vel<false, VARDEN>(Vxo, a.rdx, s01.v, s23.v, Vxo, Vxo, b, &vout);
+            } else {
+                vn = edge ? vel_update<true>(Vxo, b, s01.v, s23.v, edge_f(io, xpad_v, fx_v), edge_k(io, kx_v))
+                          : vel_update<false>(Vxo, b, s01.v, s23.v, Vxo, Vxo);
+                vout = vn;
+            }
             Vxo = ld_own(vx_in, s + R);
-            if (own_ok) st4s(a.vx_out + shot_off + (long long)xv * L.xstride + own_off, vn);
+            if (own_ok) st4s(a.vx_out + shot_off + (long long)xv * L.xstride + own_off, vout);
             sVq[((unsigned)xv % K::NQ) * kThreads] = vn;
         }
         // every thread is done with this stage and with the new-velocity buffer of plane s-1
@@ -421,8 +473,10 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
 #pragma unroll
                 for (int m = 1; m <= R; m++)
                     az[c].add(m, a.coef[m - 1], wz[K::DR + R + c + m - 1], wz[K::DR + R + c - m]);
-            // div = ((Sx / dx) + Sy / dy) + Sz / dz, then P = P - (den dt vp vp) div
-            const float2 rdx = bc2(a.rdx), rdy = bc2(a.rdy), rdz = bc2(a.rdz);
+            // div = ((Sx / dx) + Sy / dy) + Sz / dz, then P = P - (den dt vp vp) div; the adjoint
+            // weighs the sums by B (constant density) instead
+            const float2 rdx = bc2(ADJ ? a.adj_c[0] : a.rdx), rdy = bc2(ADJ ? a.adj_c[1] : a.rdy),
+                         rdz = bc2(ADJ ? a.adj_c[2] : a.rdz);
             float2 d01 = __fmul2_rn(ax01.v, rdx), d23 = __fmul2_rn(ax23.v, rdx);
             d01 = __ffma2_rn(ay01.v, rdy, d01);
             d23 = __ffma2_rn(ay23.v, rdy, d23);
@@ -437,10 +491,37 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
             }
             const float2 k01 = __fmul2_rn(__fmul2_rn(lo2(kk), lo2(vpn)), lo2(vpn));
             const float2 k23 = __fmul2_rn(__fmul2_rn(hi2(kk), hi2(vpn)), hi2(vpn));
-            float4 pn = cat4(__ffma2_rn(make_float2(-k01.x, -k01.y), d01, lo2(Pq[0])),
-                             __ffma2_rn(make_float2(-k23.x, -k23.y), d23, hi2(Pq[0])));
-            if (edge) pn = mul4(mul4(pn, edge_f(io, xpad_s, fx_s)), edge_k(io, kx_s));
-            if (own_ok) st4s(a.p_out + shot_off + (long long)s * L.xstride + own_off, pn);
+            const long long pofs = shot_off + (long long)s * L.xstride + own_off;
+            if (ADJ) {
+                // bracket = nu / K + sum (= M a Q_old + ...), nu' = M a K bracket, g += nu D_k
+                const float4 po = Pq[0];
+                const float2 b01 = __fadd2_rn(d01, make_float2(__fdividef(po.x, k01.x), __fdividef(po.y, k01.y)));
+                const float2 b23 = __fadd2_rn(d23, make_float2(__fdividef(po.z, k23.x), __fdividef(po.w, k23.y)));
+                float4 pn = cat4(__fmul2_rn(b01, k01), __fmul2_rn(b23, k23));
+                if (edge) pn = mul4(mul4(pn, edge_f(io, xpad_s, fx_s)), edge_k(io, kx_s));
+                if (own_ok) {
+                    st4s(a.p_out + pofs, pn);
+                    const float4 dk = __ldg(reinterpret_cast<const float4*>(a.adj_div + pofs));
+                    float4 g = *reinterpret_cast<const float4*>(a.adj_g + pofs);
+                    g = make_float4(fmaf(po.x, dk.x, g.x), fmaf(po.y, dk.y, g.y), fmaf(po.z, dk.z, g.z),
+                                    fmaf(po.w, dk.w, g.w));
+                    st4s(a.adj_g + pofs, g);
+                    const ShotDev& sd = a.shots[shot];
+                    if (s == sd.sx && yo == sd.sy && sd.sz >= zo && sd.sz < zo + 4) {
+                        const float bq[4] = {b01.x, b01.y, b23.x, b23.y};
+                        for (int c = 0; c < 4; c++)
+                            if (sd.sz == zo + c) a.adj_lam[(long long)shot * a.nt_max + a.step] = bq[c];
+                    }
+                }
+            } else {
+                float4 pn = cat4(__ffma2_rn(make_float2(-k01.x, -k01.y), d01, lo2(Pq[0])),
+                                 __ffma2_rn(make_float2(-k23.x, -k23.y), d23, hi2(Pq[0])));
+                if (edge) pn = mul4(mul4(pn, edge_f(io, xpad_s, fx_s)), edge_k(io, kx_s));
+                if (own_ok) {
+                    st4s(a.p_out + pofs, pn);
+                    if (a.div_out) st4s(a.div_out + pofs, cat4(d01, d23));  // recomputation for the adjoint
+                }
+            }
         }
         vpn = ld_own(a.vp, s + 1);
 #pragma unroll
@@ -451,33 +532,73 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
 }
 
 __global__ void inject3d_kernel(float* p, Layout3D L, const ShotDev* shots, const int* slot_to_shot, int active,
-                                const float* wavelets, int step) {
+                                const float* wavelets, int step, int by_slot) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active) return;
     const ShotDev sd = shots[slot_to_shot[i]];
     if (step >= sd.nt) return;
-    const long long o = (long long)slot_to_shot[i] * L.shot_stride + (long long)sd.sx * L.xstride +
+    const long long o = (long long)(by_slot ? i : slot_to_shot[i]) * L.shot_stride + (long long)sd.sx * L.xstride +
                         (long long)sd.sy * L.pitch + sd.sz;
     // P[s] -= (dt * den * vp) * w[k], AFD:250 (separate roundings)
     p[o] = __fsub_rn(p[o], __fmul_rn(sd.inj_scale, wavelets[sd.wav_off + step]));
 }
 
 __global__ void gather3d_kernel(const float* p, Layout3D L, const ShotDev* shots, const int* slot_to_shot,
-                                const int* rec_x, const int* rec_y, const int* rec_z, float* records, int step) {
+                                const int* rec_x, const int* rec_y, const int* rec_z, float* records, int step,
+                                int by_slot) {
     const int shot = slot_to_shot[blockIdx.y];
     const ShotDev sd = shots[shot];
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= sd.nrec || step >= sd.nt) return;
     const int q = sd.rec_list + r;
-    const long long o = (long long)shot * L.shot_stride + (long long)rec_x[q] * L.xstride +
+    const long long o = (long long)(by_slot ? (int)blockIdx.y : shot) * L.shot_stride + (long long)rec_x[q] * L.xstride +
                         (long long)rec_y[q] * L.pitch + rec_z[q];
     records[sd.rec_base + (long long)step * sd.nrec + r] = p[o];
 }
 
-template <int R, bool VARDEN>
+// adjoint of the receiver gather: nu[receiver] += M a K res[step] (M = 1 where the step updates P)
+__global__ void adj_inject3d_kernel(float* nu, const Acou3DArgs a, const int* rec_x, const int* rec_y,
+                                    const int* rec_z, const float* res) {
+    const int shot = a.slot_to_shot[blockIdx.y];
+    const ShotDev sd = a.shots[shot];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= sd.nrec || a.step >= sd.nt) return;
+    const Layout3D& L = a.L;
+    const int q = sd.rec_list + r;
+    const int x = rec_x[q], y = rec_y[q], z = rec_z[q];
+    if (x < a.adj_radius || x >= L.nx - a.adj_radius || y < a.adj_radius || y >= L.ny - a.adj_radius ||
+        z < a.adj_radius || z >= L.nz - a.adj_radius)
+        return;
+    const long long m = (long long)x * L.xstride + (long long)y * L.pitch + z;
+    const float vp = a.vp[m], den = a.den ? a.den[m] : a.den_c;
+    bool pad;
+    float f = axis_taper(a, x, L.nx, &pad);
+    if (!pad) {
+        f = axis_taper(a, y, L.ny, &pad);
+        if (!pad) f = axis_taper(a, z, L.nz, &pad);
+    }
+    const float v = res[sd.rec_base + (long long)a.step * sd.nrec + r];
+    const int slab = a.slab_by_slot ? (int)blockIdx.y : shot;
+    atomicAdd(nu + (long long)slab * L.shot_stride + m, den * a.dt * vp * vp * f * v);
+}
+
+__global__ void reduce3d_kernel(const double* __restrict__ acc, int nslab, Layout3D L, const float* __restrict__ vp,
+                                double* grad) {
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long xy = i / L.nz;
+        const int z = (int)(i - xy * L.nz);
+        const long long m = xy * L.pitch + z;
+        double s = 0.0;
+        for (int k = 0; k < nslab; k++) s += acc[(long long)k * L.shot_stride + m];
+        grad[i] += -2.0 * s / (double)vp[m];
+    }
+}
+
+template <int R, bool VARDEN, bool ADJ>
 cudaError_t launch_t(const Acou3DArgs& a, int active, cudaStream_t st) {
     const size_t smem = sizeof(float) * K3<R>::SMEM_FLOATS;
-    auto k = acoustic3d_step_kernel<R, VARDEN>;
+    auto k = acoustic3d_step_kernel<R, VARDEN, ADJ>;
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -499,11 +620,18 @@ void boxes_t(int bp[2], int bvy[2], int bvz[2]) {
 
 }  // namespace
 
-cudaError_t acoustic3d_launch_step(int radius, const Acou3DArgs& a, int active, bool varden, cudaStream_t st) {
+template <int R>
+cudaError_t launch_r(const Acou3DArgs& a, int active, bool varden, bool adj, cudaStream_t st) {
+    if (adj) return varden ? launch_t<R, true, true>(a, active, st) : launch_t<R, false, true>(a, active, st);
+    return varden ? launch_t<R, true, false>(a, active, st) : launch_t<R, false, false>(a, active, st);
+}
+
+cudaError_t acoustic3d_launch_step(int radius, const Acou3DArgs& a, int active, bool varden, cudaStream_t st,
+                                   bool adj) {
     if (active <= 0) return cudaSuccess;
     switch (radius) {
-    case 2: return varden ? launch_t<2, true>(a, active, st) : launch_t<2, false>(a, active, st);
-    case 4: return varden ? launch_t<4, true>(a, active, st) : launch_t<4, false>(a, active, st);
+    case 2: return launch_r<2>(a, active, varden, adj, st);
+    case 4: return launch_r<4>(a, active, varden, adj, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -517,18 +645,38 @@ bool acoustic3d_boxes(int radius, int bp[2], int bvy[2], int bvz[2]) {
 }
 
 cudaError_t acoustic3d_launch_inject(float* p, const Layout3D& L, const ShotDev* shots, const int* slot_to_shot,
-                                     int active, const float* wavelets, int step, cudaStream_t st) {
+                                     int active, const float* wavelets, int step, cudaStream_t st, int slab_by_slot) {
     if (active <= 0) return cudaSuccess;
-    inject3d_kernel<<<(active + 63) / 64, 64, 0, st>>>(p, L, shots, slot_to_shot, active, wavelets, step);
+    inject3d_kernel<<<(active + 63) / 64, 64, 0, st>>>(p, L, shots, slot_to_shot, active, wavelets, step,
+                                                       slab_by_slot);
     return cudaGetLastError();
 }
 
 cudaError_t acoustic3d_launch_gather(const float* p, const Layout3D& L, const ShotDev* shots,
                                      const int* slot_to_shot, int active, const int* rec_x, const int* rec_y,
-                                     const int* rec_z, float* records, int nrec_max, int step, cudaStream_t st) {
+                                     const int* rec_z, float* records, int nrec_max, int step, cudaStream_t st,
+                                     int slab_by_slot) {
     if (active <= 0 || nrec_max <= 0) return cudaSuccess;
     const dim3 grid((nrec_max + 255) / 256, active);
-    gather3d_kernel<<<grid, 256, 0, st>>>(p, L, shots, slot_to_shot, rec_x, rec_y, rec_z, records, step);
+    gather3d_kernel<<<grid, 256, 0, st>>>(p, L, shots, slot_to_shot, rec_x, rec_y, rec_z, records, step,
+                                          slab_by_slot);
+    return cudaGetLastError();
+}
+
+cudaError_t acoustic3d_launch_adj_inject(float* nu, const Acou3DArgs& a, const int* rec_x, const int* rec_y,
+                                         const int* rec_z, const float* res, int active, int nrec_max,
+                                         cudaStream_t st) {
+    if (active <= 0 || nrec_max <= 0) return cudaSuccess;
+    const dim3 grid((nrec_max + 255) / 256, active);
+    adj_inject3d_kernel<<<grid, 256, 0, st>>>(nu, a, rec_x, rec_y, rec_z, res);
+    return cudaGetLastError();
+}
+
+cudaError_t acoustic3d_launch_gradient_reduce(const double* acc, int nslab, const Layout3D& L, const float* vp,
+                                              double* grad, cudaStream_t st) {
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    reduce3d_kernel<<<grid, 256, 0, st>>>(acc, nslab, L, vp, grad);
     return cudaGetLastError();
 }
 

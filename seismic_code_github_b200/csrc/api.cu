@@ -52,6 +52,7 @@ struct sfd_ctx {
     std::vector<long long> rec_out_off;  // trace-major output offset per shot
     long long rec_total = 0;
     std::vector<int> order;              // shots sorted by nt, longest first
+    std::vector<int> h_ident_order;      // 0, 1, ..., nshot - 1
     std::vector<int> active_at;          // not stored per step; computed on the fly
 
     // device buffers for the acoustic 2-D scheme
@@ -125,6 +126,17 @@ struct sfd_ctx {
     double* d_grad = nullptr;   // gradient on the model grid (double)
     double* d_grad2 = nullptr;  // viscoacoustic: d misfit / d (1/Q) on the model grid
     int* d_apx0 = nullptr;      // viscoacoustic: each shot's aperture start in the model
+    // 3-D gradient (shot groups of g3_G slabs, checkpoint levels g3_C1 / g3_C2)
+    int state_slabs = 0;        // shot slabs per field held by d_state (3-D)
+    float* g3_adj = nullptr;    // adjoint state nu0 nu1 X0 X1 Y0 Y1 Z0 Z1, g3_G slabs each
+    CUtensorMap g3_tmaps[6];    // nu0 nu1 Y0 Y1 Z0 Z1
+    float* g3_div = nullptr;    // D_k of the innermost segment [C][g3_G slabs]
+    float* g3_ck1 = nullptr;    // outer checkpoints [n1][4 fields][g3_G slabs]
+    float* g3_ck2 = nullptr;    // inner checkpoints [n2][4 fields][g3_G slabs] (two levels only)
+    float* g3_gseg = nullptr;   // imaging sum of the segment (float)
+    double* g3_gacc = nullptr;  // imaging sum of the group (double)
+    int g3_G = 0, g3_C1 = 0, g3_C2 = 0, g3_n1 = 0, g3_n2 = 0;
+    size_t mem_limit = 0;       // device-memory budget of the gradient (0: what is free)
     cudaGraphExec_t grad_graph = nullptr;
     bool grad_valid = false;
     bool have_grad = false;
@@ -233,6 +245,9 @@ void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_ckpt); dfree(c->d_div); dfree(c->d_adj); dfree(c->d_gseg); dfree(c->d_gacc);
     dfree(c->d_obs_nt); dfree(c->d_obs_tn); dfree(c->d_res); dfree(c->d_lam); dfree(c->d_misfit);
     dfree(c->d_grad); dfree(c->d_grad2); dfree(c->d_apx0);
+    dfree(c->g3_adj); dfree(c->g3_div); dfree(c->g3_ck1); dfree(c->g3_ck2); dfree(c->g3_gseg); dfree(c->g3_gacc);
+    c->g3_G = c->g3_C1 = c->g3_C2 = c->g3_n1 = c->g3_n2 = 0;
+    c->state_slabs = 0;
     if (c->grad_graph) cudaGraphExecDestroy(c->grad_graph);
     c->grad_graph = nullptr;
     c->grad_valid = false;
@@ -253,6 +268,12 @@ sfd_ctx::~sfd_ctx() {
     if (eve) cudaEventDestroy(eve);
     if (stream) cudaStreamDestroy(stream);
 }
+
+namespace {
+int alloc_state_3d(sfd_ctx* ctx, int nslab);
+int full_state_3d(sfd_ctx* ctx);
+int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched);
+}  // namespace
 
 namespace {
 
@@ -317,7 +338,7 @@ int active_shots(const sfd_ctx* c, int step) {
 // Arguments of the 3-D step: buffers alternate each step like the 2-D ones.
 Acou3DArgs make_args3(const sfd_ctx* c, int step) {
     Acou3DArgs a{};
-    const long long fs = (long long)c->nshot * c->L3.shot_stride;
+    const long long fs = (long long)c->state_slabs * c->L3.shot_stride;
     const int i = step & 1, o = (step + 1) & 1;
     float* F = c->d_state;
     a.p_in = F + i * fs; a.p_out = F + o * fs;
@@ -578,6 +599,7 @@ int kernel_variant(const sfd_ctx* ctx) {
 int run_forward(sfd_ctx* ctx, float* out_dev) {
     int rc;
     long long launches = 0;
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D && (rc = full_state_3d(ctx))) return rc;
     if (snap_prepare(ctx, &rc)) ctx->graph_valid = false;
     if (rc) return rc;
     if (!ctx->graph_valid) {
@@ -916,8 +938,12 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     if (rc) return rc;
     if (!obs) return set_err(ctx, SFD_ERR_ARG, "observed records are required");
     const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D) {
+        if (grad_invq) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
+        return run_gradient_3d(ctx, obs, misfit, grad_vp, batched);
+    }
     if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
-        return set_err(ctx, SFD_ERR_UNSUPPORTED, "the gradient is implemented for the 2-D schemes");
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d has no gradient", ctx->g.scheme);
     if (grad_invq && !visco) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = grad_alloc(ctx))) return rc;
@@ -1064,6 +1090,48 @@ int q_prepare(sfd_ctx* ctx) {
     return SFD_OK;
 }
 
+// (Re)allocate the 3-D wavefields for `nslab` shot slabs per field (eight fields: P, Vx, Vy, Vz,
+// two buffers each) and encode the TMA descriptors of the P, Vy and Vz buffers.  The forward
+// holds every shot; the gradient may shrink the state to its shot-group size, and the next
+// forward grows it back (the captured time loop is rebuilt because the buffers moved).
+int alloc_state_3d(sfd_ctx* ctx, int nslab) {
+    if (ctx->d_state && ctx->state_slabs == nslab) return SFD_OK;
+    dfree(ctx->d_state);
+    ctx->state_slabs = 0;
+    ctx->graph_valid = false;
+    const Layout3D& L = ctx->L3;
+    ctx->state_floats = 8 * (size_t)nslab * L.shot_stride;
+    if (cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->d_state = nullptr;
+        return set_err(ctx, SFD_ERR_NOMEM, "3-D wavefields of %d shots need %.1f GB of device memory", nslab,
+                       ctx->state_floats * 4.0 / 1e9);
+    }
+    int bp[2], bvy[2], bvz[2];
+    acoustic3d_boxes(ctx->radius, bp, bvy, bvz);
+    const int* boxes[3] = {bp, bvy, bvz};
+    const int field_of[3] = {0, 4, 6};  // P, Vy, Vz
+    const long long fs = (long long)nslab * L.shot_stride;
+    for (int f = 0; f < 3; f++)
+        for (int b = 0; b < 2; b++) {
+            const int rc = encode_field_map3(ctx, &ctx->tmaps3[2 * f + b], ctx->d_state + (field_of[f] + b) * fs, L,
+                                             nslab, boxes[f]);
+            if (rc) return rc;
+        }
+    ctx->state_slabs = nslab;
+    return SFD_OK;
+}
+
+// The forward holds every shot's wavefields: release the gradient's buffers if the state was
+// shrunk to a shot group, then grow it back.
+int full_state_3d(sfd_ctx* ctx) {
+    if (ctx->d_state && ctx->state_slabs == ctx->nshot) return SFD_OK;
+    dfree(ctx->g3_adj); dfree(ctx->g3_div); dfree(ctx->g3_ck1); dfree(ctx->g3_ck2);
+    dfree(ctx->g3_gseg); dfree(ctx->g3_gacc);
+    ctx->g3_G = 0;
+    return alloc_state_3d(ctx, ctx->nshot);
+}
+
 // sfd_set_shots for the 3-D scheme: every shot covers the whole grid (no aperture windows);
 // sources must lie where the step updates P (R <= coordinate < n - R on every axis).
 int set_shots_3d(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
@@ -1137,6 +1205,7 @@ int set_shots_3d(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     ctx->nt_max = nt_max;
     ctx->nrec_max = nrec_max;
     ctx->order = order;
+    ctx->h_ident_order = ident;
     auto up = [&](auto** dst, const auto& v) -> int {
         using E = typename std::remove_reference<decltype(v)>::type::value_type;
         const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(E);
@@ -1152,26 +1221,318 @@ int set_shots_3d(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
     CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
-    ctx->state_floats = 8 * (size_t)nshot * L.shot_stride;
-    if (cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)) != cudaSuccess) {
-        cudaGetLastError();
-        ctx->d_state = nullptr;
-        return set_err(ctx, SFD_ERR_NOMEM, "3-D wavefields of %d shots need %.1f GB of device memory", nshot,
-                       ctx->state_floats * 4.0 / 1e9);
-    }
-    int bp[2], bvy[2], bvz[2];
-    acoustic3d_boxes(R, bp, bvy, bvz);
-    const int* boxes[3] = {bp, bvy, bvz};
-    const int field_of[3] = {0, 4, 6};  // P, Vy, Vz
-    const long long fs = (long long)nshot * L.shot_stride;
-    for (int f = 0; f < 3; f++)
-        for (int b = 0; b < 2; b++) {
-            const int rc2 = encode_field_map3(ctx, &ctx->tmaps3[2 * f + b], ctx->d_state + (field_of[f] + b) * fs, L,
-                                              nshot, boxes[f]);
-            if (rc2) return rc2;
-        }
+    const int rc3 = alloc_state_3d(ctx, nshot);
+    if (rc3) return rc3;
     ctx->have_shots = true;
     ctx->graph_valid = false;
+    return SFD_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3-D gradient.  Shots run in groups of G (launch slots 0..G-1 of a slot list, one field slab per
+// slot).  Per group: the forward keeps outer checkpoints every C1 steps and the records; then,
+// outer segment by outer segment from the last, either (one level, C2 = C1) the segment is
+// recomputed keeping D_k and transposed, or (two levels) it is recomputed keeping inner
+// checkpoints every C2 steps and each inner segment is recomputed keeping D_k and transposed.
+// G, C1 and C2 are the largest group and the cheapest schedule that fit the memory budget.
+// ---------------------------------------------------------------------------------------------
+struct Plan3 {
+    int G = 0, C1 = 0, C2 = 0, n1 = 0, n2 = 0;
+};
+
+// device bytes of a plan: wavefields and adjoint (8 + 8 slabs), imaging sums (1 float + 1 double),
+// D of one inner segment and the checkpoints (4 fields each), per slot
+double plan3_bytes(const sfd_ctx* c, const Plan3& p) {
+    const double F = 4.0 * (double)c->L3.shot_stride;
+    return F * p.G * (8.0 + 8.0 + 1.0 + 2.0 + p.C2 + 4.0 * (p.n1 + p.n2));
+}
+
+Plan3 plan3_make(int G, int C1, int C2, int nt) {
+    Plan3 p;
+    p.G = G;
+    p.C1 = std::max(1, std::min(C1, nt));
+    p.C2 = std::max(1, std::min(C2, p.C1));
+    p.n1 = (nt + p.C1 - 1) / p.C1;
+    p.n2 = p.C2 < p.C1 ? (p.C1 + p.C2 - 1) / p.C2 : 0;
+    return p;
+}
+
+int plan3_choose(sfd_ctx* ctx, int Gmax, Plan3* out) {
+    size_t freeb = 0, totb = 0;
+    CK(cudaMemGetInfo(&freeb, &totb));
+    // what this context holds and would release: the wavefields and the gradient buffers
+    double held = (double)ctx->state_floats * 4.0;
+    if (ctx->g3_G > 0) held += plan3_bytes(ctx, Plan3{ctx->g3_G, ctx->g3_C1, ctx->g3_C2, ctx->g3_n1, ctx->g3_n2});
+    // model-sized gradient, observed / residual records, adjoint source traces
+    const double fixed = 8.0 * (double)ctx->g.nx * ctx->g.ny * ctx->g.nz + 16.0 * (double)ctx->rec_total +
+                         4.0 * (double)ctx->nshot * ctx->nt_max;
+    double budget = 0.92 * ((double)freeb + held) - fixed - (double)(64u << 20);
+    if (ctx->mem_limit > 0) budget = std::min(budget, (double)ctx->mem_limit - fixed);
+    const int nt = ctx->nt_max;
+    const int ci = ctx->ckpt_interval;
+    for (int G = Gmax; G >= 1; G--) {
+        // one level: C minimises 4 ceil(nt / C) + C (or the caller's interval)
+        int best = ci > 0 ? ci : 1;
+        if (ci <= 0) {
+            double bm = 1e300;
+            for (int C = 1; C <= nt; C++) {
+                const double m = 4.0 * ((nt + C - 1) / C) + C;
+                if (m < bm) bm = m, best = C;
+            }
+        }
+        Plan3 p = plan3_make(G, best, best, nt);
+        if (plan3_bytes(ctx, p) <= budget) {
+            *out = p;
+            return SFD_OK;
+        }
+        // two levels: inner interval C2 (the caller's, or sqrt(4 C1)), outer C1 by search
+        Plan3 pb;
+        double bb = 1e300;
+        for (int C1 = 2; C1 <= nt; C1++) {
+            const int C2 = ci > 0 ? std::min(ci, C1 - 1) : std::max(1, (int)std::ceil(std::sqrt(4.0 * C1)) - 1);
+            if (C2 >= C1) continue;
+            const Plan3 q = plan3_make(G, C1, C2, nt);
+            const double m = plan3_bytes(ctx, q);
+            if (m < bb) bb = m, pb = q;
+        }
+        if (pb.G > 0 && bb <= budget) {
+            *out = pb;
+            return SFD_OK;
+        }
+    }
+    return set_err(ctx, SFD_ERR_NOMEM, "the 3-D gradient of one shot does not fit the memory budget (%.1f GB)",
+                   budget / 1e9);
+}
+
+int g3_alloc(sfd_ctx* ctx, const Plan3& p) {
+    int rc;
+    const bool same = ctx->g3_adj && p.G == ctx->g3_G && p.C1 == ctx->g3_C1 && p.C2 == ctx->g3_C2 &&
+                      ctx->state_slabs == p.G;
+    if (!same) {
+        dfree(ctx->g3_adj); dfree(ctx->g3_div); dfree(ctx->g3_ck1); dfree(ctx->g3_ck2);
+        dfree(ctx->g3_gseg); dfree(ctx->g3_gacc);
+        ctx->g3_G = 0;
+        if ((rc = alloc_state_3d(ctx, p.G))) return rc;
+        const size_t fsG = (size_t)p.G * ctx->L3.shot_stride;
+        CK(cudaMalloc(&ctx->g3_adj, sizeof(float) * fsG * 8));
+        CK(cudaMalloc(&ctx->g3_div, sizeof(float) * fsG * p.C2));
+        CK(cudaMalloc(&ctx->g3_ck1, sizeof(float) * fsG * 4 * p.n1));
+        if (p.n2 > 0) CK(cudaMalloc(&ctx->g3_ck2, sizeof(float) * fsG * 4 * p.n2));
+        CK(cudaMalloc(&ctx->g3_gseg, sizeof(float) * fsG));
+        CK(cudaMalloc(&ctx->g3_gacc, sizeof(double) * fsG));
+        int bp[2], bvy[2], bvz[2];
+        acoustic3d_boxes(ctx->radius, bp, bvy, bvz);
+        const int* boxes[3] = {bp, bvy, bvz};
+        const int field_of[3] = {0, 4, 6};  // nu, Y, Z
+        for (int f = 0; f < 3; f++)
+            for (int b = 0; b < 2; b++)
+                if ((rc = encode_field_map3(ctx, &ctx->g3_tmaps[2 * f + b], ctx->g3_adj + (field_of[f] + b) * fsG,
+                                            ctx->L3, p.G, boxes[f])))
+                    return rc;
+        ctx->g3_G = p.G; ctx->g3_C1 = p.C1; ctx->g3_C2 = p.C2; ctx->g3_n1 = p.n1; ctx->g3_n2 = p.n2;
+    }
+    if (!ctx->d_obs_nt) {
+        const size_t nrec = std::max<long long>(1, ctx->rec_total);
+        CK(cudaMalloc(&ctx->d_obs_nt, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_obs_tn, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_res, sizeof(float) * nrec));
+        CK(cudaMalloc(&ctx->d_lam, sizeof(float) * (size_t)ctx->nshot * ctx->nt_max));
+        CK(cudaMalloc(&ctx->d_misfit, sizeof(double)));
+        CK(cudaMalloc(&ctx->d_grad, sizeof(double) * (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz));
+    }
+    return SFD_OK;
+}
+
+// one forward step of the group's active slots (source before, receivers after when `gather`)
+int g3_fwd_step(sfd_ctx* ctx, const int* slots, int act, int k, float* div_out, bool gather, long long* launches) {
+    Acou3DArgs a = make_args3(ctx, k);
+    a.slot_to_shot = slots;
+    a.slab_by_slot = 1;
+    a.div_out = div_out;
+    CK(acoustic3d_launch_inject(const_cast<float*>(a.p_in), ctx->L3, ctx->d_shots, slots, act, ctx->d_wav, k,
+                                ctx->stream, 1));
+    CK(acoustic3d_launch_step(ctx->radius, a, act, ctx->varden, ctx->stream));
+    *launches += 2;
+    if (gather) {
+        CK(acoustic3d_launch_gather(a.p_out, ctx->L3, ctx->d_shots, slots, act, ctx->d_rec_x, ctx->d_rec_y,
+                                    ctx->d_rec_z, ctx->d_rec_tn, ctx->nrec_max, k, ctx->stream, 1));
+        (*launches)++;
+    }
+    return SFD_OK;
+}
+
+// adjoint of forward step k: residual of step k into nu, then the adjoint step
+int g3_adj_step(sfd_ctx* ctx, const int* slots, int act, int k, const float* div, long long* launches) {
+    Acou3DArgs a = make_args3(ctx, k);
+    const long long fsA = (long long)ctx->g3_G * ctx->L3.shot_stride;
+    const int i = (k + 1) & 1, o = k & 1;
+    float* A = ctx->g3_adj;
+    a.p_in = A + i * fsA; a.p_out = A + o * fsA;
+    a.vx_in = A + (2 + i) * fsA; a.vx_out = A + (2 + o) * fsA;
+    a.vy_out = A + (4 + o) * fsA;
+    a.vz_out = A + (6 + o) * fsA;
+    a.tm_p = ctx->g3_tmaps[i];
+    a.tm_vy = ctx->g3_tmaps[2 + i];
+    a.tm_vz = ctx->g3_tmaps[4 + i];
+    a.slot_to_shot = slots;
+    a.slab_by_slot = 1;
+    a.shots = ctx->d_shots;
+    a.adj_div = div;
+    a.adj_g = ctx->g3_gseg;
+    a.adj_lam = ctx->d_lam;
+    a.nt_max = ctx->nt_max;
+    a.step = k;
+    a.adj_radius = ctx->radius;
+    a.adj_c[0] = ctx->varden ? 1.0f : a.dtdx / ctx->den_c;
+    a.adj_c[1] = ctx->varden ? 1.0f : a.dtdy / ctx->den_c;
+    a.adj_c[2] = ctx->varden ? 1.0f : a.dtdz / ctx->den_c;
+    CK(acoustic3d_launch_adj_inject(A + i * fsA, a, ctx->d_rec_x, ctx->d_rec_y, ctx->d_rec_z, ctx->d_res, act,
+                                    ctx->nrec_max, ctx->stream));
+    CK(acoustic3d_launch_step(ctx->radius, a, act, ctx->varden, ctx->stream, true));
+    *launches += 2;
+    return SFD_OK;
+}
+
+// P, Vx, Vy, Vz of parity b (G slabs) to or from checkpoint store `ck` slot j
+int g3_copy_state(sfd_ctx* ctx, float* ck, int j, int b, bool save) {
+    const size_t fsG = (size_t)ctx->g3_G * ctx->L3.shot_stride;
+    const size_t fsS = (size_t)ctx->state_slabs * ctx->L3.shot_stride;
+    for (int f = 0; f < 4; f++) {
+        float* st = ctx->d_state + (2 * f + b) * fsS;
+        float* cp = ck + ((size_t)j * 4 + f) * fsG;
+        CK(cudaMemcpyAsync(save ? cp : st, save ? st : cp, sizeof(float) * fsG, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return SFD_OK;
+}
+
+// the gradient of one group: shots h_slots[0..n) (launch slot order, longest record first),
+// device slot list `slots`
+int g3_group(sfd_ctx* ctx, const int* slots, const std::vector<int>& h_slots, long long* launches) {
+    int rc;
+    const int n = (int)h_slots.size();
+    const int nt = ctx->h_shots[h_slots[0]].nt;
+    auto act = [&](int k) {
+        int a = 0;
+        while (a < n && ctx->h_shots[h_slots[a]].nt > k) a++;
+        return a;
+    };
+    const size_t fsG = (size_t)ctx->g3_G * ctx->L3.shot_stride;
+    const int C1 = ctx->g3_C1, C2 = ctx->g3_C2;
+    CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->g3_adj, 0, sizeof(float) * fsG * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->g3_gseg, 0, sizeof(float) * fsG, ctx->stream));
+    CK(cudaMemsetAsync(ctx->g3_gacc, 0, sizeof(double) * fsG, ctx->stream));
+    // forward with outer checkpoints and the records
+    for (int k = 0; k < nt; k++) {
+        if (k % C1 == 0 && (rc = g3_copy_state(ctx, ctx->g3_ck1, k / C1, k & 1, true))) return rc;
+        if ((rc = g3_fwd_step(ctx, slots, act(k), k, nullptr, true, launches))) return rc;
+    }
+    for (int s : h_slots) {
+        const ShotDev& sd = ctx->h_shots[s];
+        CK(launch_residual(ctx->d_rec_tn + sd.rec_base, ctx->d_obs_tn + sd.rec_base, ctx->d_res + sd.rec_base,
+                           (long long)sd.nrec * sd.nt, ctx->d_misfit, ctx->stream));
+        (*launches)++;
+    }
+    // innermost segment [a, b) restored from store ck slot j: recompute keeping D_k, transpose
+    auto inner = [&](float* ck, int j, int a, int b) -> int {
+        int r;
+        if ((r = g3_copy_state(ctx, ck, j, a & 1, false))) return r;
+        for (int k = a; k < b; k++)
+            if ((r = g3_fwd_step(ctx, slots, act(k), k, ctx->g3_div + (size_t)(k - a) * fsG, false, launches)))
+                return r;
+        for (int k = b - 1; k >= a; k--)
+            if ((r = g3_adj_step(ctx, slots, act(k), k, ctx->g3_div + (size_t)(k - a) * fsG, launches))) return r;
+        CK(launch_accumulate(ctx->g3_gacc, ctx->g3_gseg, (long long)fsG, ctx->stream));
+        CK(cudaMemsetAsync(ctx->g3_gseg, 0, sizeof(float) * fsG, ctx->stream));
+        (*launches)++;
+        return SFD_OK;
+    };
+    const int n1 = (nt + C1 - 1) / C1;
+    for (int j1 = n1 - 1; j1 >= 0; j1--) {
+        const int k0 = j1 * C1, k1 = std::min(k0 + C1, nt);
+        if (C2 >= C1) {
+            if ((rc = inner(ctx->g3_ck1, j1, k0, k1))) return rc;
+            continue;
+        }
+        if ((rc = g3_copy_state(ctx, ctx->g3_ck1, j1, k0 & 1, false))) return rc;
+        for (int k = k0; k < k1; k++) {
+            if ((k - k0) % C2 == 0 && (rc = g3_copy_state(ctx, ctx->g3_ck2, (k - k0) / C2, k & 1, true))) return rc;
+            if ((rc = g3_fwd_step(ctx, slots, act(k), k, nullptr, false, launches))) return rc;
+        }
+        for (int j2 = (k1 - k0 + C2 - 1) / C2 - 1; j2 >= 0; j2--) {
+            const int a = k0 + j2 * C2, b = std::min(a + C2, k1);
+            if ((rc = inner(ctx->g3_ck2, j2, a, b))) return rc;
+        }
+    }
+    CK(acoustic3d_launch_gradient_reduce(ctx->g3_gacc, n, ctx->L3, ctx->d_vp, ctx->d_grad, ctx->stream));
+    (*launches)++;
+    return SFD_OK;
+}
+
+int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched) {
+    int rc;
+    auto t0 = std::chrono::steady_clock::now();
+    Plan3 p;
+    if ((rc = plan3_choose(ctx, batched ? ctx->nshot : 1, &p))) return rc;
+    if ((rc = g3_alloc(ctx, p))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total, cudaMemcpyHostToDevice, ctx->stream));
+    long long launches = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_misfit, 0, sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_lam, 0, sizeof(float) * (size_t)ctx->nshot * ctx->nt_max, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_rec_tn, 0, sizeof(float) * std::max<long long>(1, ctx->rec_total), ctx->stream));
+    CK(launch_records_transpose_in(ctx->d_obs_nt, ctx->d_obs_tn, ctx->d_shots, ctx->nshot, ctx->nrec_max, ctx->nt_max,
+                                   ctx->stream));
+    launches++;
+    // groups: consecutive runs of the launch order (longest record first), or one shot each
+    const std::vector<int>& ord = batched ? ctx->order : ctx->h_ident_order;
+    const int* dslots = batched ? ctx->d_slot : ctx->d_ident;
+    const int G = batched ? p.G : 1;
+    for (int g0 = 0; g0 < ctx->nshot; g0 += G) {
+        const std::vector<int> hs(ord.begin() + g0, ord.begin() + std::min(ctx->nshot, g0 + G));
+        if ((rc = g3_group(ctx, dslots + g0, hs, &launches))) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    int err = 0;
+    CK(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_err(ctx, SFD_ERR_TIMEOUT, "a 3-D step kernel gave up waiting for its plane loads");
+    ctx->timing.loop_ms = ms;
+    ctx->timing.device_ms = ms;
+    ctx->timing.launches = launches;
+    ctx->timing.graph = 0;
+    ctx->timing.kernel_variant = 60 + (p.C2 < p.C1 ? 2 : 1);
+    double pts = 0;
+    for (const auto& sd : ctx->h_shots) pts += (double)sd.nx * ctx->g.ny * ctx->g.nz * sd.nt;
+    ctx->timing.point_updates = (p.C2 < p.C1 ? 4.0 : 3.0) * pts;  // forward, recomputation(s), adjoint
+    double mis = 0;
+    CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
+    if (misfit) *misfit = (float)mis;
+    ctx->have_grad = true;
+    const size_t nm = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    if (grad_vp) {
+        std::vector<double> g(nm);
+        CK(cudaMemcpy(g.data(), ctx->d_grad, nm * sizeof(double), cudaMemcpyDeviceToHost));
+        // source scaling: P[src] -= (dt DEN Vp) w[k]  ->  -dt DEN sum_k lambda_k[src] w[k]
+        std::vector<float> lam((size_t)ctx->nshot * ctx->nt_max);
+        CK(cudaMemcpy(lam.data(), ctx->d_lam, lam.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < ctx->nshot; s++) {
+            const ShotDev& sd = ctx->h_shots[s];
+            const size_t mi = ((size_t)sd.sx * ctx->g.ny + sd.sy) * ctx->g.nz + sd.sz;
+            const double den = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
+            double sw = 0;
+            for (int j = 0; j < sd.nt; j++) sw += (double)lam[(size_t)s * ctx->nt_max + j] * ctx->h_wav[sd.wav_off + j];
+            g[mi] += -(double)ctx->g.dt * den * sw;
+        }
+        for (size_t i = 0; i < nm; i++) grad_vp[i] = (float)g[i];
+    }
+    ctx->timing.h2d_bytes = (long long)sizeof(float) * ctx->rec_total;
+    ctx->timing.d2h_bytes = grad_vp ? (long long)sizeof(float) * nm : 0;
+    ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SFD_OK;
 }
 
@@ -1535,6 +1896,7 @@ int sfd_forward(sfd_ctx* ctx, float* records) {
 int sfd_forward_per_shot(sfd_ctx* ctx, float* records) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if (ctx->g.scheme == SFD_ACOUSTIC_3D && (rc = full_state_3d(ctx))) return rc;
     auto t0 = std::chrono::steady_clock::now();
     CK(cudaEventRecord(ctx->evs, ctx->stream));
     if ((rc = prologue(ctx)) != SFD_OK) return rc;
@@ -1583,6 +1945,8 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         if (fidx < 0) return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
         const Layout3D& L = ctx->L3;
         const int buf = sd.nt & 1;
+        if (ctx->state_slabs != ctx->nshot)
+            return set_err(ctx, SFD_ERR_STATE, "the 3-D wavefields of the last forward were released by the gradient");
         const long long fs = (long long)ctx->nshot * L.shot_stride;
         const float* base = ctx->d_state + (fidx + buf) * fs + (long long)shot * L.shot_stride;
         const int nz = ctx->g.nz;
@@ -1637,6 +2001,12 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         sfd_afd_sponge(sd.nx, nz, ctx->g.pml, a.data());
         for (size_t i = 0; i < a.size(); i++) out[i] = out[i] * a[i];
     }
+    return SFD_OK;
+}
+
+int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes) {
+    if (!ctx || bytes < 0) return SFD_ERR_ARG;
+    ctx->mem_limit = (size_t)bytes;
     return SFD_OK;
 }
 

@@ -250,16 +250,39 @@ struct Acou3DArgs {
     int pml;
     float sponge[256];                  // taper value at distance index q into the sponge
     const int* slot_to_shot;
+    int slab_by_slot;                   // 0: shot s lives in field slab s; 1: in the slab of its launch
+                                        // slot (the gradient's shot groups)
+    float* div_out;                     // optional: D = sum_a rd_a S-a V_a' of this step (own points)
+    // Adjoint mode (acoustic3d_launch_step with adj = true): the P, Vx, Vy, Vz slots hold the
+    // adjoint state nu = M K a Q, X, Y, Z (the 2-D recurrence of adjoint2d.cu with a y axis)
+    const ShotDev* shots;
+    const float* adj_div;               // D_k of the forward step being transposed
+    float* adj_g;                       // imaging sum: g += nu_old D_k
+    float* adj_lam;                     // [shot][nt_max]: adjoint of P at the source cell
+    int nt_max, step;
+    int adj_radius;                     // R: the update mask of the receiver injection
+    float adj_c[3];                     // dt / (d_a den_c) (constant density), 1 with variable density
 };
-// one time step of all active shots: velocities, then pressure, sponge (one launch)
-cudaError_t acoustic3d_launch_step(int radius, const Acou3DArgs& a, int active, bool varden, cudaStream_t st);
+// one time step of all active shots: velocities, then pressure, sponge (one launch); adj: the
+// adjoint of step a.step instead
+cudaError_t acoustic3d_launch_step(int radius, const Acou3DArgs& a, int active, bool varden, cudaStream_t st,
+                                   bool adj = false);
 // P_in[source] -= inj_scale * w[step] for the active shots (before the step)
 cudaError_t acoustic3d_launch_inject(float* p, const Layout3D& L, const ShotDev* shots, const int* slot_to_shot,
-                                     int active, const float* wavelets, int step, cudaStream_t st);
+                                     int active, const float* wavelets, int step, cudaStream_t st,
+                                     int slab_by_slot = 0);
 // records[rec_base + step * nrec + r] = P_out at receiver r (after the step)
 cudaError_t acoustic3d_launch_gather(const float* p, const Layout3D& L, const ShotDev* shots,
                                      const int* slot_to_shot, int active, const int* rec_x, const int* rec_y,
-                                     const int* rec_z, float* records, int nrec_max, int step, cudaStream_t st);
+                                     const int* rec_z, float* records, int nrec_max, int step, cudaStream_t st,
+                                     int slab_by_slot = 0);
+// adjoint: nu[receiver] += M a K res[step] (res [nt][nrec] per shot) before adjoint step `step`
+cudaError_t acoustic3d_launch_adj_inject(float* nu, const Acou3DArgs& a, const int* rec_x, const int* rec_y,
+                                         const int* rec_z, const float* res, int active, int nrec_max,
+                                         cudaStream_t st);
+// grad[x][y][z] += -(2 / vp) sum over the slabs [0, nslab) of acc (double, field layout)
+cudaError_t acoustic3d_launch_gradient_reduce(const double* acc, int nslab, const Layout3D& L, const float* vp,
+                                              double* grad, cudaStream_t st);
 // TMA box extents (z, y) of the P, Vy and Vz boxes at this radius; false if unsupported
 bool acoustic3d_boxes(int radius, int box_p[2], int box_vy[2], int box_vz[2]);
 

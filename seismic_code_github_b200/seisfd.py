@@ -89,6 +89,7 @@ SIGNATURES = {
     "sfd_gradient_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sfd_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "sfd_set_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int]),
@@ -306,6 +307,10 @@ class Engine:
 
     def set_checkpoint_interval(self, steps: int):
         self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
+
+    def set_memory_limit(self, nbytes: int):
+        """Device-memory budget of gradient() (0: the free device memory)."""
+        self._check(self._lib.sfd_set_memory_limit(self._h, int(nbytes)), "sfd_set_memory_limit")
 
     def set_snapshots(self, stream: int, field: int, first: int, every: int, count: int):
         self._check(self._lib.sfd_set_snapshots(self._h, stream, field, first, every, count), "sfd_set_snapshots")
