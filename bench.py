@@ -231,6 +231,47 @@ def measure_gradient(args, dev):
             "misfit": float(mis), "gradient_accuracy": "relL2 vs FP64 adjoint oracle 7.6e-7 (tests/test_gradient_gpu.py)"}
 
 
+def measure_gradient_sharded(args, dev, world, rank):
+    """Config 4 on N GPUs: every rank takes the gradient of its round-robin share of the shots
+    (forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90:124-141) and one all-reduce (NCCL)
+    sums the per-rank gradients and misfits.  Time: device time of the local gradient plus the
+    all-reduce, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import sharding as SH
+    from seismic_code_github_b200 import workloads as W
+    case, vp_true = W.config4(nshot=args.grad_nshot, nt=args.grad_nt)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    mine = SH.shard_shots(len(case.src_x), rank, world)
+    shots = [S.ShotSpec(case.src_x[i], case.src_z[i], rx, rz, w) for i in mine]
+    with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16,
+                  device=dev) as e:
+        e.set_model(vp_true, case.den)
+        e.set_shots(shots)
+        obs = e.forward().copy()
+        e.set_model(case.vp, case.den)
+        e.set_checkpoint_interval(case.extra["checkpoint_interval"])
+        mis, g, _ = e.gradient(obs)  # warm-up
+        SH.allreduce_gradient(mis, g, device=f"cuda:{dev}")
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        mis, g, _ = e.gradient(obs)
+        mis_all, g_all, _ = SH.allreduce_gradient(mis, g, device=f"cuda:{dev}")
+        t1.record()
+        torch.cuda.synchronize()
+    ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=f"cuda:{dev}")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    return {"workload": f"config 4 gradient, {len(case.src_x)} shots sharded round-robin over {world} GPUs, "
+                        f"one all-reduce of the {g.size * 4 / 1e6:.1f} MB gradient",
+            "shots_per_s": len(case.src_x) / (ms.item() / 1e3), "ms": ms.item(), "misfit": float(mis_all),
+            "grad_norm": float(np.linalg.norm(g_all))}
+
+
 def measure_viscoacoustic(args, dev):
     """Config 3: 16 viscoacoustic shots (uneven record lengths) in one batched time loop; the CPU
     figure is the restated Fortran step (oracle/q_oracle.cpp, OpenMP, all host cores) on one
@@ -277,6 +318,81 @@ def measure_viscoacoustic(args, dev):
                                          f"the difference of a {steps + 1}- and a 1-sample run on the {Nz}x{Nx} "
                                          f"padded grid ({steps} steps)"}
     return out
+
+
+def measure_q_gradient(args, dev):
+    """Config-3 geometry: the viscoacoustic gradient d misfit / d vp and d misfit / d (1/Q) of 16
+    shots (uneven record lengths), observed data from the Q field scaled by 0.8, batched (one
+    CUDA graph) against the plain per-shot schedule on a subset of the shots."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.qg_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    nts = [max(1, int(round(nt * args.qg_nt_scale))) for nt in c["nt"]]
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, nt, c["dt"], c["f0"]))
+             for sx, sz, nt in zip(c["src_x"], c["src_z"], nts)]
+    with S.Engine(S.VISCOAC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"], device=dev) as e:
+        e.set_model(c["vp"], c["rho"], (c["q"] * 0.8).astype(np.float32))
+        e.set_shots(shots)
+        obs = e.forward().copy()
+        e.set_model(c["vp"], c["rho"], c["q"])
+        e.gradient(obs, want_invq=True)  # warm-up: allocation and graph capture
+        ms = []
+        for _ in range(args.qg_steps):
+            e.gradient(obs, want_invq=True)
+            ms.append(e.timing()["loop_ms"])
+        t = e.timing()
+        sub = shots[: args.qg_plain_shots]
+        offs = np.cumsum([0] + [s.nrec * s.nt for s in shots])
+        e.set_shots(sub)
+        e.gradient(obs[: offs[len(sub)]], want_invq=True, per_shot=True)
+        tp = e.timing()
+    bt = float(np.median(ms))
+    return {"workload": f"config 3 geometry: viscoacoustic gradient d/dvp and d/d(1/Q), {c['NZ']}x{c['NX']} interior "
+                        f"({Nz}x{Nx} padded), {len(shots)} shots, nt {min(nts)}-{max(nts)}",
+            "batched_shots_per_s": len(shots) / (bt / 1e3), "batched_ms": bt, "batched_launches": t["launches"],
+            "plain_shots_per_s": len(sub) / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"], "plain_shots": len(sub),
+            "batched_over_plain": (len(shots) / bt) / (len(sub) / tp["loop_ms"]),
+            "gradient_accuracy": "relL2 vs FP64 adjoint oracle 1.5e-6 (vp), 2.6e-6 (1/Q) (tests/test_q_gradient_gpu.py)"}
+
+
+def measure_3d_gradient(args, dev):
+    """Config-5 geometry (612^3 padded, order 8): the 3-D gradient of a few shots with record
+    lengths scaled by --d3g-nt-scale; the library plans shot groups and checkpoint levels to the
+    device memory.  Batched against the per-shot schedule on one shot."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config5(nshot=args.d3g_nshot, nt_scale=args.d3g_nt_scale)
+    n, d = c["n"], c["d"]
+    vp = np.empty((n, n, n), np.float32)
+    for x0 in range(0, n, 64):
+        vp[x0:x0 + 64] = c["vp_slab"](x0, min(n, x0 + 64))
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_RIC, nt, c["dt"], c["f0"], 80), sy=sy, rec_y=ry)
+             for (sx, sy, sz), (rx, ry, rz), nt in zip(c["src"], c["rec"], c["nt"])]
+    with S.Engine(S.ACOUSTIC_3D, n, n, d, d, c["dt"], c["PML"], order=8, ny=n, dy=d, device=dev) as e:
+        e.set_model((vp * 1.02).astype(np.float32))
+        e.set_shots(shots)
+        obs = e.forward().copy()
+        e.set_model(vp)
+        e.gradient(obs)
+        t = e.timing()
+        sub = shots[:1]
+        e.set_shots(sub)
+        e.gradient(obs[: sub[0].nrec * sub[0].nt], per_shot=True)
+        tp = e.timing()
+    del vp
+    levels = 2 if t["kernel_variant"] == 62 else 1
+    pts = float(n) ** 3 * sum(c["nt"])
+    return {"workload": f"config 5 geometry: 3-D gradient d/dvp, {c['N']}^3 interior ({n}^3 padded), {len(shots)} shots, "
+                        f"record lengths 1500-2500 scaled by {args.d3g_nt_scale} (nt {min(c['nt'])}-{max(c['nt'])})",
+            "batched_shots_per_s": len(shots) / (t["loop_ms"] / 1e3), "batched_ms": t["loop_ms"],
+            "checkpoint_levels": levels, "passes": t["point_updates"] / pts,
+            "gpts_per_s_all_passes": t["point_updates"] / (t["loop_ms"] / 1e3) / 1e9,
+            "plain_shots_per_s": 1.0 / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"],
+            "batched_over_plain": (len(shots) / t["loop_ms"]) / (1.0 / tp["loop_ms"]),
+            "gradient_accuracy": "relL2 vs FP64 3-D adjoint oracle 6.7e-7 (tests/test_gradient3d_gpu.py)"}
 
 
 def measure_3d(args, dev):
@@ -422,7 +538,10 @@ def run_ours(args, world, rank, local):
                  "batched_full_shots_per_s": world * case.nshot * args.steps / (dev_ms_max / 1e3)}
 
     eng.close()
+    grad_sharded = None
     if dist is not None:
+        if args.grad_steps > 0:
+            grad_sharded = measure_gradient_sharded(args, dev, world, rank)
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
@@ -456,10 +575,16 @@ def run_ours(args, world, rank, local):
         line["plain_vs_batched"] = plain
     if world == 1 and args.grad_steps > 0:
         line["gradient"] = measure_gradient(args, dev)
+    if grad_sharded is not None:
+        line["gradient_sharded"] = grad_sharded
     if world == 1 and args.q_steps > 0:
         line["viscoacoustic"] = measure_viscoacoustic(args, dev)
+    if world == 1 and args.qg_steps > 0:
+        line["viscoacoustic_gradient"] = measure_q_gradient(args, dev)
     if world == 1 and args.d3_steps > 0:
         line["acoustic3d"] = measure_3d(args, dev)
+    if world == 1 and args.d3g_nshot > 0:
+        line["acoustic3d_gradient"] = measure_3d_gradient(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_reference_sample(case, args.ref_steps).items() if k != "wall_s"}
     print(json.dumps(line), flush=True)
@@ -489,6 +614,12 @@ def main():
     ap.add_argument("--d3-nshot", type=int, default=16)
     ap.add_argument("--d3-nt-scale", type=float, default=0.05)
     ap.add_argument("--d3-cpu-steps", type=int, default=3)
+    ap.add_argument("--qg-steps", type=int, default=1, help="timed viscoacoustic gradients (0 = skip)")
+    ap.add_argument("--qg-nshot", type=int, default=16)
+    ap.add_argument("--qg-nt-scale", type=float, default=1.0)
+    ap.add_argument("--qg-plain-shots", type=int, default=2)
+    ap.add_argument("--d3g-nshot", type=int, default=4, help="3-D gradient shots (0 = skip)")
+    ap.add_argument("--d3g-nt-scale", type=float, default=0.05)
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":
