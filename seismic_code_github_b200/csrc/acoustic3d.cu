@@ -289,6 +289,14 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
         const float* st = smem + stg * K::STAGE;
         float* nby = smem + K::OFF_NB + stg * K::NBUF;  // new Vy region of this plane
         float* nbz = nby + K::NB_NZ;                     // new Vz region of this plane
+        // adjoint: D_k and the imaging sum of the own points of plane s, requested before the
+        // velocity phases so that their latency is covered
+        float4 adk = make_float4(0.f, 0.f, 0.f, 0.f), agk = adk;
+        if (ADJ && s >= R && own_ok) {
+            const long long pofs = shot_off + (long long)s * L.xstride + own_off;
+            adk = __ldg(reinterpret_cast<const float4*>(a.adj_div + pofs));
+            agk = *reinterpret_cast<const float4*>(a.adj_g + pofs);
+        }
         // the loads of the next plane's own values are issued as soon as this plane's are used
         const int xv = s + R - 1;  // plane of this iteration's new Vx
         const bool edge = !yz_int || !(s >= E && xv < nx - E);
@@ -501,8 +509,8 @@ __global__ void __launch_bounds__(kThreads, 2) acoustic3d_step_kernel(const __gr
                 if (edge) pn = mul4(mul4(pn, edge_f(io, xpad_s, fx_s)), edge_k(io, kx_s));
                 if (own_ok) {
                     st4s(a.p_out + pofs, pn);
-                    const float4 dk = __ldg(reinterpret_cast<const float4*>(a.adj_div + pofs));
-                    float4 g = *reinterpret_cast<const float4*>(a.adj_g + pofs);
+                    const float4 dk = adk;
+                    float4 g = agk;
                     g = make_float4(fmaf(po.x, dk.x, g.x), fmaf(po.y, dk.y, g.y), fmaf(po.z, dk.z, g.z),
                                     fmaf(po.w, dk.w, g.w));
                     st4s(a.adj_g + pofs, g);

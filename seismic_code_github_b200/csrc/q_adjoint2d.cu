@@ -40,6 +40,8 @@ constexpr int HZ = 8;              // z halo rounded for float4 staging
 constexpr int SROWS = TX + 2 * H;  // staged rows x0-5 .. x0+TX+4
 constexpr int SW = TZ + 2 * HZ;    // staged columns z0-8 .. z0+TZ+7
 constexpr int SMEM = SROWS * SW;
+constexpr int kPer = TX * TZ / kThreads;  // cells per thread
+constexpr int kNB = 4;                    // cells per load batch
 
 struct Tile {
     int shot, tile, x0, z0;
@@ -118,34 +120,51 @@ __global__ void __launch_bounds__(kThreads) q_adj_velocity_kernel(const __grid_c
     float c[5];
 #pragma unroll
     for (int m = 0; m < 5; m++) c[m] = a.a[m];
-    for (int i = threadIdx.x; i < TX * TZ; i += kThreads) {
-        const int r = i / TZ, z = i - r * TZ;
-        const int gx = t.x0 + r, gz = t.z0 + z;
-        if (gx >= nx || gz >= nz) continue;
-        const float* p1s = sT1 + (r + H) * SW + z + HZ;
-        const float* p4s = sT4 + (r + H) * SW + z + HZ;
-        auto T1 = [&](int dx, int dz) { return p1s[dx * SW + dz]; };
-        auto T4 = [&](int dx, int dz) { return p4s[dx * SW + dz]; };
-        float s1 = 0.0f, s4 = 0.0f;
+    // kNB cells per batch: the global loads of a batch are issued before its arithmetic
+    for (int j0 = 0; j0 < kPer; j0 += kNB) {
+        float vxo[kNB], vzo[kNB], bu[kNB];
+        long long cc[kNB];
+        bool ok[kNB];
 #pragma unroll
-        for (int m = 0; m < 5; m++) {
-            // Dx1^T: t(x-1-m, z-1-m) - t(x+m, z+m) + t(x-1-m, z+m) - t(x+m, z-1-m); Dz1^T flips the cross terms
-            const float a1 = T1(-1 - m, -1 - m) - T1(m, m), b1 = T1(-1 - m, m) - T1(m, -1 - m);
-            const float a4 = T4(-1 - m, -1 - m) - T4(m, m), b4 = T4(-1 - m, m) - T4(m, -1 - m);
-            s1 = fmaf(c[m], a1 + b1, s1);
-            s4 = fmaf(c[m], a4 - b4, s4);
+        for (int u = 0; u < kNB; u++) {
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            ok[u] = gx < nx && gz < nz;
+            cc[u] = cell(a, t.shot, gx, gz);
+            if (ok[u]) {
+                vxo[u] = a.avx[cc[u]];
+                vzo[u] = a.avz[cc[u]];
+                bu[u] = __ldg(a.busg + (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz);
+            }
         }
-        const long long cc = cell(a, t.shot, gx, gz);
-        const float ax = sp(gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
-        const float az = sp(gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
-        const float vx = ax * fmaf(a.hx, s1, a.avx[cc]);
-        const float vz = az * fmaf(a.hz, s4, a.avz[cc]);
-        const long long mi = (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
-        const float db = dt * __ldg(a.busg + mi);
-        a.avx[cc] = vx;
-        a.avz[cc] = vz;
-        a.qx[cc] = db * vx;
-        a.qz[cc] = db * vz;
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            if (!ok[u]) continue;
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            const float* p1s = sT1 + (r + H) * SW + z + HZ;
+            const float* p4s = sT4 + (r + H) * SW + z + HZ;
+            auto T1 = [&](int dx, int dz) { return p1s[dx * SW + dz]; };
+            auto T4 = [&](int dx, int dz) { return p4s[dx * SW + dz]; };
+            float s1 = 0.0f, s4 = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 5; m++) {
+                // Dx1^T: t(x-1-m, z-1-m) - t(x+m, z+m) + t(x-1-m, z+m) - t(x+m, z-1-m); Dz1^T flips the cross terms
+                const float a1 = T1(-1 - m, -1 - m) - T1(m, m), b1 = T1(-1 - m, m) - T1(m, -1 - m);
+                const float a4 = T4(-1 - m, -1 - m) - T4(m, m), b4 = T4(-1 - m, m) - T4(m, -1 - m);
+                s1 = fmaf(c[m], a1 + b1, s1);
+                s4 = fmaf(c[m], a4 - b4, s4);
+            }
+            const float ax = sp(gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
+            const float az = sp(gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
+            const float vx = ax * fmaf(a.hx, s1, vxo[u]);
+            const float vz = az * fmaf(a.hz, s4, vzo[u]);
+            const float db = dt * bu[u];
+            a.avx[cc[u]] = vx;
+            a.avz[cc[u]] = vz;
+            a.qx[cc[u]] = db * vx;
+            a.qz[cc[u]] = db * vz;
+        }
     }
     // wavelet gradient: dw_k = dt / dz^2 sum over the source stamp of sx^ (QS:1384 transposed)
     const ShotDev& sd = t.sd;
@@ -187,40 +206,58 @@ __global__ void __launch_bounds__(kThreads) q_adj_stress_kernel(const __grid_con
 #pragma unroll
     for (int m = 0; m < 5; m++) c[m] = a.a[m];
     const float dt = a.dt, f = a.f_mem;
-    for (int i = threadIdx.x; i < TX * TZ; i += kThreads) {
-        const int r = i / TZ, z = i - r * TZ;
-        const int gx = t.x0 + r, gz = t.z0 + z;
-        if (gx >= nx || gz >= nz) continue;
-        const float* px = sQx + (r + H) * SW + z + HZ;
-        const float* pz = sQz + (r + H) * SW + z + HZ;
-        auto QX = [&](int dx, int dz) { return px[dx * SW + dz]; };
-        auto QZ = [&](int dx, int dz) { return pz[dx * SW + dz]; };
-        float sx = 0.0f, sz = 0.0f;
+    for (int j0 = 0; j0 < kPer; j0 += kNB) {
+        float hsx[kNB], hsz[kNB], hsr[kNB], hrx[kNB], hrz[kNB], hrr[kNB], d1[kNB], d4[kNB], g1[kNB], g2[kNB];
+        long long cc[kNB];
+        bool ok[kNB];
 #pragma unroll
-        for (int m = 0; m < 5; m++) {
-            // Dx0^T: t(x-m, z-m) - t(x+1+m, z+1+m) + t(x-m, z+1+m) - t(x+1+m, z-m); Dz0^T flips the cross terms
-            const float ax_ = QX(-m, -m) - QX(1 + m, 1 + m), bx_ = QX(-m, 1 + m) - QX(1 + m, -m);
-            const float az_ = QZ(-m, -m) - QZ(1 + m, 1 + m), bz_ = QZ(-m, 1 + m) - QZ(1 + m, -m);
-            sx = fmaf(c[m], ax_ + bx_, sx);
-            sz = fmaf(c[m], az_ - bz_, sz);
+        for (int u = 0; u < kNB; u++) {
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            ok[u] = gx < nx && gz < nz;
+            const long long c = cell(a, t.shot, gx, gz);
+            cc[u] = c;
+            if (ok[u]) {
+                hsx[u] = a.asx[c]; hsz[u] = a.asz[c]; hsr[u] = a.asr[c];
+                hrx[u] = a.arx[c]; hrz[u] = a.arz[c]; hrr[u] = a.arr[c];
+                d1[u] = __ldg(a.d1 + c); d4[u] = __ldg(a.d4 + c);
+                g1[u] = a.g1[c]; g2[u] = a.g2[c];
+            }
         }
-        const float aS = fmaf(a.hx, sx, a.hz * sz);
-        const long long cc = cell(a, t.shot, gx, gz);
-        const float axs = sp(gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-        const float azs = sp(gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
-        const float u1 = axs * a.asx[cc], u4 = azs * a.asz[cc];
-        const float w1 = axs * a.arx[cc], w4 = azs * a.arz[cc];
-        const float srh = a.asr[cc], rrh = a.arr[cc];
-        const float aR = fmaf(f, rrh, dt * srh);
-        const float d1 = __ldg(a.d1 + cc), d4 = __ldg(a.d4 + cc);
-        a.g1[cc] += fmaf(d1, u1, d4 * u4);
-        a.g2[cc] += fmaf(d1, w1, d4 * w4);
-        a.asx[cc] = u1 + aS;
-        a.asz[cc] = u4 + aS;
-        a.asr[cc] = srh + aS;
-        a.arx[cc] = w1 + aR;
-        a.arz[cc] = w4 + aR;
-        a.arr[cc] = rrh + aR;
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            if (!ok[u]) continue;
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            const float* px = sQx + (r + H) * SW + z + HZ;
+            const float* pz = sQz + (r + H) * SW + z + HZ;
+            auto QX = [&](int dx, int dz) { return px[dx * SW + dz]; };
+            auto QZ = [&](int dx, int dz) { return pz[dx * SW + dz]; };
+            float sx = 0.0f, sz = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 5; m++) {
+                // Dx0^T: t(x-m, z-m) - t(x+1+m, z+1+m) + t(x-m, z+1+m) - t(x+1+m, z-m); Dz0^T flips the cross terms
+                const float ax_ = QX(-m, -m) - QX(1 + m, 1 + m), bx_ = QX(-m, 1 + m) - QX(1 + m, -m);
+                const float az_ = QZ(-m, -m) - QZ(1 + m, 1 + m), bz_ = QZ(-m, 1 + m) - QZ(1 + m, -m);
+                sx = fmaf(c[m], ax_ + bx_, sx);
+                sz = fmaf(c[m], az_ - bz_, sz);
+            }
+            const float aS = fmaf(a.hx, sx, a.hz * sz);
+            const long long cu = cc[u];
+            const float axs = sp(gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
+            const float azs = sp(gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
+            const float u1 = axs * hsx[u], u4 = azs * hsz[u];
+            const float w1 = axs * hrx[u], w4 = azs * hrz[u];
+            const float aR = fmaf(f, hrr[u], dt * hsr[u]);
+            a.g1[cu] = g1[u] + fmaf(d1[u], u1, d4[u] * u4);
+            a.g2[cu] = g2[u] + fmaf(d1[u], w1, d4[u] * w4);
+            a.asx[cu] = u1 + aS;
+            a.asz[cu] = u4 + aS;
+            a.asr[cu] = hsr[u] + aS;
+            a.arx[cu] = w1 + aR;
+            a.arz[cu] = w4 + aR;
+            a.arr[cu] = hrr[u] + aR;
+        }
     }
     // residual of step k-1 at the receivers of this tile (QM:452-459 transposed): S^ -> sx^, sz^, sr^
     const ShotDev& sd = t.sd;

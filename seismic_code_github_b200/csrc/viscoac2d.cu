@@ -32,6 +32,9 @@ constexpr int HZ = 8;                   // z halo rounded for float4 staging
 constexpr int SROWS = TX + 2 * H;       // 74
 constexpr int SW = TZ + 2 * HZ;         // 80
 constexpr int SMEM = SROWS * SW;        // floats per staged field
+constexpr int kPer = TX * TZ / kThreads;  // cells per thread
+constexpr int kNB = 4;                  // cells per load batch
+static_assert(kPer % kNB == 0, "whole batches");
 
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
@@ -111,21 +114,39 @@ __global__ void __launch_bounds__(kThreads) q_velocity_kernel(const __grid_const
     const int nx = t.sd.nx, nz = a.nz;
     const float* tb = a.spg;
     const int st = a.spg_stride;
-    for (int i = threadIdx.x; i < TX * TZ; i += kThreads) {
-        const int r = i / TZ, z = i - r * TZ;
-        const int gx = t.x0 + r, gz = t.z0 + z;
-        if (gx >= nx || gz >= nz) continue;
-        const float d1 = rsg<true, 0>(sS, r + H, z + HZ, a.a, a.hx);
-        const float d2 = rsg<false, 0>(sS, r + H, z + HZ, a.a, a.hz);
-        const long long mi = (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
-        const float dtb = fm(a.dt, __ldg(a.busg + mi));
-        const long long c = cell(a, t.shot, gx, gz);
-        float vx = fa(a.vx[c], fm(dtb, d1));
-        float vz = fa(a.vz[c], fm(dtb, d2));
-        vx = xs(vx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);   // spgxn, spgxp
-        vz = xs(vz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);   // spgzn, spgzp
-        a.vx[c] = fa(vx, 0.0f);  // vx = vxx + vxz with vxz = 0
-        a.vz[c] = fa(0.0f, vz);  // vz = vzx + vzz with vzx = 0
+    // NB cells per batch: all global loads of a batch are issued before its arithmetic, so that
+    // their latencies overlap (thread t handles column z = t % TZ of rows t / TZ + 4 j)
+    for (int j0 = 0; j0 < kPer; j0 += kNB) {
+        float vxo[kNB], vzo[kNB], bu[kNB];
+        long long cc[kNB];
+        bool ok[kNB];
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            ok[u] = gx < nx && gz < nz;
+            cc[u] = cell(a, t.shot, gx, gz);
+            if (ok[u]) {
+                vxo[u] = a.vx[cc[u]];
+                vzo[u] = a.vz[cc[u]];
+                bu[u] = __ldg(a.busg + (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            if (!ok[u]) continue;
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            const float d1 = rsg<true, 0>(sS, r + H, z + HZ, a.a, a.hx);
+            const float d2 = rsg<false, 0>(sS, r + H, z + HZ, a.a, a.hz);
+            const float dtb = fm(a.dt, bu[u]);
+            float vx = fa(vxo[u], fm(dtb, d1));
+            float vz = fa(vzo[u], fm(dtb, d2));
+            vx = xs(vx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);   // spgxn, spgxp
+            vz = xs(vz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);   // spgzn, spgzp
+            a.vx[cc[u]] = fa(vx, 0.0f);  // vx = vxx + vxz with vxz = 0
+            a.vz[cc[u]] = fa(0.0f, vz);  // vz = vzx + vzz with vzx = 0
+        }
     }
 }
 
@@ -143,39 +164,57 @@ __global__ void __launch_bounds__(kThreads) q_stress_kernel(const __grid_constan
     const int step = a.step;
     const float wav = __ldg(a.wavelets + t.sd.wav_off + step);
     const ShotDev& sd = t.sd;
-    for (int i = threadIdx.x; i < TX * TZ; i += kThreads) {
-        const int r = i / TZ, z = i - r * TZ;
-        const int gx = t.x0 + r, gz = t.z0 + z;
-        if (gx >= nx || gz >= nz) continue;
-        const float d1 = rsg<true, 1>(sVx, r + H, z + HZ, a.a, a.hx);
-        const float d4 = rsg<false, 1>(sVz, r + H, z + HZ, a.a, a.hz);
-        const long long mi = (long long)min(sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
-        const float p1 = __ldg(a.p1 + mi), p2 = __ldg(a.p2 + mi);
-        const long long c = cell(a, t.shot, gx, gz);
-        const float rx0 = a.rx[c], rz0 = a.rz[c], rr0 = a.rr[c];
-        const float rold = fa(fa(rx0, rz0), rr0);  // QS rxx of the previous step
-        // calpstrxx (QS:993-1020) with mu = 0, split sponge (QS:800), source (QS:801)
-        float sx = fa(a.sx[c], fm(a.dt, fm(p1, d1)));
-        float sz = fa(a.sz[c], fm(a.dt, fm(p1, d4)));
-        const float sr = fa(a.sr[c], fm(a.dt, rold));
-        sx = xs(sx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);   // spg1xn, spg2xp
-        sz = xs(sz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);   // spg1zn, spg2zp
-        const int bx = gx - sd.stamp_x0, bz = gz - sd.stamp_z0;
-        if (bx >= 0 && bx < sd.stamp_w && bz >= 0 && bz < sd.stamp_h) {
-            const float g = __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz);
-            sx = fa(__fdiv_rn(fm(fm(wav, g), a.dt), a.dz2), sx);   // QS:1384
+    for (int j0 = 0; j0 < kPer; j0 += kNB) {
+        float p1[kNB], p2[kNB], sx0[kNB], sz0[kNB], sr0[kNB], rx0[kNB], rz0[kNB], rr0[kNB];
+        long long cc[kNB];
+        bool ok[kNB];
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            ok[u] = gx < nx && gz < nz;
+            cc[u] = cell(a, t.shot, gx, gz);
+            if (ok[u]) {
+                const long long mi = (long long)min(sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
+                p1[u] = __ldg(a.p1 + mi);
+                p2[u] = __ldg(a.p2 + mi);
+                const long long c = cc[u];
+                sx0[u] = a.sx[c]; sz0[u] = a.sz[c]; sr0[u] = a.sr[c];
+                rx0[u] = a.rx[c]; rz0[u] = a.rz[c]; rr0[u] = a.rr[c];
+            }
         }
-        // calprxx (QS:1135-1170)
-        float rx = fa(rx0, fm(a.f_mem, fm(p2, d1)));
-        float rz = fa(rz0, fm(a.f_mem, fm(p2, d4)));
-        const float rr = fa(rr0, fm(a.f_mem, rold));
-        rx = xs(rx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-        rz = xs(rz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
-        a.sx[c] = sx; a.sz[c] = sz; a.sr[c] = sr;
-        a.rx[c] = rx; a.rz[c] = rz; a.rr[c] = rr;
-        if (a.d1_out) {  // gradient recomputation keeps the derivatives for the imaging condition
-            a.d1_out[c] = d1;
-            a.d4_out[c] = d4;
+#pragma unroll
+        for (int u = 0; u < kNB; u++) {
+            if (!ok[u]) continue;
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            const long long c = cc[u];
+            const float d1 = rsg<true, 1>(sVx, r + H, z + HZ, a.a, a.hx);
+            const float d4 = rsg<false, 1>(sVz, r + H, z + HZ, a.a, a.hz);
+            const float rold = fa(fa(rx0[u], rz0[u]), rr0[u]);  // QS rxx of the previous step
+            // calpstrxx (QS:993-1020) with mu = 0, split sponge (QS:800), source (QS:801)
+            float sx = fa(sx0[u], fm(a.dt, fm(p1[u], d1)));
+            float sz = fa(sz0[u], fm(a.dt, fm(p1[u], d4)));
+            const float sr = fa(sr0[u], fm(a.dt, rold));
+            sx = xs(sx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);   // spg1xn, spg2xp
+            sz = xs(sz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);   // spg1zn, spg2zp
+            const int bx = gx - sd.stamp_x0, bz = gz - sd.stamp_z0;
+            if (bx >= 0 && bx < sd.stamp_w && bz >= 0 && bz < sd.stamp_h) {
+                const float g = __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz);
+                sx = fa(__fdiv_rn(fm(fm(wav, g), a.dt), a.dz2), sx);   // QS:1384
+            }
+            // calprxx (QS:1135-1170)
+            float rx = fa(rx0[u], fm(a.f_mem, fm(p2[u], d1)));
+            float rz = fa(rz0[u], fm(a.f_mem, fm(p2[u], d4)));
+            const float rr = fa(rr0[u], fm(a.f_mem, rold));
+            rx = xs(rx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
+            rz = xs(rz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
+            a.sx[c] = sx; a.sz[c] = sz; a.sr[c] = sr;
+            a.rx[c] = rx; a.rz[c] = rz; a.rr[c] = rr;
+            if (a.d1_out) {  // gradient recomputation keeps the derivatives for the imaging condition
+                a.d1_out[c] = d1;
+                a.d4_out[c] = d4;
+            }
         }
     }
     // receivers: strzz (= strxx) = (sx + sz) + sr (QM:452-459)
