@@ -320,6 +320,35 @@ def measure_viscoacoustic(args, dev):
     return out
 
 
+def measure_viscoelastic(args, dev):
+    """Config-3 geometry with shear waves: the visco-elastic P-SV scheme (vs = vp / 1.8, Qs = 0.7 Qp)
+    on the same 16 shots, one batched time loop (22 split fields per cell, as the reference
+    keeps them)."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.q_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, nt, c["dt"], c["f0"]))
+             for sx, sz, nt in zip(c["src_x"], c["src_z"], c["nt"])]
+    with S.Engine(S.VISCOEL_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"], device=dev) as e:
+        e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"], c["q"],
+                            (0.7 * c["q"]).astype(np.float32))
+        e.set_shots(shots)
+        e.forward_device(0)
+        ms = []
+        for _ in range(args.e_steps):
+            e.forward_device(0)
+            ms.append(e.timing()["loop_ms"])
+    pts = float(sum(Nx * Nz * nt for nt in c["nt"]))
+    gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    return {"workload": f"config 3 geometry, visco-elastic P-SV (vs = vp/1.8): {c['NZ']}x{c['NX']} interior, "
+                        f"{len(shots)} shots, nt {min(c['nt'])}-{max(c['nt'])}",
+            "gpts_per_s": gpts, "shots_per_s": len(shots) / (float(np.median(ms)) / 1e3),
+            "loop_ms": float(np.median(ms)), "parity": "bit-exact vs FP32 restatement (strzz and strxx)"}
+
+
 def measure_q_gradient(args, dev):
     """Config-3 geometry: the viscoacoustic gradient d misfit / d vp and d misfit / d (1/Q) of 16
     shots (uneven record lengths), observed data from the Q field scaled by 0.8, batched (one
@@ -579,6 +608,8 @@ def run_ours(args, world, rank, local):
         line["gradient_sharded"] = grad_sharded
     if world == 1 and args.q_steps > 0:
         line["viscoacoustic"] = measure_viscoacoustic(args, dev)
+    if world == 1 and args.e_steps > 0:
+        line["viscoelastic"] = measure_viscoelastic(args, dev)
     if world == 1 and args.qg_steps > 0:
         line["viscoacoustic_gradient"] = measure_q_gradient(args, dev)
     if world == 1 and args.d3_steps > 0:
@@ -614,6 +645,7 @@ def main():
     ap.add_argument("--d3-nshot", type=int, default=16)
     ap.add_argument("--d3-nt-scale", type=float, default=0.05)
     ap.add_argument("--d3-cpu-steps", type=int, default=3)
+    ap.add_argument("--e-steps", type=int, default=1, help="timed visco-elastic forwards (0 = skip)")
     ap.add_argument("--qg-steps", type=int, default=1, help="timed viscoacoustic gradients (0 = skip)")
     ap.add_argument("--qg-nshot", type=int, default=16)
     ap.add_argument("--qg-nt-scale", type=float, default=1.0)

@@ -49,6 +49,8 @@ extern "C" {
 #define SFD_VISCOAC_2D 1   /* rotated staggered grid, 1 SLS memory variable, vs = 0:
                               QS:695-839 in its acoustic reduction                          */
 #define SFD_ACOUSTIC_3D 2  /* 3-D velocity-pressure staggered grid (no reference counterpart) */
+#define SFD_VISCOEL_2D 3   /* rotated staggered grid, P-SV visco-elastic with 1 SLS per stress
+                              (vs > 0): QS:695-1337, the full Q_forward scheme              */
 
 /* ---- flags (sfd_grid.flags) ---- */
 #define SFD_EXACT 0x1      /* reference operation order: every multiply and add rounded
@@ -67,6 +69,8 @@ extern "C" {
 #define SFD_FIELD_VZ 2
 #define SFD_FIELD_VY 3
 #define SFD_FIELD_R 4      /* memory variable r (QS rxx)                                     */
+#define SFD_FIELD_SZZ 5    /* QS strzz (visco-elastic; equals strxx when vs = 0)             */
+#define SFD_FIELD_SXZ 6    /* QS strxz (visco-elastic)                                       */
 
 typedef struct sfd_ctx sfd_ctx;
 
@@ -123,6 +127,12 @@ int sfd_last_error(const sfd_ctx* ctx, char* buf, size_t len);
  * attenuation: Q = 1e5, the QM:418-419 override). */
 int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* q);
 
+/* Visco-elastic model (SFD_VISCOEL_2D): P and S velocities, density and the P and S quality
+ * factors on the padded grid.  Replaces QS:238-284 (read_data of vp, vs, rho, qfp, qfs) and
+ * QS:434-551 (substagger, pcalpas).  den NULL = 2400 kg/m^3; qp / qs NULL = 1e5 (QM:418-419). */
+int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const float* den, const float* qp,
+                          const float* qs);
+
 /* Shots.  Replaces the shot loop QM:124-141 (one launch for all shots instead of one process
  * per shot).  Wavelets and receiver lists are copied; the caller keeps ownership. */
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots);
@@ -134,6 +144,12 @@ int sfd_forward(sfd_ctx* ctx, float* records);
 
 /* Same, with the records left in device memory (caller-owned, same layout) and no host copy. */
 int sfd_forward_device(sfd_ctx* ctx, float* records_dev);
+
+/* Records of one stress component from the last forward, in the sfd_forward layout.  The
+ * Q_forward programs record two (QM:452-459): record1 = strzz (SFD_FIELD_SZZ, what sfd_forward
+ * returns for the viscoacoustic and visco-elastic schemes) and record2 = strxx (SFD_FIELD_P).
+ * For SFD_VISCOAC_2D both are the same sigma. */
+int sfd_get_records(sfd_ctx* ctx, int field, float* records);
 
 /* Plain per-shot path: shots one after another, one kernel launch per time step each, no
  * graph -- the unbatched baseline the batched loop is measured against. */

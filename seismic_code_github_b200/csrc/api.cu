@@ -108,6 +108,13 @@ struct sfd_ctx {
     float* d_spg = nullptr;
     int spg_stride = 0;
     float* d_stamps = nullptr;
+    // visco-elastic scheme: the six stress coefficients (QS:473-551) and the strxx records
+    float* e_q[6] = {};             // q1 q2 q3 m1 m2 m3 in the prepared-model layout
+    std::vector<float> h_vs, h_qs;  // S velocity and S quality factor as given (empty: 0 / 1e5)
+    float* d_rec2_tn = nullptr;     // strxx records [nt][nrec] per shot
+    float* d_rec2_nt = nullptr;     // ... trace-major
+    bool rec2_ready = false;
+    bool elastic_call = false;      // sfd_set_model is running on behalf of sfd_set_model_elastic
 
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
@@ -233,6 +240,8 @@ void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
     dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri); dfree(c->d_rec_y);
     dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps); dfree(c->d_src_pre);
+    dfree(c->d_rec2_tn); dfree(c->d_rec2_nt);
+    c->rec2_ready = false;
     for (auto& sn : c->snaps) {
         dfree(sn.d_buf);
         dfree(sn.d_off);
@@ -262,6 +271,7 @@ sfd_ctx::~sfd_ctx() {
     free_shot_buffers(this);
     dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag); dfree(d_err);
     dfree(q_busg); dfree(q_p1); dfree(q_p2); dfree(d_spg);
+    for (auto& p : e_q) dfree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evs) cudaEventDestroy(evs);
@@ -401,6 +411,30 @@ QArgs make_qargs(const sfd_ctx* c, int step) {
     return a;
 }
 
+// Arguments of the visco-elastic step (22 in-place split fields per shot).
+EArgs make_eargs(const sfd_ctx* c, int step) {
+    EArgs a{};
+    const QArgs q = make_qargs(c, step);
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    for (int i = 0; i < E_NFIELDS; i++) a.f[i] = c->d_state + i * fs;
+    a.L = q.L;
+    a.nz = q.nz; a.npx = q.npx; a.npz = q.npz;
+    a.busg = q.busg;
+    a.q1 = c->e_q[0] + kModelGhostZ; a.q2 = c->e_q[1] + kModelGhostZ; a.q3 = c->e_q[2] + kModelGhostZ;
+    a.m1 = c->e_q[3] + kModelGhostZ; a.m2 = c->e_q[4] + kModelGhostZ; a.m3 = c->e_q[5] + kModelGhostZ;
+    a.mpitch = q.mpitch; a.nx_model = q.nx_model;
+    a.dt = q.dt; a.f_mem = q.f_mem; a.hx = q.hx; a.hz = q.hz; a.dz2 = q.dz2;
+    std::memcpy(a.a, q.a, sizeof(a.a));
+    a.spg = q.spg; a.spg_stride = q.spg_stride;
+    a.shots = q.shots; a.slot_to_shot = q.slot_to_shot;
+    a.wavelets = q.wavelets; a.stamps = q.stamps;
+    a.rec_x = q.rec_x; a.rec_z = q.rec_z; a.tile_rec_ptr = q.tile_rec_ptr; a.tile_rec_idx = q.tile_rec_idx;
+    a.records = c->d_rec_tn;
+    a.records2 = c->d_rec2_tn;
+    a.step = step;
+    return a;
+}
+
 // Size the snapshot buffers for the current shot set; returns true if a buffer moved (the
 // captured time loop holds their addresses).
 bool snap_prepare(sfd_ctx* ctx, int* rc) {
@@ -454,6 +488,18 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
             const int f0 = sn.field == SFD_FIELD_VX ? 0 : sn.field == SFD_FIELD_VZ ? 1 : sn.field == SFD_FIELD_P ? 2 : 5;
             s.nsum = (sn.field == SFD_FIELD_P || sn.field == SFD_FIELD_R) ? 3 : 1;
             for (int i = 0; i < s.nsum; i++) s.f[i] = F + (f0 + i) * fs;
+        } else if (ctx->g.scheme == SFD_VISCOEL_2D) {
+            int f0;  // first split part; velocities have two, stresses and memory variables three
+            switch (sn.field) {
+            case SFD_FIELD_VX: f0 = E_VXX; break;
+            case SFD_FIELD_VZ: f0 = E_VZX; break;
+            case SFD_FIELD_P: f0 = E_SXXX; break;
+            case SFD_FIELD_SZZ: f0 = E_SZZX; break;
+            case SFD_FIELD_SXZ: f0 = E_SXZX; break;
+            default: f0 = E_RXXX; break;
+            }
+            s.nsum = f0 < E_SXXX ? 2 : 3;
+            for (int i = 0; i < s.nsum; i++) s.f[i] = F + (f0 + i) * fs;
         } else {
             const int o = (k + 1) & 1;  // buffer written by step k
             const int f0 = sn.field == SFD_FIELD_P ? 0 : sn.field == SFD_FIELD_VX ? 2 : 4;
@@ -497,6 +543,13 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         *launches += 2;
         return SFD_OK;
     }
+    if (ctx->g.scheme == SFD_VISCOEL_2D) {
+        EArgs e = make_eargs(ctx, k);
+        e.slot_to_shot = slots;
+        CK(viscoel2d_launch_step(e, act, ctx->stream));
+        *launches += 2;
+        return SFD_OK;
+    }
     Acou2DArgs a = make_args(ctx, k);
     a.slot_to_shot = slots;
     CK(acoustic2d_launch_step(ctx->plan, a, act, (ctx->g.flags & SFD_EXACT) != 0, ctx->varden, ctx->stream));
@@ -509,6 +562,8 @@ int prologue(sfd_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->d_state, 0, ctx->state_floats * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_rec_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
+    if (ctx->d_rec2_tn)
+        CK(cudaMemsetAsync(ctx->d_rec2_tn, 0, std::max<long long>(ctx->rec_total, 1) * sizeof(float), ctx->stream));
     // the viscoacoustic source is added inside every step, the 3-D one by its own launch
     if (ctx->g.scheme != SFD_ACOUSTIC_2D) return SFD_OK;
     Acou2DArgs a = make_args(ctx, -1);  // step -1 writes into buffer 0
@@ -529,6 +584,11 @@ int enqueue_loop(sfd_ctx* ctx, long long* launches) {
 int epilogue(sfd_ctx* ctx, float* out_dev) {
     CK(launch_records_transpose(ctx->d_rec_tn, out_dev, ctx->d_shots, ctx->nshot, ctx->nrec_max, ctx->nt_max,
                                 ctx->stream));
+    if (ctx->d_rec2_tn) {
+        CK(launch_records_transpose(ctx->d_rec2_tn, ctx->d_rec2_nt, ctx->d_shots, ctx->nshot, ctx->nrec_max,
+                                    ctx->nt_max, ctx->stream));
+        ctx->rec2_ready = true;
+    }
     if (ctx->g.flags & SFD_NAN_CHECK) {
         CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
         CK(launch_nan_scan(out_dev, ctx->rec_total, ctx->d_flag, ctx->stream));
@@ -593,6 +653,7 @@ int tune_schedule(sfd_ctx* ctx) {
 int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
     if (ctx->g.scheme == SFD_VISCOAC_2D) return 40;
+    if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     return (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
 }
 
@@ -1033,7 +1094,8 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
 // start and width) gets its own block of the prepared arrays; shot x0 becomes that block's start.
 // Without shots the whole grid is one window.
 int q_prepare(sfd_ctx* ctx) {
-    if (ctx->g.scheme != SFD_VISCOAC_2D || !ctx->have_model) return SFD_OK;
+    const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
+    if ((ctx->g.scheme != SFD_VISCOAC_2D && !elastic) || !ctx->have_model) return SFD_OK;
     const int nz = ctx->g.nz;
     std::vector<std::pair<int, int>> wins;  // (x0, nx)
     std::vector<int> blk(ctx->have_shots ? ctx->nshot : 0);
@@ -1054,14 +1116,24 @@ int q_prepare(sfd_ctx* ctx) {
         width += wins[b].second;
     }
     std::vector<float> busg((size_t)width * nz), p1((size_t)width * nz), p2((size_t)width * nz);
+    std::vector<std::vector<float>> eq(elastic ? 6 : 0, std::vector<float>((size_t)width * nz));
     for (size_t b = 0; b < wins.size(); b++) {
         const size_t off = (size_t)wins[b].first * nz, len = (size_t)wins[b].second * nz;
         std::vector<float> rho(len, ctx->den_c);
         if (!ctx->h_den.empty()) rho.assign(ctx->h_den.begin() + off, ctx->h_den.begin() + off + len);
         const float* qw = ctx->h_q.empty() ? nullptr : ctx->h_q.data() + off;
-        viscoac2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, rho.data(), qw, ctx->g.f0,
-                          busg.data() + (size_t)start[b] * nz, p1.data() + (size_t)start[b] * nz,
-                          p2.data() + (size_t)start[b] * nz, &ctx->q_rtau);
+        const size_t o = (size_t)start[b] * nz;
+        if (elastic) {
+            std::vector<float> vs(len, 0.0f);
+            if (!ctx->h_vs.empty()) vs.assign(ctx->h_vs.begin() + off, ctx->h_vs.begin() + off + len);
+            const float* qsw = ctx->h_qs.empty() ? nullptr : ctx->h_qs.data() + off;
+            viscoel2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(), qw, qsw, ctx->g.f0,
+                              busg.data() + o, eq[0].data() + o, eq[1].data() + o, eq[2].data() + o,
+                              eq[3].data() + o, eq[4].data() + o, eq[5].data() + o, &ctx->q_rtau);
+        } else {
+            viscoac2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, rho.data(), qw, ctx->g.f0, busg.data() + o,
+                              p1.data() + o, p2.data() + o, &ctx->q_rtau);
+        }
     }
     // upload with kModelGhostZ replicated rows (the layout of the other model arrays)
     const size_t mfloats = (size_t)width * ctx->mpitch;
@@ -1079,8 +1151,13 @@ int q_prepare(sfd_ctx* ctx) {
         return SFD_OK;
     };
     int rc;
-    if ((rc = upload(&ctx->q_busg, busg)) || (rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2)))
+    if ((rc = upload(&ctx->q_busg, busg))) return rc;
+    if (elastic) {
+        for (int i = 0; i < 6; i++)
+            if ((rc = upload(&ctx->e_q[i], eq[i]))) return rc;
+    } else if ((rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2))) {
         return rc;
+    }
     if (width != ctx->q_width) ctx->graph_valid = ctx->grad_valid = false;
     ctx->q_width = width;
     if (ctx->have_shots) {
@@ -1566,7 +1643,8 @@ int sfd_last_error(const sfd_ctx* ctx, char* buf, size_t len) {
 int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     if (!g || !out) return SFD_ERR_ARG;
     *out = nullptr;
-    if (g->scheme != SFD_ACOUSTIC_2D && g->scheme != SFD_VISCOAC_2D && g->scheme != SFD_ACOUSTIC_3D)
+    if (g->scheme != SFD_ACOUSTIC_2D && g->scheme != SFD_VISCOAC_2D && g->scheme != SFD_ACOUSTIC_3D &&
+        g->scheme != SFD_VISCOEL_2D)
         return SFD_ERR_ARG;
     const bool is3d = g->scheme == SFD_ACOUSTIC_3D;
     if (g->nx <= 0 || g->nz <= 0 || (is3d ? g->ny <= 0 : g->ny > 1)) return SFD_ERR_ARG;
@@ -1595,10 +1673,10 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
     if (g->scheme == SFD_ACOUSTIC_2D && !acoustic2d_plan(R, &c->plan))
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "no kernel for radius %d", R);
-    if (g->scheme == SFD_VISCOAC_2D) {
+    if (g->scheme == SFD_VISCOAC_2D || g->scheme == SFD_VISCOEL_2D) {
         // the rotated staggered grid of QS is 10th order only (a100..a104, QS:9-28)
-        if (g->order != 10) return set_err(ctx, SFD_ERR_UNSUPPORTED, "the viscoacoustic scheme is 10th order");
-        if (!(g->f0 > 0)) return set_err(ctx, SFD_ERR_ARG, "the viscoacoustic scheme needs f0 > 0 (QS:509)");
+        if (g->order != 10) return set_err(ctx, SFD_ERR_UNSUPPORTED, "the Q_forward schemes are 10th order");
+        if (!(g->f0 > 0)) return set_err(ctx, SFD_ERR_ARG, "the Q_forward schemes need f0 > 0 (QS:509)");
         c->plan.radius = 5;
         c->plan.tx = kTileX;
         c->plan.tz = kTileZ;
@@ -1678,7 +1756,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     } else {
         dfree(ctx->d_den);
     }
-    if (ctx->g.scheme == SFD_VISCOAC_2D) {
+    if (ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D) {
         // QS:434-551 on the padded grid: averaged density -> buoyancy, Lame and Blanch tau
         if (q)
             for (size_t i = 0; i < n; i++)
@@ -1687,6 +1765,10 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
                                    (double)q[i]);
         if (q) ctx->h_q.assign(q, q + n);
         else ctx->h_q.clear();
+        if (ctx->g.scheme == SFD_VISCOEL_2D && !ctx->elastic_call) {  // no S waves: vs = 0, Qs = Qp
+            ctx->h_vs.clear();
+            ctx->h_qs = ctx->h_q;
+        }
         ctx->have_model = true;
         if ((urc = q_prepare(ctx))) return urc;
     }
@@ -1696,7 +1778,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     }
     ctx->have_model = true;
     // source scale factors depend on the model (the viscoacoustic source is a stamp)
-    if (ctx->have_shots && ctx->g.scheme != SFD_VISCOAC_2D) {
+    if (ctx->have_shots && ctx->g.scheme != SFD_VISCOAC_2D && ctx->g.scheme != SFD_VISCOEL_2D) {
         for (auto& s : ctx->h_shots) {
             const size_t mi = ((size_t)(s.x0 + s.sx) * ctx->g.ny + s.sy) * ctx->g.nz + s.sz;
             const float d = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
@@ -1709,10 +1791,34 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     return SFD_OK;
 }
 
+int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const float* den, const float* qp,
+                          const float* qs) {
+    if (!ctx || !vp || !vs) return SFD_ERR_ARG;
+    if (ctx->g.scheme != SFD_VISCOEL_2D)
+        return set_err(ctx, SFD_ERR_ARG, "sfd_set_model_elastic applies to SFD_VISCOEL_2D");
+    const size_t n = (size_t)ctx->g.nx * ctx->g.nz;
+    for (size_t i = 0; i < n; i++)
+        if (!(vs[i] >= 0.0f) || !std::isfinite(vs[i]))
+            return set_err(ctx, SFD_ERR_ARG, "vs[%zu] = %g is not a finite non-negative velocity", i, (double)vs[i]);
+    if (qs)
+        for (size_t i = 0; i < n; i++)
+            if (!(qs[i] > 0.0f) || !std::isfinite(qs[i]))
+                return set_err(ctx, SFD_ERR_ARG, "qs[%zu] = %g is not a positive finite quality factor", i,
+                               (double)qs[i]);
+    ctx->h_vs.assign(vs, vs + n);
+    if (qs) ctx->h_qs.assign(qs, qs + n);
+    else ctx->h_qs.clear();
+    ctx->elastic_call = true;
+    const int rc = sfd_set_model(ctx, vp, den, qp);
+    ctx->elastic_call = false;
+    return rc;
+}
+
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     if (!ctx || nshot <= 0 || !shots) return SFD_ERR_ARG;
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return set_shots_3d(ctx, nshot, shots);
-    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D || elastic;  // the Q_forward schemes
     if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d is not implemented", ctx->g.scheme);
     CK(cudaSetDevice(ctx->device));
@@ -1827,7 +1933,11 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
     CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
-    ctx->state_floats = (visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
+    if (elastic) {
+        CK(cudaMalloc(&ctx->d_rec2_tn, rec_bytes));
+        CK(cudaMalloc(&ctx->d_rec2_nt, rec_bytes));
+    }
+    ctx->state_floats = (elastic ? E_NFIELDS : visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
     CK(cudaMalloc(&ctx->d_src_pre, sizeof(float) * nshot));
     if (visco) {
@@ -1985,6 +2095,33 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         for (size_t i = 0; i < n; i++) out[i] = (a[i] + b[i]) + c[i];
         return SFD_OK;
     }
+    if (ctx->g.scheme == SFD_VISCOEL_2D) {
+        // sums of the split parts in the reference's order (QS:1273-1337)
+        const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
+        const int nz = ctx->g.nz;
+        int f0;
+        switch (field) {
+        case SFD_FIELD_VX: f0 = E_VXX; break;
+        case SFD_FIELD_VZ: f0 = E_VZX; break;
+        case SFD_FIELD_P: f0 = E_SXXX; break;
+        case SFD_FIELD_SZZ: f0 = E_SZZX; break;
+        case SFD_FIELD_SXZ: f0 = E_SXZX; break;
+        case SFD_FIELD_R: f0 = E_RXXX; break;
+        default: return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+        }
+        const int np = f0 < E_SXXX ? 2 : 3;
+        const size_t n = (size_t)sd.nx * nz;
+        std::vector<float> part(n);
+        for (int i = 0; i < np; i++) {
+            const float* base = ctx->d_state + (f0 + i) * fs + (long long)shot * ctx->L.shot_stride +
+                                (long long)ctx->L.gx * ctx->L.pitch + ctx->L.gz;
+            CK(cudaMemcpy2D(i == 0 ? out : part.data(), sizeof(float) * nz, base, sizeof(float) * ctx->L.pitch,
+                            sizeof(float) * nz, sd.nx, cudaMemcpyDeviceToHost));
+            if (i > 0)
+                for (size_t j = 0; j < n; j++) out[j] = out[j] + part[j];
+        }
+        return SFD_OK;
+    }
     if (field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
     const int buf = sd.nt & 1;  // state after nt steps lives in buffer nt % 2
@@ -2041,9 +2178,10 @@ int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int
     if (!ctx || id < 0 || id >= 4 || count < 0 || first < 0 || (count > 0 && every < 1)) return SFD_ERR_ARG;
     if (ctx->g.scheme == SFD_ACOUSTIC_3D && count > 0)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "snapshots are taken for the 2-D schemes");
-    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D;
+    const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
     if (count > 0 && field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ &&
-        !(visco && field == SFD_FIELD_R))
+        !(visco && field == SFD_FIELD_R) && !(elastic && (field == SFD_FIELD_SZZ || field == SFD_FIELD_SXZ)))
         return set_err(ctx, SFD_ERR_ARG, "field %d cannot be recorded for this scheme", field);
     auto& sn = ctx->snaps[id];
     sn.field = field;
@@ -2052,6 +2190,25 @@ int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int
     sn.count = count;
     sn.ready = false;
     ctx->graph_valid = false;
+    return SFD_OK;
+}
+
+int sfd_get_records(sfd_ctx* ctx, int field, float* records) {
+    if (!ctx || !records) return SFD_ERR_ARG;
+    if (!ctx->have_shots) return set_err(ctx, SFD_ERR_STATE, "no shots");
+    const bool q = ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D;
+    if (!q || (field != SFD_FIELD_SZZ && field != SFD_FIELD_P))
+        return set_err(ctx, SFD_ERR_UNSUPPORTED, "records of field %d are not recorded for this scheme", field);
+    CK(cudaSetDevice(ctx->device));
+    // the time-major records of the last forward, transposed to the output layout: strzz, or
+    // strxx, which only the visco-elastic scheme keeps apart (for vs = 0 both are sigma)
+    const bool sxx = field == SFD_FIELD_P && ctx->g.scheme == SFD_VISCOEL_2D;
+    if (sxx && !ctx->rec2_ready) return set_err(ctx, SFD_ERR_STATE, "no forward has run");
+    float* tn = sxx ? ctx->d_rec2_tn : ctx->d_rec_tn;
+    float* nt = sxx ? ctx->d_rec2_nt : ctx->d_rec_nt;
+    CK(launch_records_transpose(tn, nt, ctx->d_shots, ctx->nshot, ctx->nrec_max, ctx->nt_max, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->rec_total > 0) CK(cudaMemcpy(records, nt, sizeof(float) * ctx->rec_total, cudaMemcpyDeviceToHost));
     return SFD_OK;
 }
 

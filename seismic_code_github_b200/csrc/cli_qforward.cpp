@@ -1,5 +1,6 @@
 // q_forward: drop-in for the forward/Q_forward program (Q_multishot_fd_main_fsbc_zy_rotated.f90,
-// QM) on one GPU, for the viscoacoustic case (vs = 0 everywhere).
+// QM) on one GPU: the viscoacoustic scheme when the vs file is zero everywhere, the full
+// visco-elastic P-SV scheme otherwise.
 //
 //   q_forward PARFILE [--use-q] [--snapshots DIR] [--keep-parts] [--device N]
 //
@@ -89,9 +90,8 @@ int main(int argc, char** argv) {
     for (int f = 0; f < 5; f++)
         if ((rc = sfd_read_floats(strip(files[f]).c_str(), (long long)nm, arrays[f]->data())))
             return fail(files[f], rc, nullptr);
-    for (size_t i = 0; i < nm; i++)
-        if (vs[i] != 0.0f)
-            return fail("vs file: visco-elastic modelling (vs > 0) is not implemented", SFD_ERR_UNSUPPORTED, nullptr);
+    bool elastic = false;  // any shear velocity: the full P-SV scheme (QS:751-835)
+    for (size_t i = 0; i < nm; i++) elastic = elastic || vs[i] != 0.0f;
     // QS:1364-1366 (single precision): wavelet length and the decay steps before recording
     const int nwt = 2 * nint(1.2f / (p.f0 * p.dt));
     const int decay = nint(nwt / 2.0f);
@@ -130,7 +130,7 @@ int main(int argc, char** argv) {
         width += blocks[b].second + 2 * np;
     }
     const size_t nme = (size_t)width * nzea;
-    std::vector<float> vpe(nme), rhoe(nme), qpe(nme);
+    std::vector<float> vpe(nme), rhoe(nme), qpe(nme), vse(elastic ? nme : 0), qse(elastic ? nme : 0);
     for (size_t b = 0; b < blocks.size(); b++) {
         const int ixmine = blocks[b].first, nxe = blocks[b].second, nxea = nxe + 2 * np;
         for (int c = 0; c < nxea; c++) {
@@ -145,12 +145,16 @@ int main(int argc, char** argv) {
                 vpe[dst] = vp[src];
                 rhoe[dst] = rho[src];
                 qpe[dst] = qp[src];
+                if (elastic) {
+                    vse[dst] = vs[src];
+                    qse[dst] = qs[src];
+                }
             }
         }
     }
 
     sfd_grid g{};
-    g.scheme = SFD_VISCOAC_2D;
+    g.scheme = elastic ? SFD_VISCOEL_2D : SFD_VISCOAC_2D;
     g.nx = width;
     g.ny = 1;
     g.nz = nzea;
@@ -162,8 +166,13 @@ int main(int argc, char** argv) {
     g.f0 = p.f0;
     sfd_ctx* ctx = nullptr;
     if ((rc = sfd_create(&g, device, &ctx))) return fail("sfd_create", rc, ctx);
-    if ((rc = sfd_set_model(ctx, vpe.data(), rhoe.data(), use_q ? qpe.data() : nullptr)))
+    if (elastic) {
+        if ((rc = sfd_set_model_elastic(ctx, vpe.data(), vse.data(), rhoe.data(), use_q ? qpe.data() : nullptr,
+                                        use_q ? qse.data() : nullptr)))
+            return fail("sfd_set_model_elastic", rc, ctx);
+    } else if ((rc = sfd_set_model(ctx, vpe.data(), rhoe.data(), use_q ? qpe.data() : nullptr))) {
         return fail("sfd_set_model", rc, ctx);
+    }
     std::vector<sfd_shot> desc(p.nshot);
     std::vector<std::vector<int>> rx(p.nshot), rz(p.nshot);
     for (int i = 0; i < p.nshot; i++) {
@@ -185,12 +194,20 @@ int main(int argc, char** argv) {
     }
     if ((rc = sfd_set_shots(ctx, p.nshot, desc.data()))) return fail("sfd_set_shots", rc, ctx);
     const int nsnap = nt_run / 50;
-    if (!snap_dir.empty() && nsnap > 0 && (rc = sfd_set_snapshots(ctx, 0, SFD_FIELD_P, 49, 50, nsnap)))
+    // QM:462-481: strxx (snapx) and strzz (snapz) every 50 steps
+    if (!snap_dir.empty() && nsnap > 0 &&
+        ((rc = sfd_set_snapshots(ctx, 0, SFD_FIELD_P, 49, 50, nsnap)) ||
+         (elastic && (rc = sfd_set_snapshots(ctx, 1, SFD_FIELD_SZZ, 49, 50, nsnap)))))
         return fail("sfd_set_snapshots", rc, ctx);
     long long total = 0;
     for (const auto& s : shots) total += (long long)s.nxe * nt_run;
-    std::vector<float> rec(total);
-    if ((rc = sfd_forward(ctx, rec.data()))) return fail("sfd_forward", rc, ctx);
+    std::vector<float> rec(total), rec2;
+    if ((rc = sfd_forward(ctx, rec.data()))) return fail("sfd_forward", rc, ctx);  // record1: strzz
+    if (elastic) {  // record2: strxx (for vs = 0 the same sigma)
+        rec2.resize(total);
+        if ((rc = sfd_get_records(ctx, SFD_FIELD_P, rec2.data()))) return fail("sfd_get_records", rc, ctx);
+    }
+    const std::vector<float>& recx = elastic ? rec2 : rec;
 
     // SU output per shot (record1 -> shot_fn1, record2 -> shot_fn3), then the merge
     const std::string f1 = strip(p.shot1), f2 = strip(p.shot2), f3 = strip(p.shot3), f4 = strip(p.shot4);
@@ -198,14 +215,17 @@ int main(int argc, char** argv) {
     long long off = 0;
     for (int i = 0; i < p.nshot; i++) {
         const ShotInfo& s = shots[i];
-        std::vector<float> tr((size_t)s.nxe * p.nt);
-        for (int r = 0; r < s.nxe; r++)
+        std::vector<float> tr((size_t)s.nxe * p.nt), tx((size_t)s.nxe * p.nt);
+        for (int r = 0; r < s.nxe; r++) {
             std::memcpy(tr.data() + (size_t)r * p.nt, rec.data() + off + (long long)r * nt_run + decay,
                         sizeof(float) * p.nt);
+            std::memcpy(tx.data() + (size_t)r * p.nt, recx.data() + off + (long long)r * nt_run + decay,
+                        sizeof(float) * p.nt);
+        }
         off += (long long)s.nxe * nt_run;
         const std::string n1 = f1 + std::to_string(i + 1) + ".su", n3 = f3 + std::to_string(i + 1) + ".su";
         if ((rc = sfd_su_write(n1.c_str(), tr.data(), s.nxe, p.nt, i + 1, s.isx, s.ixmine, p.dx, p.dt)) ||
-            (rc = sfd_su_write(n3.c_str(), tr.data(), s.nxe, p.nt, i + 1, s.isx, s.ixmine, p.dx, p.dt)))
+            (rc = sfd_su_write(n3.c_str(), tx.data(), s.nxe, p.nt, i + 1, s.isx, s.ixmine, p.dx, p.dt)))
             return fail("SU write", rc, ctx);
         parts1.push_back(n1);
         parts3.push_back(n3);
@@ -219,13 +239,18 @@ int main(int argc, char** argv) {
     if (!snap_dir.empty() && nsnap > 0) {
         const int last = p.nshot - 1;
         const long long nf = (long long)shots[last].nxe * nz;
-        std::vector<float> frames((size_t)nsnap * nf);
-        int got = 0;
+        std::vector<float> frames((size_t)nsnap * nf), framez;
+        int got = 0, gotz = 0;
         if ((rc = sfd_get_snapshots(ctx, 0, last, frames.data(), &got))) return fail("snapshots", rc, ctx);
+        if (elastic) {
+            framez.resize(frames.size());
+            if ((rc = sfd_get_snapshots(ctx, 1, last, framez.data(), &gotz))) return fail("snapshots", rc, ctx);
+        }
+        const std::vector<float>& fz = elastic ? framez : frames;  // strzz (= strxx for vs = 0)
         for (int j = 0; j < got; j++) {
             const std::string it = std::to_string(50 * (j + 1));
             if ((rc = sfd_write_floats((snap_dir + "/iso_vx_elastic_" + it).c_str(), frames.data() + j * nf, nf, 0)) ||
-                (rc = sfd_write_floats((snap_dir + "/iso_vz_elastic_" + it).c_str(), frames.data() + j * nf, nf, 0)))
+                (rc = sfd_write_floats((snap_dir + "/iso_vz_elastic_" + it).c_str(), fz.data() + j * nf, nf, 0)))
                 return fail("snapshot files", rc, ctx);
         }
     }

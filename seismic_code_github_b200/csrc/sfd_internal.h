@@ -75,6 +75,43 @@ struct QArgs {
 };
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
 
+// Visco-elastic split fields (viscoel2d.cu), in the order of their slabs in the state buffer.
+enum EField {
+    E_VXX, E_VXZ, E_VZX, E_VZZ,
+    E_SXXX, E_SXXZ, E_SXXR, E_SZZX, E_SZZZ, E_SZZR, E_SXZX, E_SXZZ, E_SXZR,
+    E_RXXX, E_RXXZ, E_RXXR, E_RZZX, E_RZZZ, E_RZZR, E_RXZX, E_RXZZ, E_RXZR,
+    E_NFIELDS
+};
+
+// Arguments of the visco-elastic kernels (viscoel2d.cu): 22 in-place split fields.
+struct EArgs {
+    float* f[E_NFIELDS];
+    Layout2D L;
+    int nz, npx, npz;
+    const float* busg;                    // 1/averaged density (QS:434-469)
+    const float* q1; const float* q2; const float* q3;  // lambda tau_p, lambda tau_p - 2 mu tau_s, mu tau_s
+    const float* m1; const float* m2; const float* m3;  // the same with tau - 1 (memory variables)
+    int mpitch, nx_model;
+    float dt, f_mem, hx, hz, dz2;
+    float a[5];
+    const float* spg;
+    int spg_stride;
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* wavelets;
+    const float* stamps;
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr; const int* tile_rec_idx;
+    float* records;                       // strzz (record1), [nt][nrec] per shot
+    float* records2;                      // strxx (record2)
+    int step;
+};
+cudaError_t viscoel2d_launch_step(const EArgs& a, int active, cudaStream_t st);
+// QS:434-551 with vs: busg and the six stress coefficients on the padded grid, and rtaustss
+void viscoel2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, const float* qp,
+                       const float* qs, float f0, float* busg, float* q1, float* q2, float* q3, float* m1, float* m2,
+                       float* m3, float* rtau_out);
+
 // Arguments of the viscoacoustic adjoint kernels (q_adjoint2d.cu): adjoint fields in place.
 struct QAdjArgs {
     float* avx; float* avz;               // adjoints of vx, vz

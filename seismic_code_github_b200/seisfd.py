@@ -12,10 +12,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libseisfd.so")
 
 OK, ERR_ARG, ERR_IO, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE = range(9)
-ACOUSTIC_2D, VISCOAC_2D, ACOUSTIC_3D = 0, 1, 2
+ACOUSTIC_2D, VISCOAC_2D, ACOUSTIC_3D, VISCOEL_2D = 0, 1, 2, 3
 EXACT, NAN_CHECK = 0x1, 0x2
 WAVELET_AFD, WAVELET_RIC, WAVELET_Q = 0, 1, 2
-FIELD_P, FIELD_VX, FIELD_VZ, FIELD_VY, FIELD_R = 0, 1, 2, 3, 4
+FIELD_P, FIELD_VX, FIELD_VZ, FIELD_VY, FIELD_R, FIELD_SZZ, FIELD_SXZ = 0, 1, 2, 3, 4, 5, 6
 
 _F32P = ctypes.POINTER(ctypes.c_float)
 _I32P = ctypes.POINTER(ctypes.c_int)
@@ -80,6 +80,8 @@ SIGNATURES = {
     "sfd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "sfd_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "sfd_set_model": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P]),
+    "sfd_set_model_elastic": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P, _F32P]),
+    "sfd_get_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_shots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Shot)]),
     "sfd_forward": (ctypes.c_int, [ctypes.c_void_p, _F32P]),
     "sfd_forward_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -246,6 +248,20 @@ class Engine:
         q = None if q is None else np.ascontiguousarray(q, np.float32)
         self._keep_model = (vp, den, q)
         self._check(self._lib.sfd_set_model(self._h, _fp(vp), _fp(den), _fp(q)), "sfd_set_model")
+
+    def set_model_elastic(self, vp: np.ndarray, vs: np.ndarray, den: Optional[np.ndarray] = None,
+                          qp: Optional[np.ndarray] = None, qs: Optional[np.ndarray] = None):
+        """P and S velocities, density and quality factors of the visco-elastic scheme."""
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (vp, vs, den, qp, qs)]
+        self._keep_model = tuple(arrs)
+        self._check(self._lib.sfd_set_model_elastic(self._h, *[_fp(a) for a in arrs]), "sfd_set_model_elastic")
+
+    def records(self, field: int) -> np.ndarray:
+        """Records of one stress component from the last forward: FIELD_SZZ (record1, strzz) or
+        FIELD_P (record2, strxx), in the layout of forward()."""
+        out = np.empty(self.record_size(), np.float32)
+        self._check(self._lib.sfd_get_records(self._h, field, _fp(out)), "sfd_get_records")
+        return out
 
     def set_shots(self, shots: Sequence[ShotSpec]):
         arr = (Shot * len(shots))()

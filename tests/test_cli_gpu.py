@@ -61,7 +61,7 @@ def test_afd_fd_fast_path_within_tolerance(tmp_path):
     assert not (tmp_path / "Pall.dat").exists()
 
 
-def qcard_case(tmp_path):
+def qcard_case(tmp_path, elastic=False):
     nx, nz = 120, 80
     rng = np.random.default_rng(11)
     z = np.arange(nz)
@@ -69,16 +69,18 @@ def qcard_case(tmp_path):
     vp += rng.uniform(-50, 50, vp.shape).astype(np.float32)
     rho = (2000.0 + 300.0 * rng.random((nx, nz))).astype(np.float32)
     qp = (30.0 + 150.0 * rng.random((nx, nz))).astype(np.float32)
-    for name, a in (("vp", vp), ("vs", vp * 0), ("rho", rho), ("qp", qp), ("qs", qp)):
+    vs = (vp / 1.8).astype(np.float32) if elastic else vp * 0
+    qs = (0.7 * qp).astype(np.float32) if elastic else qp
+    for name, a in (("vp", vp), ("vs", vs), ("rho", rho), ("qp", qp), ("qs", qs)):
         a.tofile(tmp_path / f"{name}.bin")
     card = CARD.format(d=str(tmp_path)).replace("0.001\n", "0.0005\n").replace("500\n!*dt", "400\n!*dt")
     (tmp_path / "card.par").write_text(card)
-    return S.read_qpar(str(tmp_path / "card.par")), vp, rho, qp
+    return S.read_qpar(str(tmp_path / "card.par")), vp, vs, rho, qp, qs
 
 
-@pytest.mark.parametrize("use_q", [False, True])
-def test_q_forward_program_against_restatement(tmp_path, use_q):
-    p, vp, rho, qp = qcard_case(tmp_path)
+@pytest.mark.parametrize("use_q,elastic", [(False, False), (True, False), (True, True)])
+def test_q_forward_program_against_restatement(tmp_path, use_q, elastic):
+    p, vp, vs, rho, qp, qs = qcard_case(tmp_path, elastic)
     assert p.nt == 400 and np.float32(p.dt) == np.float32(0.0005)
     cmd = [os.path.join(BIN, "q_forward"), str(tmp_path / "card.par")] + (["--use-q"] if use_q else [])
     run(cmd, cwd=tmp_path)
@@ -93,7 +95,7 @@ def test_q_forward_program_against_restatement(tmp_path, use_q):
             isx = isx0 + nint((i - 1) * p.dsx / p.dx)
             ixmine, ixmaxe = isx + nint(p.offset_min / p.dx), isx + nint(p.offset_max / p.dx)
             nxe = ixmaxe - ixmine + 1
-            r1, r2, _ = ol.q_forward(vp, vp * 0, rho, qp, qp, p.dx, p.dz, p.dt, p.f0, p.nt, np_, np_,
+            r1, r2, _ = ol.q_forward(vp, vs, rho, qp, qs, p.dx, p.dz, p.dt, p.f0, p.nt, np_, np_,
                                      isx - ixmine + np_ + 1, nsz0 + np_ + 1, nrz0=nrz0, ixmine=ixmine,
                                      ixmaxe=ixmaxe, q_override=not use_q)
             ref = r1 if stem == "pz" else r2
