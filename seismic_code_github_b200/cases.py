@@ -6,6 +6,7 @@
     python -m seismic_code_github_b200.cases forward2d --nshot 16 --nt 40
     python -m seismic_code_github_b200.cases qgradient --nshot 4 --nt 100
     python -m seismic_code_github_b200.cases gradient3d --n 384 --nshot 2 --nt 6
+    python -m seismic_code_github_b200.cases viscoel --nshot 4 --nt 60
 
 Each run builds a seeded synthetic model, runs one warm-up call and one timed call of the
 batched path and prints the engine's timing record.  Sizes are chosen on the command line so
@@ -46,6 +47,22 @@ def viscoac(args):
              for sx, sz in zip(c["src_x"], c["src_z"])]
     with S.Engine(S.VISCOAC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
         e.set_model(c["vp"], c["rho"], c["q"])
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def viscoel(args):
+    c = W.config3(nshot=args.nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, args.nt, c["dt"], c["f0"]))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.VISCOEL_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"], c["q"],
+                            (0.7 * c["q"]).astype(np.float32))
         e.set_shots(shots)
         e.forward_device(0)
         e.forward_device(0)
@@ -119,13 +136,14 @@ def gradient3d(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient", "forward2d", "qgradient", "gradient3d"])
+    ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient", "forward2d", "qgradient", "gradient3d",
+                                     "viscoel"])
     ap.add_argument("--n", type=int, default=384, help="3-D padded grid size per axis")
     ap.add_argument("--nshot", type=int, default=2)
     ap.add_argument("--nt", type=int, default=3)
     args = ap.parse_args()
     cases = {"acoustic3d": acoustic3d, "viscoac": viscoac, "gradient": gradient, "forward2d": forward2d,
-             "qgradient": qgradient, "gradient3d": gradient3d}
+             "qgradient": qgradient, "gradient3d": gradient3d, "viscoel": viscoel}
     t = cases[args.case](args)
     print(json.dumps(t))
 

@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(kThreads) q_adj_velocity_kernel(const __grid_c
     if (threadIdx.x == 0) s_dw = 0.0f;
     // T1, T4 on the tile plus halo (zero outside the grid: the forward never updates there)
     constexpr int W4 = SW / 4;
+#pragma unroll 3  // several rows' loads in flight before their shared-memory stores
     for (int i = threadIdx.x; i < SROWS * W4; i += kThreads) {
         const int r = i / W4, c = i - r * W4;
         const int gx = t.x0 - H + r, gz0 = t.z0 - HZ + 4 * c;
@@ -195,6 +196,7 @@ __global__ void __launch_bounds__(kThreads) q_adj_stress_kernel(const __grid_con
     const float* tb = a.spg;
     const int st = a.spg_stride;
     constexpr int W4 = SW / 4;
+#pragma unroll 3  // several rows' loads in flight before their shared-memory stores
     for (int i = threadIdx.x; i < SROWS * W4; i += kThreads) {
         const int r = i / W4, c = i - r * W4;
         const long long off = cell(a, t.shot, t.x0 - H + r, t.z0 - HZ + 4 * c);

@@ -85,6 +85,7 @@ template <int NF>
 __device__ __forceinline__ void stage(float* s, const QArgs& a, const TileRef& t, const float* f0, const float* f1,
                                       const float* f2) {
     constexpr int W4 = SW / 4;
+#pragma unroll 3  // several rows' loads in flight before their shared-memory stores
     for (int i = threadIdx.x; i < SROWS * W4; i += kThreads) {
         const int r = i / W4, c = i - r * W4;
         const long long off = cell(a, t.shot, t.x0 - H + r, t.z0 - HZ + 4 * c);
