@@ -132,22 +132,39 @@ __global__ void __launch_bounds__(kThreads) e_velocity_kernel(const __grid_const
     float* vxz = a.f[E_VXZ];
     float* vzx = a.f[E_VZX];
     float* vzz = a.f[E_VZZ];
-    for (int j = 0; j < kPer; j++) {
-        const int i = threadIdx.x + j * kThreads, r = i / TZ, z = i - r * TZ;
-        const int gx = t.x0 + r, gz = t.z0 + z;
-        if (gx >= nx || gz >= nz) continue;
-        const long long c = cell(a, t.shot, gx, gz);
-        const float o_xx = vxx[c], o_xz = vxz[c], o_zx = vzx[c], o_zz = vzz[c];
-        const float dtb = fm(a.dt, __ldg(a.busg + (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz));
-        float n_xx = fa(o_xx, fm(dtb, rsg<true, 0>(sSxx, r + H, z + HZ, a.a, a.hx)));   // QS:713-720
-        float n_xz = fa(o_xz, fm(dtb, rsg<false, 0>(sSxz, r + H, z + HZ, a.a, a.hz)));  // QS:722-729
-        n_xx = xs(n_xx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
-        n_xz = xs(n_xz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
-        float n_zx = fa(o_zx, fm(dtb, rsg<true, 0>(sSxz, r + H, z + HZ, a.a, a.hx)));   // QS:733-740
-        float n_zz = fa(o_zz, fm(dtb, rsg<false, 0>(sSzz, r + H, z + HZ, a.a, a.hz)));  // QS:741-748
-        n_zx = xs(n_zx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
-        n_zz = xs(n_zz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
-        vxx[c] = n_xx; vxz[c] = n_xz; vzx[c] = n_zx; vzz[c] = n_zz;
+    // four cells per batch: the batch's global loads are issued before its arithmetic
+    for (int j0 = 0; j0 < kPer; j0 += 4) {
+        float o[4][4], bu[4];
+        long long cc[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            ok[u] = gx < nx && gz < nz;
+            cc[u] = cell(a, t.shot, gx, gz);
+            if (ok[u]) {
+                o[u][0] = vxx[cc[u]]; o[u][1] = vxz[cc[u]]; o[u][2] = vzx[cc[u]]; o[u][3] = vzz[cc[u]];
+                bu[u] = __ldg(a.busg + (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (!ok[u]) continue;
+            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
+            const int gx = t.x0 + r, gz = t.z0 + z;
+            const long long c = cc[u];
+            const float dtb = fm(a.dt, bu[u]);
+            float n_xx = fa(o[u][0], fm(dtb, rsg<true, 0>(sSxx, r + H, z + HZ, a.a, a.hx)));   // QS:713-720
+            float n_xz = fa(o[u][1], fm(dtb, rsg<false, 0>(sSxz, r + H, z + HZ, a.a, a.hz)));  // QS:722-729
+            n_xx = xs(n_xx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
+            n_xz = xs(n_xz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
+            float n_zx = fa(o[u][2], fm(dtb, rsg<true, 0>(sSxz, r + H, z + HZ, a.a, a.hx)));   // QS:733-740
+            float n_zz = fa(o[u][3], fm(dtb, rsg<false, 0>(sSzz, r + H, z + HZ, a.a, a.hz)));  // QS:741-748
+            n_zx = xs(n_zx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
+            n_zz = xs(n_zz, gz, nz, a.npz, tb + 2 * st, tb + 3 * st);
+            vxx[c] = n_xx; vxz[c] = n_xz; vzx[c] = n_zx; vzz[c] = n_zz;
+        }
     }
 }
 
