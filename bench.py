@@ -191,7 +191,7 @@ def run_reference_arm(args, world, rank):
 def measure_gradient(args, dev):
     """Config 4: batched adjoint gradient (all shots in one CUDA graph: checkpointed forward,
     per-segment recomputation, adjoint, imaging) against the plain per-shot path (shots one
-    after another, one launch per step, no graph) on a subset of the shots."""
+    after another, one launch per step, no graph) on the same shots."""
     from seismic_code_github_b200 import seisfd as S
     from seismic_code_github_b200 import workloads as W
     case, vp_true = W.config4(nshot=args.grad_nshot, nt=args.grad_nt)
@@ -213,12 +213,12 @@ def measure_gradient(args, dev):
             times.append(t["loop_ms"])
             launches = t["launches"]
         bt = float(np.median(times))
-        # plain per-shot path on the first `grad_plain_shots` shots (it scales linearly in shots)
-        sub = shots[: args.grad_plain_shots]
-        e.set_shots(sub)
-        obs_sub = np.concatenate([r.reshape(-1) for r in
-                                  [obs.reshape(len(shots), len(rx), case.nt)[i] for i in range(len(sub))]])
-        e.gradient(obs_sub, per_shot=True)
+        # plain per-shot path (one shot after another, one launch per step, no graph) on the same
+        # engine and shot set, so both schedules have the same memory for kept D_k slots
+        sub = shots if args.grad_plain_shots <= 0 else shots[: args.grad_plain_shots]
+        if len(sub) < len(shots):
+            e.set_shots(sub)
+        e.gradient(obs[: len(sub) * len(rx) * case.nt], per_shot=True)
         t_plain = e.timing()
     batched_sps = len(shots) / (bt / 1e3)
     plain_sps = len(sub) / (t_plain["loop_ms"] / 1e3)
@@ -352,7 +352,7 @@ def measure_viscoelastic(args, dev):
 def measure_q_gradient(args, dev):
     """Config-3 geometry: the viscoacoustic gradient d misfit / d vp and d misfit / d (1/Q) of 16
     shots (uneven record lengths), observed data from the Q field scaled by 0.8, batched (one
-    CUDA graph) against the plain per-shot schedule on a subset of the shots."""
+    CUDA graph) against the plain per-shot schedule on the same shots."""
     from seismic_code_github_b200 import seisfd as S
     from seismic_code_github_b200 import workloads as W
     c = W.config3(nshot=args.qg_nshot)
@@ -373,9 +373,10 @@ def measure_q_gradient(args, dev):
             e.gradient(obs, want_invq=True)
             ms.append(e.timing()["loop_ms"])
         t = e.timing()
-        sub = shots[: args.qg_plain_shots]
+        sub = shots if args.qg_plain_shots <= 0 else shots[: args.qg_plain_shots]
         offs = np.cumsum([0] + [s.nrec * s.nt for s in shots])
-        e.set_shots(sub)
+        if len(sub) < len(shots):
+            e.set_shots(sub)
         e.gradient(obs[: offs[len(sub)]], want_invq=True, per_shot=True)
         tp = e.timing()
     bt = float(np.median(ms))
@@ -390,7 +391,7 @@ def measure_q_gradient(args, dev):
 def measure_3d_gradient(args, dev):
     """Config-5 geometry (612^3 padded, order 8): the 3-D gradient of a few shots with record
     lengths scaled by --d3g-nt-scale; the library plans shot groups and checkpoint levels to the
-    device memory.  Batched against the per-shot schedule on one shot."""
+    device memory.  Batched against the per-shot schedule on the same shots."""
     from seismic_code_github_b200 import seisfd as S
     from seismic_code_github_b200 import workloads as W
     c = W.config5(nshot=args.d3g_nshot, nt_scale=args.d3g_nt_scale)
@@ -407,9 +408,7 @@ def measure_3d_gradient(args, dev):
         e.set_model(vp)
         e.gradient(obs)
         t = e.timing()
-        sub = shots[:1]
-        e.set_shots(sub)
-        e.gradient(obs[: sub[0].nrec * sub[0].nt], per_shot=True)
+        e.gradient(obs, per_shot=True)  # the same shots and memory, one shot per group
         tp = e.timing()
     del vp
     levels = 2 if t["kernel_variant"] == 62 else 1
@@ -419,8 +418,8 @@ def measure_3d_gradient(args, dev):
             "batched_shots_per_s": len(shots) / (t["loop_ms"] / 1e3), "batched_ms": t["loop_ms"],
             "checkpoint_levels": levels, "passes": t["point_updates"] / pts,
             "gpts_per_s_all_passes": t["point_updates"] / (t["loop_ms"] / 1e3) / 1e9,
-            "plain_shots_per_s": 1.0 / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"],
-            "batched_over_plain": (len(shots) / t["loop_ms"]) / (1.0 / tp["loop_ms"]),
+            "plain_shots_per_s": len(shots) / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"],
+            "batched_over_plain": tp["loop_ms"] / t["loop_ms"],
             "gradient_accuracy": "relL2 vs FP64 3-D adjoint oracle 6.7e-7 (tests/test_gradient3d_gpu.py)"}
 
 
@@ -637,7 +636,7 @@ def main():
     ap.add_argument("--grad-steps", type=int, default=2, help="timed batched gradients (0 = skip)")
     ap.add_argument("--grad-nshot", type=int, default=32)
     ap.add_argument("--grad-nt", type=int, default=3000)
-    ap.add_argument("--grad-plain-shots", type=int, default=8)
+    ap.add_argument("--grad-plain-shots", type=int, default=0, help="plain per-shot gradient shots (0 = all)")
     ap.add_argument("--q-steps", type=int, default=2, help="timed viscoacoustic forwards (0 = skip)")
     ap.add_argument("--q-nshot", type=int, default=16)
     ap.add_argument("--q-cpu-steps", type=int, default=120)
@@ -649,7 +648,7 @@ def main():
     ap.add_argument("--qg-steps", type=int, default=1, help="timed viscoacoustic gradients (0 = skip)")
     ap.add_argument("--qg-nshot", type=int, default=16)
     ap.add_argument("--qg-nt-scale", type=float, default=1.0)
-    ap.add_argument("--qg-plain-shots", type=int, default=2)
+    ap.add_argument("--qg-plain-shots", type=int, default=0, help="plain per-shot gradient shots (0 = all)")
     ap.add_argument("--d3g-nshot", type=int, default=4, help="3-D gradient shots (0 = skip)")
     ap.add_argument("--d3g-nt-scale", type=float, default=0.05)
     args = ap.parse_args()

@@ -119,8 +119,9 @@ struct sfd_ctx {
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
     int grad_C = 0, grad_ncp = 0;
+    int grad_keep = 0;          // first segment whose D_k the first forward keeps (no recomputation)
     float* d_ckpt = nullptr;    // [ncp][3 fields][nshot * shot_stride]
-    float* d_div = nullptr;     // [C][nshot * shot_stride]: D_k of the segment being recomputed
+    float* d_div = nullptr;     // D_k slots: [C] of the segment being recomputed, then the kept tail
     float* d_adj = nullptr;     // adjoint state: nu0 nu1 x0 x1 z0 z1 (viscoacoustic: 8 adjoints + Qx Qz)
     CUtensorMap adj_tmaps[6];   // TMA descriptors of the acoustic adjoint buffers
     float* d_gseg = nullptr;    // per-segment imaging sum (float)
@@ -749,7 +750,6 @@ int grad_alloc(sfd_ctx* ctx) {
     const size_t fs = (size_t)ctx->nshot * ctx->L.shot_stride;
     const size_t nrec = std::max<long long>(1, ctx->rec_total);
     CK(cudaMalloc(&ctx->d_ckpt, sizeof(float) * fs * gs.ckpt * ncp));
-    CK(cudaMalloc(&ctx->d_div, sizeof(float) * fs * gs.div * C));
     if (!ctx->d_adj) {
         CK(cudaMalloc(&ctx->d_adj, sizeof(float) * fs * gs.adj));
         CK(cudaMalloc(&ctx->d_gseg, sizeof(float) * fs * gs.img));
@@ -776,6 +776,24 @@ int grad_alloc(sfd_ctx* ctx) {
         CK(cudaMalloc(&ctx->d_misfit, sizeof(double)));
         CK(cudaMalloc(&ctx->d_grad, sizeof(double) * (size_t)ctx->g.nx * ctx->g.nz));
     }
+    // D_k slots: C for the segment being recomputed, plus as many tail steps as the memory budget
+    // holds (whole segments from the last one back): the first forward keeps their D_k, and those
+    // segments are transposed without recomputation
+    const size_t slot = sizeof(float) * fs * gs.div;
+    size_t freeb = 0, totb = 0;
+    CK(cudaMemGetInfo(&freeb, &totb));
+    double budget = 0.85 * (double)freeb - (double)(1ull << 30) - (double)slot * C;
+    if (ctx->mem_limit > 0) budget = std::min(budget, (double)ctx->mem_limit - (double)slot * C);
+    const long long extra = budget > 0 ? (long long)(budget / (double)slot) : 0;
+    int keep = ncp;  // segments keep .. ncp-1 are kept
+    while (keep > 0 && (long long)ctx->nt_max - (long long)(keep - 1) * C <= extra) keep--;
+    const long long nslots = C + ((long long)ctx->nt_max - (long long)keep * C);
+    if (cudaMalloc(&ctx->d_div, slot * nslots) != cudaSuccess) {
+        cudaGetLastError();
+        keep = ncp;
+        CK(cudaMalloc(&ctx->d_div, slot * C));
+    }
+    ctx->grad_keep = keep;
     ctx->grad_C = C;
     ctx->grad_ncp = ncp;
     return SFD_OK;
@@ -909,12 +927,18 @@ int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches
     const int per_step = visco ? 2 : 1;  // launches per forward or adjoint step
     int nrec_max = 0;
     for (int s = r.first; s < r.first + r.count; s++) nrec_max = std::max(nrec_max, ctx->h_shots[s].nrec);
-    // forward with checkpoints
+    // D_k slot of step k: kept tail steps after the C recomputation slots
+    const int kkeep = ctx->grad_keep * C;
+    auto dslot = [&](int k, int k0) -> float* {
+        const size_t i = k >= kkeep ? (size_t)C + (k - kkeep) : (size_t)(k - k0);
+        return ctx->d_div + i * gs.div * fs;
+    };
+    // forward with checkpoints (and D_k of the kept tail)
     for (int k = 0; k < ctx->nt_max; k++) {
         const int act = range_active(ctx, r, k);
         if (act == 0) break;
         if (k % C == 0 && (rc = grad_copy_state(ctx, r, k / C, k & 1, true))) return rc;
-        if ((rc = grad_fwd_step(ctx, r, k, act, nullptr))) return rc;
+        if ((rc = grad_fwd_step(ctx, r, k, act, k >= kkeep ? dslot(k, 0) : nullptr))) return rc;
         *launches += per_step;
     }
     // residuals of this range and the misfit
@@ -933,19 +957,21 @@ int enqueue_gradient_range(sfd_ctx* ctx, const GradRange& r, long long* launches
     for (int j = ncp - 1; j >= 0; j--) {
         const int k0 = j * C, k1 = std::min(k0 + C, ctx->nt_max);
         if (range_active(ctx, r, k0) == 0) continue;
-        if ((rc = grad_copy_state(ctx, r, j, k0 & 1, false))) return rc;
         for (int i = 0; i < gs.img; i++)
             CK(cudaMemsetAsync(ctx->d_gseg + i * fs + off, 0, len * sizeof(float), ctx->stream));
-        for (int k = k0; k < k1; k++) {
-            const int act = range_active(ctx, r, k);
-            if (act == 0) break;
-            if ((rc = grad_fwd_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * gs.div * fs))) return rc;
-            *launches += per_step;
+        if (j < ctx->grad_keep) {  // recompute the segment from its checkpoint, keeping D_k
+            if ((rc = grad_copy_state(ctx, r, j, k0 & 1, false))) return rc;
+            for (int k = k0; k < k1; k++) {
+                const int act = range_active(ctx, r, k);
+                if (act == 0) break;
+                if ((rc = grad_fwd_step(ctx, r, k, act, dslot(k, k0)))) return rc;
+                *launches += per_step;
+            }
         }
         for (int k = k1 - 1; k >= k0; k--) {
             const int act = range_active(ctx, r, k);
             if (act == 0) continue;
-            if ((rc = grad_adj_step(ctx, r, k, act, ctx->d_div + (size_t)(k - k0) * gs.div * fs))) return rc;
+            if ((rc = grad_adj_step(ctx, r, k, act, dslot(k, k0)))) return rc;
             *launches += per_step;
         }
         for (int i = 0; i < gs.img; i++) {
@@ -1047,9 +1073,11 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     ctx->timing.device_ms = ms;
     ctx->timing.graph = batched ? 1 : 0;
     ctx->timing.kernel_variant = visco ? 50 : 20 + ctx->plan.stages;
+    // forward, recomputation of the segments before the kept tail, adjoint
     double pts = 0;
-    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * s.nt;
-    ctx->timing.point_updates = 3 * pts;  // forward, recomputation, adjoint
+    const int kkeep = ctx->grad_keep * ctx->grad_C;
+    for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * (2.0 * s.nt + std::min(s.nt, kkeep));
+    ctx->timing.point_updates = pts;
     double mis = 0;
     CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
     if (misfit) *misfit = (float)mis;
