@@ -222,13 +222,29 @@ def measure_gradient(args, dev):
         t_plain = e.timing()
     batched_sps = len(shots) / (bt / 1e3)
     plain_sps = len(sub) / (t_plain["loop_ms"] / 1e3)
+    oracle = None
+    if not args.no_cpu_baseline:
+        # the reference has no adjoint: the FP64 adjoint oracle is timed beside the GPU path as a
+        # labelled oracle on a bounded sample (one shot, the first grad_cpu_steps steps)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        n = args.grad_cpu_steps
+        o = obs.reshape(len(shots), len(rx), case.nt)[0][:, :n]
+        t0 = time.perf_counter()
+        ol.afd_gradient_f64(case.Nx, case.Nz, case.PML, n, case.dx, case.dz, case.dt, case.vp, case.den, w[:n],
+                            case.src_x[0], case.src_z[0], rx, rz, o)
+        wall = time.perf_counter() - t0
+        oracle = {"shots_per_s_equivalent": (n / case.nt) / wall, "cores": os.cpu_count(), "kind": "oracle (FP64)",
+                  "sample": f"one shot of the FP64 adjoint oracle (oracle/adj_oracle.cpp, OpenMP), {n} of {case.nt} "
+                            f"steps: forward, residual, adjoint and imaging; scaled to whole shots"}
     return {"workload": f"config 4: adjoint gradient d(misfit)/d(vp), {case.NZ}x{case.NX} interior "
                         f"({case.Nz}x{case.Nx} padded), {len(shots)} shots, nt={case.nt}, checkpoints every "
                         f"{case.extra['checkpoint_interval']} steps, start model = true model smoothed (sigma 15)",
             "batched_shots_per_s": batched_sps, "batched_ms": bt, "batched_launches": launches,
             "plain_shots_per_s": plain_sps, "plain_ms": t_plain["loop_ms"], "plain_shots": len(sub),
             "plain_launches": t_plain["launches"], "batched_over_plain": batched_sps / plain_sps,
-            "misfit": float(mis), "gradient_accuracy": "relL2 vs FP64 adjoint oracle 7.6e-7 (tests/test_gradient_gpu.py)"}
+            "misfit": float(mis), "gradient_accuracy": "relL2 vs FP64 adjoint oracle 7.6e-7 (tests/test_gradient_gpu.py)",
+            "cpu_oracle": oracle}
 
 
 def measure_gradient_sharded(args, dev, world, rank):
@@ -343,10 +359,28 @@ def measure_viscoelastic(args, dev):
             ms.append(e.timing()["loop_ms"])
     pts = float(sum(Nx * Nz * nt for nt in c["nt"]))
     gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        vp, rho, q = c["interior"]
+        vs, qs = (vp / 1.8).astype(np.float32), (0.7 * q).astype(np.float32)
+        steps = max(1, args.q_cpu_steps // 2)
+        run = lambda n: ol.q_forward(vp, vs, rho, q, qs, c["dx"], c["dz"], c["dt"], c["f0"], n, c["PML"], c["PML"],
+                                     c["src_x"][0] + 1, c["src_z"][0] + 1)
+        t0 = time.perf_counter()
+        run(1)
+        t1 = time.perf_counter()
+        run(1 + steps)
+        wall = (time.perf_counter() - t1) - (t1 - t0)
+        cpu = {"value": Nx * Nz * steps / max(wall, 1e-9) / 1e9, "unit": "Gpts/s", "cores": os.cpu_count(),
+               "kind": "port", "sample": f"restated visco-elastic Q_forward step (oracle/q_oracle.cpp, OpenMP) on one "
+                                         f"shot: the difference of a {steps + 1}- and a 1-sample run ({steps} steps)"}
     return {"workload": f"config 3 geometry, visco-elastic P-SV (vs = vp/1.8): {c['NZ']}x{c['NX']} interior, "
                         f"{len(shots)} shots, nt {min(c['nt'])}-{max(c['nt'])}",
             "gpts_per_s": gpts, "shots_per_s": len(shots) / (float(np.median(ms)) / 1e3),
-            "loop_ms": float(np.median(ms)), "parity": "bit-exact vs FP32 restatement (strzz and strxx)"}
+            "loop_ms": float(np.median(ms)), "parity": "bit-exact vs FP32 restatement (strzz and strxx)",
+            "cpu_baseline": cpu}
 
 
 def measure_q_gradient(args, dev):
@@ -637,6 +671,7 @@ def main():
     ap.add_argument("--grad-nshot", type=int, default=32)
     ap.add_argument("--grad-nt", type=int, default=3000)
     ap.add_argument("--grad-plain-shots", type=int, default=0, help="plain per-shot gradient shots (0 = all)")
+    ap.add_argument("--grad-cpu-steps", type=int, default=100, help="steps of the timed FP64 adjoint oracle sample")
     ap.add_argument("--q-steps", type=int, default=2, help="timed viscoacoustic forwards (0 = skip)")
     ap.add_argument("--q-nshot", type=int, default=16)
     ap.add_argument("--q-cpu-steps", type=int, default=120)
