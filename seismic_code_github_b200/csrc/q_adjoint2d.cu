@@ -41,7 +41,8 @@ constexpr int SROWS = TX + 2 * H;  // staged rows x0-5 .. x0+TX+4
 constexpr int SW = TZ + 2 * HZ;    // staged columns z0-8 .. z0+TZ+7
 constexpr int SMEM = SROWS * SW;
 constexpr int kPer = TX * TZ / kThreads;  // cells per thread
-constexpr int kNB = 4;                    // cells per load batch
+constexpr int kNB = 4;    // cells per load batch
+constexpr int kNBS = 2;  // cells per load batch of the stress kernel (three CTAs per SM)
 
 struct Tile {
     int shot, tile, x0, z0;
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kThreads) q_adj_velocity_kernel(const __grid_c
     }
 }
 
-__global__ void __launch_bounds__(kThreads) q_adj_stress_kernel(const __grid_constant__ QAdjArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) q_adj_stress_kernel(const __grid_constant__ QAdjArgs a) {
     __shared__ __align__(16) float sQx[SMEM];
     __shared__ __align__(16) float sQz[SMEM];
     Tile t;
@@ -208,12 +209,12 @@ __global__ void __launch_bounds__(kThreads) q_adj_stress_kernel(const __grid_con
 #pragma unroll
     for (int m = 0; m < 5; m++) c[m] = a.a[m];
     const float dt = a.dt, f = a.f_mem;
-    for (int j0 = 0; j0 < kPer; j0 += kNB) {
-        float hsx[kNB], hsz[kNB], hsr[kNB], hrx[kNB], hrz[kNB], hrr[kNB], d1[kNB], d4[kNB], g1[kNB], g2[kNB];
-        long long cc[kNB];
-        bool ok[kNB];
+    for (int j0 = 0; j0 < kPer; j0 += kNBS) {
+        float hsx[kNBS], hsz[kNBS], hsr[kNBS], hrx[kNBS], hrz[kNBS], hrr[kNBS], d1[kNBS], d4[kNBS], g1[kNBS], g2[kNBS];
+        long long cc[kNBS];
+        bool ok[kNBS];
 #pragma unroll
-        for (int u = 0; u < kNB; u++) {
+        for (int u = 0; u < kNBS; u++) {
             const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
             const int gx = t.x0 + r, gz = t.z0 + z;
             ok[u] = gx < nx && gz < nz;
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) q_adj_stress_kernel(const __grid_con
             }
         }
 #pragma unroll
-        for (int u = 0; u < kNB; u++) {
+        for (int u = 0; u < kNBS; u++) {
             if (!ok[u]) continue;
             const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
             const int gx = t.x0 + r, gz = t.z0 + z;

@@ -33,7 +33,8 @@ constexpr int SROWS = TX + 2 * H;       // 74
 constexpr int SW = TZ + 2 * HZ;         // 80
 constexpr int SMEM = SROWS * SW;        // floats per staged field
 constexpr int kPer = TX * TZ / kThreads;  // cells per thread
-constexpr int kNB = 4;                  // cells per load batch
+constexpr int kNB = 4;    // cells per load batch
+constexpr int kNBS = 2;  // cells per load batch of the stress kernel (three CTAs per SM)
 static_assert(kPer % kNB == 0, "whole batches");
 
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(kThreads) q_velocity_kernel(const __grid_const
     }
 }
 
-__global__ void __launch_bounds__(kThreads) q_stress_kernel(const __grid_constant__ QArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) q_stress_kernel(const __grid_constant__ QArgs a) {
     __shared__ __align__(16) float sVx[SMEM];
     __shared__ __align__(16) float sVz[SMEM];
     TileRef t;
@@ -165,12 +166,12 @@ __global__ void __launch_bounds__(kThreads) q_stress_kernel(const __grid_constan
     const int step = a.step;
     const float wav = __ldg(a.wavelets + t.sd.wav_off + step);
     const ShotDev& sd = t.sd;
-    for (int j0 = 0; j0 < kPer; j0 += kNB) {
-        float p1[kNB], p2[kNB], sx0[kNB], sz0[kNB], sr0[kNB], rx0[kNB], rz0[kNB], rr0[kNB];
-        long long cc[kNB];
-        bool ok[kNB];
+    for (int j0 = 0; j0 < kPer; j0 += kNBS) {
+        float p1[kNBS], p2[kNBS], sx0[kNBS], sz0[kNBS], sr0[kNBS], rx0[kNBS], rz0[kNBS], rr0[kNBS];
+        long long cc[kNBS];
+        bool ok[kNBS];
 #pragma unroll
-        for (int u = 0; u < kNB; u++) {
+        for (int u = 0; u < kNBS; u++) {
             const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
             const int gx = t.x0 + r, gz = t.z0 + z;
             ok[u] = gx < nx && gz < nz;
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) q_stress_kernel(const __grid_constan
             }
         }
 #pragma unroll
-        for (int u = 0; u < kNB; u++) {
+        for (int u = 0; u < kNBS; u++) {
             if (!ok[u]) continue;
             const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
             const int gx = t.x0 + r, gz = t.z0 + z;
