@@ -1,0 +1,370 @@
+// ORACLE -- test infrastructure only. CPU restatement of the reference's isotropic elastic
+// standard-staggered-grid modelling of one shot (forward/yang_version_2016_2_2, 'abc' mode:
+// cosine sponge on all four sides) for a flat surface, used by tests/ as the checker of the
+// SFD_ELASTIC_2D GPU path.  The reference is Fortran 90 + MPI + OpenMP and cannot be compiled in
+// this environment (no Fortran compiler), so this restatement is not pinned by a run of the
+// reference: "parity unpinned" for this scheme; it is checked by physics properties instead
+// (tests/test_iso_oracle.py).
+//
+// Files of forward/yang_version_2016_2_2: YMOD = Iso_multishot_fd_module_zy_m2.f90,
+// YPRI = Iso_multishot_fd_subroutine_fsbc_zy_m2_pri.f90, YPUB = Iso_multishot_fd_subroutine_fsbc_zy_m2_pub.f90
+//   YMOD:23-27     coefficients a100..a104 (10th order)
+//   YPUB:188-313   window, edge padding, itopoe = nint(topo/dz) + npzn, source cell, gc2d (sigma 2)
+//   YPUB:323-547   substagger: Lame moduli, staggered buoyancies and moduli, rows above itopoe
+//                  refilled from row itopoe
+//   YPUB:549-634   modipapml / gauss_filter_2d: rows k <= itopoe(i) replaced IN PLACE by the
+//                  gc2d-weighted sum of their window.  The reference runs this loop under an
+//                  OpenMP DO while it overwrites u, so with several threads its result depends on
+//                  the schedule; the restatement takes the serial (one-thread) order.
+//   YPUB:796-849   csponge                        YPUB:851-897 calpmlbclrtb (split sponge)
+//   YPUB:1095-1157 caluxabs    YPUB:1347-1407 caluzabs    YPUB:1410-1426 calu (sums)
+//   YPUB:1429-1466 addsrc      YPUB:1470-1501 get_gauss_filter_coe
+//   YPRI:234-386   isoewm2dabc (time loop)     YPUB:2-16 get_record (record1 = vx, record2 = vz)
+// The split fields also hold a row k = 0 (YPUB:1095 `ux(0:nz,nx)`, loops from itopo - npzn = 0);
+// calu and get_record never read it, so it is not kept here.  Fortran (k, i), k = z, i = x,
+// maps to C index (i-1)*nz + (k-1).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "oracle.h"
+
+namespace {
+
+template <typename T>
+struct Field {  // (lo_k:hi_k, lo_i:hi_i), Fortran order
+    int lk, hk, li, hi, nk;
+    std::vector<T> d;
+    Field() {}
+    Field(int lk_, int hk_, int li_, int hi_) : lk(lk_), hk(hk_), li(li_), hi(hi_), nk(hk_ - lk_ + 1) {
+        d.assign((size_t)nk * (hi_ - li_ + 1), T(0));
+    }
+    T& operator()(int k, int i) { return d[(size_t)(i - li) * nk + (k - lk)]; }
+    T operator()(int k, int i) const { return d[(size_t)(i - li) * nk + (k - lk)]; }
+};
+
+template <typename T>
+struct IsoSolver {
+    int nx, nz, npxn, npxp, npzn, npzp;
+    T dx, dz, dt;
+    T a[5];
+    Field<T> vx, vz, sxx, szz, sxz;                                     // (-4:nz+5, -4:nx+5)
+    Field<T> vxx, vxz, vzx, vzz, sxxx, sxxz, szzx, szzz, sxzx, sxzz;    // (1:nz, 1:nx)
+    Field<T> busg1e, busg2e, lambsg, lambmusg, musge;                   // (1:nz, 1:nx)
+    std::vector<T> spgxn, spgxp, spgzn, spgzp, spg1xn, spg2xp, spg1zn, spg2zp;
+
+    void alloc() {
+        auto H = [&] { return Field<T>(-4, nz + 5, -4, nx + 5); };
+        auto N = [&] { return Field<T>(1, nz, 1, nx); };
+        vx = H(); vz = H(); sxx = H(); szz = H(); sxz = H();
+        for (auto* f : {&vxx, &vxz, &vzx, &vzz, &sxxx, &sxxz, &szzx, &szzz, &sxzx, &sxzz}) *f = N();
+    }
+
+    // YPUB:1095-1157 (x) and YPUB:1347-1407 (z); flag 0: u(i) - u(i-1) ..., flag 1: u(i+1) - u(i) ...
+    T der(const Field<T>& u, int k, int i, bool xdir, int flag) const {
+        auto U = [&](int o) { return xdir ? u(k, i + o) : u(k + o, i); };
+        T s = 0;
+        for (int m = 0; m < 5; m++) {
+            const T t = flag == 0 ? U(m) - U(-1 - m) : U(1 + m) - U(-m);
+            s = (m == 0) ? a[0] * t : s + a[m] * t;
+        }
+        return s;
+    }
+    // ux(k,i) = ux(k,i) + (dt/dh)*pa(k,i)*(...)
+    void update(Field<T>& ux, const Field<T>& u, const Field<T>& pa, bool xdir, int flag) {
+        const T c = xdir ? dt / dx : dt / dz;
+#pragma omp parallel for schedule(static)
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= nz; k++) ux(k, i) = ux(k, i) + c * pa(k, i) * der(u, k, i, xdir, flag);
+    }
+    // YPUB:851-897, flat surface (itopo(i) - npzn = 0); the top loop runs k = 0..npzn with
+    // factor spgzn(k + 1), of which rows 1..npzn are kept here
+    void sponge(Field<T>& ux, Field<T>& uz, const std::vector<T>& sxn, const std::vector<T>& sxp,
+                const std::vector<T>& szn, const std::vector<T>& szp) {
+        for (int i = 1; i <= npxn + 1; i++)
+            for (int k = 1; k <= nz; k++) ux(k, i) = ux(k, i) * sxn[i - 1];
+        for (int i = 1; i <= npxp + 1; i++)
+            for (int k = 1; k <= nz; k++) ux(k, nx - i + 1) = ux(k, nx - i + 1) * sxp[i - 1];
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= npzn; k++) uz(k, i) = uz(k, i) * szn[k];
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= npzp + 1; k++) uz(nz - k + 1, i) = uz(nz - k + 1, i) * szp[k - 1];
+    }
+    void sum2(Field<T>& v, const Field<T>& a_, const Field<T>& b_) {  // YPUB:1410-1426
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= nz; k++) v(k, i) = a_(k, i) + b_(k, i);
+    }
+
+    // YPRI:305-359, one step of isoewm2dabc; `src` adds the source to a split stress
+    template <typename Src>
+    void step(Src&& src) {
+        update(vxx, sxx, busg2e, true, 0);     // xflag 0, strxx
+        update(vxz, sxz, busg2e, false, 0);    // zflag 0, strxz
+        sponge(vxx, vxz, spgxn, spgxp, spgzn, spgzp);
+        sum2(vx, vxx, vxz);
+        update(vzx, sxz, busg1e, true, 1);     // xflag 1, strxz
+        update(vzz, szz, busg1e, false, 1);    // zflag 1, strzz
+        sponge(vzx, vzz, spg1xn, spg2xp, spg1zn, spg2zp);
+        sum2(vz, vzx, vzz);
+        update(sxxx, vx, lambmusg, true, 1);
+        update(sxxz, vz, lambsg, false, 0);
+        sponge(sxxx, sxxz, spg1xn, spg2xp, spgzn, spgzp);
+        src(sxxx);
+        sum2(sxx, sxxx, sxxz);
+        update(szzx, vx, lambsg, true, 1);
+        update(szzz, vz, lambmusg, false, 0);
+        sponge(szzx, szzz, spg1xn, spg2xp, spgzn, spgzp);
+        src(szzx);
+        sum2(szz, szzx, szzz);
+        update(sxzx, vz, musge, true, 0);
+        update(sxzz, vx, musge, false, 1);
+        sponge(sxzx, sxzz, spgxn, spgxp, spg1zn, spg2zp);
+        sum2(sxz, sxzx, sxzz);
+    }
+};
+
+// YPUB:592-634, serial order: rows k = 1..itopo of every column, each replaced by the weighted
+// sum of its (2 rgau - 1)^2 window as it stands at that moment
+template <typename T>
+void gauss_filter(Field<T>& u, int nx, int nz, int rgau, int itopo, const Field<T>& gc) {
+    const int w = 2 * rgau - 1;
+    for (int i = 1; i <= nx; i++)
+        for (int k = 1; k <= itopo; k++) {
+            T s = 0;
+            int idx2 = 1;
+            for (int n = i - (rgau - 1); n <= i + (rgau - 1); n++) {
+                int idx1 = 1;
+                for (int m = k - (rgau - 1); m <= k + (rgau - 1); m++) {
+                    if (n >= 1 && n <= nx && m >= 1 && m <= nz && idx2 <= w && idx1 <= w) s = s + u(m, n) * gc(idx1, idx2);
+                    idx1++;
+                }
+                idx2++;
+            }
+            u(k, i) = s;
+        }
+}
+
+// Model preparation of one shot window (YPUB:188-634) into S; the Gaussian table into gc.
+template <typename T>
+int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const float* rho_in, IsoSolver<T>& S,
+            Field<T>& gc) {
+    const int nx_m = c->nx, nz_m = c->nz;
+    const int nxe = c->ixmaxe - c->ixmine + 1, nze = nz_m;
+    if (c->rgau < 1 || c->npxn < 1 || c->npxp < 1 || c->npzn < 1 || c->npzp < 1) return 1;
+    S.npxn = c->npxn; S.npxp = c->npxp; S.npzn = c->npzn; S.npzp = c->npzp;
+    S.nx = nxe + c->npxn + c->npxp;
+    S.nz = nze + c->npzn + c->npzp;
+    S.dx = c->dx; S.dz = c->dz; S.dt = c->dt;
+    // YMOD:23-27, single precision constants
+    const float af[5] = {19845.0f / 16384.0f, -735.0f / 8192.0f, 567.0f / 40960.0f, -405.0f / 229376.0f,
+                         35.0f / 294912.0f};
+    for (int m = 0; m < 5; m++) S.a[m] = (T)af[m];
+    if (S.nx < 12 || S.nz < 12) return 1;
+    S.alloc();
+    const int NX = S.nx, NZ = S.nz;
+    const int itopo = c->npzn;  // flat surface: nint(0/dz) + npzn (YPUB:306-308)
+    // YPUB:210-258 window and edge padding
+    Field<T> vpe(1, NZ, 1, NX), vse(1, NZ, 1, NX), rhoe(1, NZ, 1, NX);
+    auto in = [&](const float* m, int k, int i) { return (T)m[(size_t)(i - 1) * nz_m + (k - 1)]; };
+    for (int i = 1; i <= nxe; i++) {
+        int io = i + c->ixmine;
+        if (io < 1) io = 1;
+        if (io > nx_m) io = nx_m;
+        for (int k = 1; k <= nze; k++) {
+            vpe(k + c->npzn, i + c->npxn) = in(vp_in, k, io);
+            vse(k + c->npzn, i + c->npxn) = in(vs_in, k, io);
+            rhoe(k + c->npzn, i + c->npxn) = in(rho_in, k, io);
+        }
+    }
+    for (auto* f : {&vpe, &vse, &rhoe}) {
+        for (int k = 1; k <= c->npzn; k++)
+            for (int i = 1; i <= NX; i++) (*f)(k, i) = (*f)(c->npzn + 1, i);
+        for (int k = c->npzn + nze + 1; k <= NZ; k++)
+            for (int i = 1; i <= NX; i++) (*f)(k, i) = (*f)(c->npzn + nz_m, i);
+        for (int k = 1; k <= NZ; k++)
+            for (int i = 1; i <= c->npxn; i++) (*f)(k, i) = (*f)(k, c->npxn + 1);
+        for (int k = 1; k <= NZ; k++)
+            for (int i = c->npxn + nxe + 1; i <= NX; i++) (*f)(k, i) = (*f)(k, c->npxn + nxe);
+    }
+    // YPUB:1470-1501 Gaussian coefficients, sigma = 2.0 cells, (2 rgau - 1)^2 window, normalised
+    const T pi = (T)3.1415926f;
+    const int w = 2 * c->rgau - 1;
+    gc = Field<T>(1, w, 1, w);
+    {
+        const T sigma2 = T(2.0) * T(2.0);
+        const int cen = (w + 1) / 2;
+        T sum_tmp = 0;
+        for (int j = 1; j <= w; j++)
+            for (int i = 1; i <= w; i++) {
+                const T dis = (T)((j - cen) * (j - cen) + (i - cen) * (i - cen));
+                gc(i, j) = T(1) / (T(2) * pi * sigma2) * std::exp(-(dis / (T(2) * sigma2)));
+            }
+        for (int j = 1; j <= w; j++)
+            for (int i = 1; i <= w; i++) sum_tmp = sum_tmp + gc(i, j);
+        for (auto& v : gc.d) v = v / sum_tmp;
+    }
+    // YPUB:323-547 substagger
+    Field<T> mu(1, NZ, 1, NX), lamb(1, NZ, 1, NX), busg1(1, NZ, 1, NX), busg2(1, NZ, 1, NX), musg(1, NZ, 1, NX);
+    S.busg1e = Field<T>(1, NZ, 1, NX); S.busg2e = Field<T>(1, NZ, 1, NX); S.musge = Field<T>(1, NZ, 1, NX);
+    S.lambsg = Field<T>(1, NZ, 1, NX); S.lambmusg = Field<T>(1, NZ, 1, NX);
+    for (int i = 1; i <= NX; i++)
+        for (int k = 1; k <= NZ; k++) {
+            mu(k, i) = rhoe(k, i) * vse(k, i) * vse(k, i);
+            lamb(k, i) = rhoe(k, i) * vpe(k, i) * vpe(k, i) - T(2.0) * mu(k, i);
+        }
+    for (int i = 1; i <= NX - 1; i++)
+        for (int k = 1; k <= NZ - 1; k++)
+            busg1(k, i) = T(0.25) * (rhoe(k, i) + rhoe(k + 1, i) + rhoe(k + 1, i + 1) + rhoe(k, i + 1));
+    for (int i = 1; i <= NX; i++) busg1(NZ, i) = busg1(NZ - 1, i);
+    for (int k = 1; k <= NZ; k++) busg1(k, NX) = busg1(k, NX - 1);
+    for (int i = 1; i <= NX; i++)
+        for (int k = 1; k <= NZ; k++) {
+            if (busg1(k, i) == T(0)) return 2;  // YPUB:371 stops here
+            busg1(k, i) = T(1.0) / busg1(k, i);
+        }
+    for (int i = 1; i <= NX; i++)
+        for (int k = 2; k <= NZ; k++) S.busg1e(k, i) = T(0.5) * (busg1(k, i) + busg1(k - 1, i));
+    for (int i = 1; i <= NX; i++) S.busg1e(1, i) = busg1(1, i);
+    for (int i = 1; i <= NX; i++)
+        for (int k = 1; k <= NZ; k++) {
+            if (rhoe(k, i) == T(0)) return 2;
+            busg2(k, i) = T(1.0) / rhoe(k, i);
+        }
+    for (int i = 1; i <= NX - 1; i++)
+        for (int k = 1; k <= NZ; k++) S.busg2e(k, i) = T(0.5) * (busg2(k, i) + busg2(k, i + 1));
+    for (int k = 1; k <= NZ; k++) S.busg2e(k, NX) = busg2(k, NX);
+    for (int i = 1; i <= NX; i++)
+        for (int k = 1; k <= NZ - 1; k++) musg(k, i) = T(0.5) * (mu(k + 1, i) + mu(k, i));
+    for (int i = 1; i <= NX; i++) musg(NZ, i) = mu(NZ, i);
+    for (int i = 1; i <= NX - 1; i++)
+        for (int k = 2; k <= NZ; k++) {
+            if (musg(k, i) != T(0) && musg(k - 1, i) != T(0) && musg(k, i + 1) != T(0) && musg(k - 1, i + 1) != T(0))
+                S.musge(k, i) = T(4.0) / (T(1.0) / musg(k, i) + T(1.0) / musg(k, i + 1) + T(1.0) / musg(k - 1, i + 1) +
+                                          T(1.0) / musg(k - 1, i));
+            else
+                S.musge(k, i) = T(0);
+        }
+    for (int i = 1; i <= NX; i++) S.musge(1, i) = musg(1, i);
+    for (int k = 1; k <= NZ; k++) S.musge(k, NX) = musg(k, NX);
+    for (int k = 1; k <= NZ; k++)
+        for (int i = 1; i <= NX - 1; i++) S.lambsg(k, i) = T(0.5) * (lamb(k, i + 1) + lamb(k, i));
+    for (int k = 1; k <= NZ; k++) S.lambsg(k, NX) = lamb(k, NX);
+    for (int i = 1; i <= NX - 1; i++)
+        for (int k = 1; k <= NZ; k++)
+            S.lambmusg(k, i) = T(0.5) * (lamb(k, i) + T(2) * mu(k, i) + lamb(k, i + 1) + T(2) * mu(k, i + 1));
+    for (int k = 1; k <= NZ; k++) S.lambmusg(k, NX) = lamb(k, NX) + T(2) * mu(k, NX);
+    // YPUB:475-491 rows above itopo take row itopo's values (only the time loop's five arrays
+    // are carried further)
+    for (auto* f : {&S.lambsg, &S.lambmusg, &S.musge, &S.busg1e, &S.busg2e})
+        for (int i = 1; i <= NX; i++)
+            for (int k = itopo; k >= 2; k--) (*f)(k - 1, i) = (*f)(k, i);
+    // YPRI:301-302 modipapml, abc mode only
+    for (auto* f : {&S.lambsg, &S.musge, &S.lambmusg, &S.busg1e, &S.busg2e}) gauss_filter(*f, NX, NZ, c->rgau, itopo, gc);
+    // YPUB:796-849 cosine sponge, R = 1e-3
+    {
+        const T Rr = (T)1.0e-3f;
+        const T fxn = std::acos(Rr) / (T(c->npxn) * S.dx), fxp = std::acos(Rr) / (T(c->npxp) * S.dx);
+        const T fzn = std::acos(Rr) / (T(c->npzn) * S.dz), fzp = std::acos(Rr) / (T(c->npzp) * S.dz);
+        S.spgxn.resize(c->npxn + 1); S.spg1xn.resize(c->npxn + 1);
+        S.spgzn.resize(c->npzn + 1); S.spg1zn.resize(c->npzn + 1);
+        S.spgxp.resize(c->npxp + 1); S.spg2xp.resize(c->npxp + 1);
+        S.spgzp.resize(c->npzp + 1); S.spg2zp.resize(c->npzp + 1);
+        for (int i = 1; i <= c->npxn + 1; i++) {
+            S.spgxn[i - 1] = std::cos(fxn * T(c->npxn - i + 1) * S.dx);
+            S.spg1xn[i - 1] = (i == c->npxn + 1) ? T(1) : std::cos(fxn * (T(c->npxn - i + 1) * S.dx - S.dx / 2));
+        }
+        for (int i = 1; i <= c->npzn + 1; i++) {
+            S.spgzn[i - 1] = std::cos(fzn * T(c->npzn - i + 1) * S.dz);
+            S.spg1zn[i - 1] = (i == c->npzn + 1) ? T(1) : std::cos(fzn * (T(c->npzn - i + 1) * S.dz - S.dz / 2));
+        }
+        for (int i = 1; i <= c->npxp + 1; i++) {
+            S.spgxp[i - 1] = std::cos(fxp * T(c->npxp - i + 1) * S.dx);
+            S.spg2xp[i - 1] = std::cos(fxp * (T(c->npxp - i + 1) * S.dx + S.dx / 2));
+        }
+        for (int i = 1; i <= c->npzp + 1; i++) {
+            S.spgzp[i - 1] = std::cos(fzp * T(c->npzp - i + 1) * S.dz);
+            S.spg2zp[i - 1] = std::cos(fzp * (T(c->npzp - i + 1) * S.dz + S.dz / 2));
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+int run_iso(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const float* rho_in, T* rec1, T* rec2,
+            T* final_vx) {
+    IsoSolver<T> S;
+    Field<T> gc;
+    const int rc = prepare(c, vp_in, vs_in, rho_in, S, gc);
+    if (rc) return rc;
+    const int NX = S.nx, NZ = S.nz, nxe = c->ixmaxe - c->ixmine + 1;
+    const int itopo = c->npzn;
+    const T pi = (T)3.1415926f;
+    // YPUB:1429-1466 addsrc: the (2 rgau - 1)^2 window around the source; cells with an exact zero
+    // weight are left out (adding a zero leaves u unchanged)
+    const int isxe = c->isxe, isze = c->isze;
+    struct Tap { int m, n; T g; };
+    std::vector<Tap> taps;
+    {
+        int idx2 = 1;
+        for (int n = isxe - (c->rgau - 1); n <= isxe + (c->rgau - 1); n++) {
+            int idx1 = 1;
+            for (int m = isze - (c->rgau - 1); m <= isze + (c->rgau - 1); m++) {
+                if (n >= 1 && n <= NX && m >= 1 && m <= NZ && gc(idx1, idx2) != T(0)) taps.push_back({m, n, gc(idx1, idx2)});
+                idx1++;
+            }
+            idx2++;
+        }
+    }
+    int it_cur = 0;
+    const T f0 = c->f0;
+    auto addsrc = [&](Field<T>& u) {
+        const T b = pi * f0 * (T(it_cur) * S.dt - T(c->idecay) * S.dt);
+        const T wav = std::exp(-(b * b)) * (T(1) - T(2) * (b * b));
+        for (const Tap& t : taps) u(t.m, t.n) = wav * t.g * S.dt / (S.dz * S.dz) + u(t.m, t.n);
+    };
+    // YPRI:305-367
+    const int nt = c->nt;
+    const int kr = itopo + c->nrz0;
+    for (int it = 1; it <= nt + c->idecay; it++) {
+        it_cur = it;
+        S.step(addsrc);
+        const int iit = it - c->idecay;
+        if (iit >= 1) {
+            for (int i = 1; i <= nxe; i++) {
+                if (rec1) rec1[(size_t)(i - 1) * nt + (iit - 1)] = S.vx(kr, i + c->npxn);
+                if (rec2) rec2[(size_t)(i - 1) * nt + (iit - 1)] = S.vz(kr, i + c->npxn);
+            }
+        }
+    }
+    if (final_vx)
+        for (int i = 1; i <= NX; i++)
+            for (int k = 1; k <= NZ; k++) final_vx[(size_t)(i - 1) * NZ + (k - 1)] = S.vx(k, i);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_iso_prepare_f32(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, float* out) {
+    IsoSolver<float> S;
+    Field<float> gc;
+    const int rc = prepare(c, vp, vs, rho, S, gc);
+    if (rc) return rc;
+    const size_t n = (size_t)S.nx * S.nz;
+    const Field<float>* arrs[5] = {&S.busg2e, &S.busg1e, &S.lambmusg, &S.lambsg, &S.musge};
+    for (int a = 0; a < 5; a++) std::memcpy(out + a * n, arrs[a]->d.data(), n * sizeof(float));
+    return 0;
+}
+
+int oracle_iso_f32(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, float* rec1, float* rec2,
+                   float* final_vx) {
+    return run_iso<float>(c, vp, vs, rho, rec1, rec2, final_vx);
+}
+
+int oracle_iso_f64(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, double* rec1,
+                   double* rec2, double* final_vx) {
+    return run_iso<double>(c, vp, vs, rho, rec1, rec2, final_vx);
+}
+
+}  // extern "C"

@@ -47,6 +47,27 @@ int oracle_q_f32(const OracleQCfg* c, const float* vp, const float* vs, const fl
                  const float* qs, float* rec1, float* rec2, float* final_sxx);
 int oracle_q_f64(const OracleQCfg* c, const float* vp, const float* vs, const float* rho, const float* qp,
                  const float* qs, double* rec1, double* rec2, double* final_sxx);
+// Isotropic elastic standard staggered grid, 'abc' mode, flat surface (forward/yang_version_2016_2_2,
+// oracle/iso_oracle.cpp).  Interior model (nz, nx) Fortran order = x-major float arrays; cells are
+// 1-based as in the Fortran; records [nxe][nt], record1 = vx, record2 = vz.
+typedef struct {
+    int nx, nz;                    // interior model
+    float dx, dz, dt, f0;
+    int nt;                        // recorded samples (the loop runs nt + idecay steps)
+    int npxn, npxp, npzn, npzp;    // sponge cells, nint(pp/dx) + 1 (YPRI:26-29)
+    int ixmine, ixmaxe;            // window, 0-based model columns (i_ori = i + ixmine)
+    int isxe, isze;                // source cell in the padded window, 1-based
+    int nrz0;                      // receiver row offset below itopo, nint(rz0/dz) + 1
+    int idecay;                    // nint(decay/dt): steps before the first recorded sample
+    int rgau;                      // Gaussian window half-width (2 rgau - 1 cells), the .par's rgau
+} OracleIsoCfg;
+// the five arrays of the time loop after substagger and the PML smoothing (YPUB:323-634):
+// busg2e, busg1e, lambmusg, lambsg, musge, each [NX][NZ] of the padded window
+int oracle_iso_prepare_f32(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, float* out);
+int oracle_iso_f32(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, float* rec1, float* rec2,
+                   float* final_vx);
+int oracle_iso_f64(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, double* rec1,
+                   double* rec2, double* final_vx);
 // 3-D velocity-pressure staggered grid (the AFD scheme with a y axis; no reference counterpart).
 // Arrays are [x][y][z], z fastest; record[r*nt + k] = P after step k's sponge at receiver r.
 typedef struct {

@@ -176,6 +176,45 @@ def q_forward(vp, vs, rho, qp, qs, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz
     return r1, r2, fin
 
 
+class OracleIsoCfg(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int), ("npxn", ctypes.c_int),
+                ("npxp", ctypes.c_int), ("npzn", ctypes.c_int), ("npzp", ctypes.c_int), ("ixmine", ctypes.c_int),
+                ("ixmaxe", ctypes.c_int), ("isxe", ctypes.c_int), ("isze", ctypes.c_int), ("nrz0", ctypes.c_int),
+                ("idecay", ctypes.c_int), ("rgau", ctypes.c_int)]
+
+
+def iso_forward(vp, vs, rho, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz0=1, idecay=0, rgau=50, ixmine=None,
+                ixmaxe=None, fp64=False, want_final=False):
+    """Restated yang_version isotropic elastic modelling, abc mode, flat surface
+    (oracle/iso_oracle.cpp).  Model arrays are the interior (nx, nz) float32 x-major arrays; npx /
+    npz are the sponge cells on both sides (npxn = npxp, npzn = npzp); source and receiver row
+    1-based as in the Fortran.  Returns (record1 = vx, record2 = vz, final vx or None), records
+    [nxe][nt]."""
+    L = lib()
+    if not hasattr(L, "_iso_sig"):
+        tp = ctypes.POINTER(OracleIsoCfg)
+        L.oracle_iso_f32.argtypes = [tp, _F32P, _F32P, _F32P, _F32P, _F32P, _F32P]
+        L.oracle_iso_f64.argtypes = [tp, _F32P, _F32P, _F32P, _F64P, _F64P, _F64P]
+        L._iso_sig = True
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (vp, vs, rho)]
+    nx, nz = arrs[0].shape
+    ixmine = 0 if ixmine is None else ixmine
+    ixmaxe = nx - 1 if ixmaxe is None else ixmaxe
+    nxe = ixmaxe - ixmine + 1
+    cfg = OracleIsoCfg(nx, nz, dx, dz, dt, f0, nt, npx, npx, npz, npz, ixmine, ixmaxe, isxe, isze, nrz0, idecay, rgau)
+    dt_ = np.float64 if fp64 else np.float32
+    tp = _F64P if fp64 else _F32P
+    r1 = np.zeros((nxe, nt), dt_)
+    r2 = np.zeros((nxe, nt), dt_)
+    fin = np.zeros((nxe + 2 * npx, nz + 2 * npz), dt_) if want_final else None
+    fn = L.oracle_iso_f64 if fp64 else L.oracle_iso_f32
+    rc = fn(ctypes.byref(cfg), *[_p(a) for a in arrs], _p(r1, tp), _p(r2, tp), _p(fin, tp))
+    if rc != 0:
+        raise ValueError(f"oracle_iso rejected the configuration (rc={rc})")
+    return r1, r2, fin
+
+
 class OracleAfd3Cfg(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("pml", ctypes.c_int),
                 ("nt", ctypes.c_int), ("radius", ctypes.c_int), ("dx", ctypes.c_float), ("dy", ctypes.c_float),
