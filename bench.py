@@ -383,6 +383,62 @@ def measure_viscoelastic(args, dev):
             "cpu_baseline": cpu}
 
 
+def measure_elastic(args, dev):
+    """Config-3 geometry, isotropic elastic P-SV on the standard staggered grid (the abc mode of
+    forward/yang_version_2016_2_2; vs = vp / 1.8): 16 shots with uneven record lengths in one
+    batched time loop, ten split fields per cell as the reference keeps them.  The model
+    preparation (substagger on the host, the serial top-sponge smoothing on the device) is timed
+    apart.  The CPU figure is the restated step (oracle/iso_oracle.cpp, OpenMP, all host cores)."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.q_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    idecay = int(round(1.2 / c["f0"] / c["dt"]))  # the .par's recommended decay = 1.2 / f0 (s)
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_ISO, nt, c["dt"], c["f0"], delay=idecay))
+             for sx, sz, nt in zip(c["src_x"], c["src_z"], c["nt"])]
+    vs = (c["vp"] / 1.8).astype(np.float32)
+    with S.Engine(S.ELASTIC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"], device=dev) as e:
+        t0 = time.perf_counter()
+        e.set_model_elastic(c["vp"], vs, c["rho"])
+        e.set_shots(shots)
+        prep_s = time.perf_counter() - t0
+        e.forward_device(0)
+        ms = []
+        for _ in range(args.el_steps):
+            e.forward_device(0)
+            t = e.timing()
+            ms.append(t["loop_ms"])
+    pts = float(sum(Nx * Nz * nt for nt in c["nt"]))
+    gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    out = {"workload": f"config 3 geometry, isotropic elastic P-SV standard staggered grid (vs = vp/1.8): "
+                       f"{c['NZ']}x{c['NX']} interior ({Nz}x{Nx} padded), {len(shots)} shots, "
+                       f"nt {min(c['nt'])}-{max(c['nt'])}, Gaussian radius 50",
+           "gpts_per_s": gpts, "shots_per_s": len(shots) / (float(np.median(ms)) / 1e3),
+           "loop_ms": float(np.median(ms)), "launches": t["launches"], "bytes_per_point": 100,
+           "hbm_frac_of_measured": 100 * gpts / read_peaks()[0], "prepare_s": prep_s,
+           "parity": "bit-exact vs FP32 restatement (vx and vz)"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        vp, rho, _ = c["interior"]
+        vsi = (vp / 1.8).astype(np.float32)
+        steps = max(1, args.q_cpu_steps // 2)
+        run = lambda n: ol.iso_forward(vp, vsi, rho, c["dx"], c["dz"], c["dt"], c["f0"], n, c["PML"], c["PML"],
+                                       c["src_x"][0] + 1, c["src_z"][0] + 1, idecay=0)
+        t0 = time.perf_counter()
+        run(1)  # set-up (incl. the serial smoothing) and one step
+        t1 = time.perf_counter()
+        run(1 + steps)
+        wall = (time.perf_counter() - t1) - (t1 - t0)
+        out["cpu_baseline"] = {"value": Nx * Nz * steps / max(wall, 1e-9) / 1e9, "unit": "Gpts/s",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"restated yang_version abc step (oracle/iso_oracle.cpp, OpenMP) on one "
+                                         f"shot: the difference of a {steps + 1}- and a 1-step run ({steps} steps)"}
+    return out
+
+
 def measure_q_gradient(args, dev):
     """Config-3 geometry: the viscoacoustic gradient d misfit / d vp and d misfit / d (1/Q) of 16
     shots (uneven record lengths), observed data from the Q field scaled by 0.8, batched (one
@@ -643,6 +699,8 @@ def run_ours(args, world, rank, local):
         line["viscoacoustic"] = measure_viscoacoustic(args, dev)
     if world == 1 and args.e_steps > 0:
         line["viscoelastic"] = measure_viscoelastic(args, dev)
+    if world == 1 and args.el_steps > 0:
+        line["elastic"] = measure_elastic(args, dev)
     if world == 1 and args.qg_steps > 0:
         line["viscoacoustic_gradient"] = measure_q_gradient(args, dev)
     if world == 1 and args.d3_steps > 0:
@@ -680,6 +738,7 @@ def main():
     ap.add_argument("--d3-nt-scale", type=float, default=0.05)
     ap.add_argument("--d3-cpu-steps", type=int, default=3)
     ap.add_argument("--e-steps", type=int, default=1, help="timed visco-elastic forwards (0 = skip)")
+    ap.add_argument("--el-steps", type=int, default=1, help="timed isotropic elastic forwards (0 = skip)")
     ap.add_argument("--qg-steps", type=int, default=1, help="timed viscoacoustic gradients (0 = skip)")
     ap.add_argument("--qg-nshot", type=int, default=16)
     ap.add_argument("--qg-nt-scale", type=float, default=1.0)

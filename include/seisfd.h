@@ -9,6 +9,7 @@
  *   forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90               (QM)
  *   forward/Q_forward/Q_multishot_fd_subroutine_fsbc_zy_rotated.f90         (QS)
  *   tools/ricker.cpp                                                        (RIC)
+ *   forward/yang_version_2016_2_2/Iso_multishot_fd_subroutine_fsbc_zy_m2_{pub,pri}.f90 (YPUB, YPRI)
  *
  * Conventions (the reference's in-memory and file layouts):
  *   - grids are x-major with z fastest: a[x * nz + z] (AFD:51-100 `P[i][j]`, i = x, j = z;
@@ -51,6 +52,10 @@ extern "C" {
 #define SFD_ACOUSTIC_3D 2  /* 3-D velocity-pressure staggered grid (no reference counterpart) */
 #define SFD_VISCOEL_2D 3   /* rotated staggered grid, P-SV visco-elastic with 1 SLS per stress
                               (vs > 0): QS:695-1337, the full Q_forward scheme              */
+#define SFD_ELASTIC_2D 4   /* standard staggered grid, isotropic elastic P-SV, 10th order,
+                              cosine sponge on four sides with the top sponge's moduli
+                              Gaussian-smoothed: the 'abc' mode of forward/yang_version_2016_2_2
+                              (YPRI:234-386), flat surface                                  */
 
 /* ---- flags (sfd_grid.flags) ---- */
 #define SFD_EXACT 0x1      /* reference operation order: every multiply and add rounded
@@ -62,6 +67,8 @@ extern "C" {
 #define SFD_WAVELET_RIC 1  /* RIC:44: (1-2a^2)exp(-a^2), a = pi f0 (j-delay) dt, f0 integer  */
 #define SFD_WAVELET_Q 2    /* QS:1376 (single precision): exp(-b^2)(1-2b^2),
                               b = pi f0 (it dt - 1.2/f0), it = j+1                           */
+#define SFD_WAVELET_ISO 3  /* YPUB:1447-1448 (single precision): exp(-b^2)(1-2b^2),
+                              b = pi f0 (it dt - delay dt), it = j+1, delay = nint(decay/dt) */
 
 /* ---- wavefield selectors (sfd_get_wavefield) ---- */
 #define SFD_FIELD_P 0      /* pressure (AFD P1) / stress sigma (QS strxx)                   */
@@ -69,8 +76,8 @@ extern "C" {
 #define SFD_FIELD_VZ 2
 #define SFD_FIELD_VY 3
 #define SFD_FIELD_R 4      /* memory variable r (QS rxx)                                     */
-#define SFD_FIELD_SZZ 5    /* QS strzz (visco-elastic; equals strxx when vs = 0)             */
-#define SFD_FIELD_SXZ 6    /* QS strxz (visco-elastic)                                       */
+#define SFD_FIELD_SZZ 5    /* QS / YPUB strzz (elastic schemes; equals strxx when vs = 0)   */
+#define SFD_FIELD_SXZ 6    /* QS / YPUB strxz (elastic schemes)                              */
 
 typedef struct sfd_ctx sfd_ctx;
 
@@ -129,9 +136,17 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
 
 /* Visco-elastic model (SFD_VISCOEL_2D): P and S velocities, density and the P and S quality
  * factors on the padded grid.  Replaces QS:238-284 (read_data of vp, vs, rho, qfp, qfs) and
- * QS:434-551 (substagger, pcalpas).  den NULL = 2400 kg/m^3; qp / qs NULL = 1e5 (QM:418-419). */
+ * QS:434-551 (substagger, pcalpas).  den NULL = 2400 kg/m^3; qp / qs NULL = 1e5 (QM:418-419).
+ * Elastic model (SFD_ELASTIC_2D): vp, vs, den; qp and qs must be NULL.  Replaces YPUB:148-184
+ * (read_data) and YPUB:323-634 (substagger, then modipapml: the moduli and buoyancies of the top
+ * sponge rows z < pml smoothed in place with the Gaussian of sfd_set_gauss_radius). */
 int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const float* den, const float* qp,
                           const float* qs);
+
+/* Half-width rgau of the Gaussian (sigma 2 cells, window 2 rgau - 1 cells) that spreads the
+ * source and smooths the top sponge of SFD_ELASTIC_2D (YPUB:1470-1501, the .par's "rad of gauss
+ * smooth"; default 50).  Re-prepares the model and the source stamps if they are set. */
+int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau);
 
 /* Shots.  Replaces the shot loop QM:124-141 (one launch for all shots instead of one process
  * per shot).  Wavelets and receiver lists are copied; the caller keeps ownership. */
@@ -145,10 +160,11 @@ int sfd_forward(sfd_ctx* ctx, float* records);
 /* Same, with the records left in device memory (caller-owned, same layout) and no host copy. */
 int sfd_forward_device(sfd_ctx* ctx, float* records_dev);
 
-/* Records of one stress component from the last forward, in the sfd_forward layout.  The
+/* Records of one component from the last forward, in the sfd_forward layout.  The
  * Q_forward programs record two (QM:452-459): record1 = strzz (SFD_FIELD_SZZ, what sfd_forward
  * returns for the viscoacoustic and visco-elastic schemes) and record2 = strxx (SFD_FIELD_P).
- * For SFD_VISCOAC_2D both are the same sigma. */
+ * For SFD_VISCOAC_2D both are the same sigma.  SFD_ELASTIC_2D records vx (record1,
+ * SFD_FIELD_VX, what sfd_forward returns) and vz (record2, SFD_FIELD_VZ), YPRI:361-367. */
 int sfd_get_records(sfd_ctx* ctx, int field, float* records);
 
 /* Plain per-shot path: shots one after another, one kernel launch per time step each, no
@@ -216,8 +232,8 @@ int sfd_forward_noalloc(const sfd_grid* grid, const float* vp_dev, const float* 
                         void* stream);
 
 /* Host helpers (no context). */
-/* Source wavelet in one of the reference's three conventions (AFD:199-209, RIC:44, QS:1376).
- * delay: RIC only, in samples (RIC uses 150). */
+/* Source wavelet in one of the reference's conventions (AFD:199-209, RIC:44, QS:1376,
+ * YPUB:1447-1448).  delay: in samples, RIC (RIC uses 150) and ISO (idecay) only. */
 int sfd_wavelet(int convention, int nt, float dt, float f0, int delay, float* out);
 /* AFD sponge factors absorb[x][z] (AFD:164-194; bottom loop bound j < Nz, see AFD:190). */
 int sfd_afd_sponge(int nx, int nz, int pml, float* absorb);

@@ -162,8 +162,8 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     if (S.nx < 12 || S.nz < 12) return 1;
     S.alloc();
     const int NX = S.nx, NZ = S.nz;
-    const int itopo = c->npzn;  // flat surface: nint(0/dz) + npzn (YPUB:306-308)
-    // YPUB:210-258 window and edge padding
+    const int itopo = c->npzn;  // flat surface: nint(0/dz) + npzn (YPUB:271)
+    // YPUB:210-266 window and edge padding
     Field<T> vpe(1, NZ, 1, NX), vse(1, NZ, 1, NX), rhoe(1, NZ, 1, NX);
     auto in = [&](const float* m, int k, int i) { return (T)m[(size_t)(i - 1) * nz_m + (k - 1)]; };
     for (int i = 1; i <= nxe; i++) {
@@ -219,7 +219,7 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     for (int k = 1; k <= NZ; k++) busg1(k, NX) = busg1(k, NX - 1);
     for (int i = 1; i <= NX; i++)
         for (int k = 1; k <= NZ; k++) {
-            if (busg1(k, i) == T(0)) return 2;  // YPUB:371 stops here
+            if (busg1(k, i) == T(0)) return 2;  // YPUB:370 stops here
             busg1(k, i) = T(1.0) / busg1(k, i);
         }
     for (int i = 1; i <= NX; i++)
@@ -253,7 +253,7 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
         for (int k = 1; k <= NZ; k++)
             S.lambmusg(k, i) = T(0.5) * (lamb(k, i) + T(2) * mu(k, i) + lamb(k, i + 1) + T(2) * mu(k, i + 1));
     for (int k = 1; k <= NZ; k++) S.lambmusg(k, NX) = lamb(k, NX) + T(2) * mu(k, NX);
-    // YPUB:475-491 rows above itopo take row itopo's values (only the time loop's five arrays
+    // YPUB:484-501 rows above itopo take row itopo's values (only the time loop's five arrays
     // are carried further)
     for (auto* f : {&S.lambsg, &S.lambmusg, &S.musge, &S.busg1e, &S.busg2e})
         for (int i = 1; i <= NX; i++)

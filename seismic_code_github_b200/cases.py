@@ -7,6 +7,7 @@
     python -m seismic_code_github_b200.cases qgradient --nshot 4 --nt 100
     python -m seismic_code_github_b200.cases gradient3d --n 384 --nshot 2 --nt 6
     python -m seismic_code_github_b200.cases viscoel --nshot 4 --nt 60
+    python -m seismic_code_github_b200.cases elastic --nshot 4 --nt 60
 
 Each run builds a seeded synthetic model, runs one warm-up call and one timed call of the
 batched path and prints the engine's timing record.  Sizes are chosen on the command line so
@@ -63,6 +64,21 @@ def viscoel(args):
     with S.Engine(S.VISCOEL_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
         e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"], c["q"],
                             (0.7 * c["q"]).astype(np.float32))
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def elastic(args):
+    c = W.config3(nshot=args.nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_ISO, args.nt, c["dt"], c["f0"], delay=args.nt // 2))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.ELASTIC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"])
         e.set_shots(shots)
         e.forward_device(0)
         e.forward_device(0)
@@ -137,13 +153,13 @@ def gradient3d(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient", "forward2d", "qgradient", "gradient3d",
-                                     "viscoel"])
+                                     "viscoel", "elastic"])
     ap.add_argument("--n", type=int, default=384, help="3-D padded grid size per axis")
     ap.add_argument("--nshot", type=int, default=2)
     ap.add_argument("--nt", type=int, default=3)
     args = ap.parse_args()
     cases = {"acoustic3d": acoustic3d, "viscoac": viscoac, "gradient": gradient, "forward2d": forward2d,
-             "qgradient": qgradient, "gradient3d": gradient3d, "viscoel": viscoel}
+             "qgradient": qgradient, "gradient3d": gradient3d, "viscoel": viscoel, "elastic": elastic}
     t = cases[args.case](args)
     print(json.dumps(t))
 

@@ -115,6 +115,17 @@ struct sfd_ctx {
     float* d_rec2_nt = nullptr;     // ... trace-major
     bool rec2_ready = false;
     bool elastic_call = false;      // sfd_set_model is running on behalf of sfd_set_model_elastic
+    // isotropic elastic scheme (yang_version): Gaussian half-width, its table and non-zero range;
+    // the prepared model lives in e_q[0..4] (busg2e, busg1e, lambmusg, lambsg, musge)
+    int iso_rgau = 50;
+    std::vector<float> iso_gc;
+    int iso_lo = 0, iso_hi = -1;
+    long long model_gen = 0;        // bumped by every sfd_set_model
+    // what the prepared model was built from (windows, model generation, rgau): a call with the
+    // same inputs only re-targets the shots at the existing blocks
+    std::vector<std::pair<int, int>> prep_wins;
+    long long prep_gen = -1;
+    int prep_rgau = -1;
 
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
@@ -436,6 +447,41 @@ EArgs make_eargs(const sfd_ctx* c, int step) {
     return a;
 }
 
+// Arguments of the isotropic elastic step (ten in-place split fields per shot).
+IArgs make_iargs(const sfd_ctx* c, int step) {
+    IArgs a{};
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    for (int i = 0; i < I_NFIELDS; i++) a.f[i] = c->d_state + i * fs;
+    a.L = c->L;
+    a.nz = c->g.nz;
+    a.npx = a.npz = c->g.pml;
+    a.b2e = c->e_q[0] + kModelGhostZ; a.b1e = c->e_q[1] + kModelGhostZ; a.lm2 = c->e_q[2] + kModelGhostZ;
+    a.lam = c->e_q[3] + kModelGhostZ; a.mue = c->e_q[4] + kModelGhostZ;
+    a.mpitch = c->mpitch;
+    a.nx_model = c->q_width;
+    a.dt = c->g.dt;
+    a.dtdx = c->g.dt / c->g.dx;  // YPUB:1113 (dt/dx)
+    a.dtdz = c->g.dt / c->g.dz;
+    a.dz2 = c->g.dz * c->g.dz;
+    const float af[5] = {19845.0f / 16384.0f, -735.0f / 8192.0f, 567.0f / 40960.0f, -405.0f / 229376.0f,
+                         35.0f / 294912.0f};  // YMOD:23-27
+    std::memcpy(a.a, af, sizeof(af));
+    a.spg = c->d_spg;
+    a.spg_stride = c->spg_stride;
+    a.shots = c->d_shots;
+    a.slot_to_shot = c->d_slot;
+    a.wavelets = c->d_wav;
+    a.stamps = c->d_stamps;
+    a.rec_x = c->d_rec_x;
+    a.rec_z = c->d_rec_z;
+    a.tile_rec_ptr = c->d_trp;
+    a.tile_rec_idx = c->d_tri;
+    a.records = c->d_rec_tn;
+    a.records2 = c->d_rec2_tn;
+    a.step = step;
+    return a;
+}
+
 // Size the snapshot buffers for the current shot set; returns true if a buffer moved (the
 // captured time loop holds their addresses).
 bool snap_prepare(sfd_ctx* ctx, int* rc) {
@@ -489,6 +535,17 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
             const int f0 = sn.field == SFD_FIELD_VX ? 0 : sn.field == SFD_FIELD_VZ ? 1 : sn.field == SFD_FIELD_P ? 2 : 5;
             s.nsum = (sn.field == SFD_FIELD_P || sn.field == SFD_FIELD_R) ? 3 : 1;
             for (int i = 0; i < s.nsum; i++) s.f[i] = F + (f0 + i) * fs;
+        } else if (ctx->g.scheme == SFD_ELASTIC_2D) {
+            int f0;  // first of the field's two split parts
+            switch (sn.field) {
+            case SFD_FIELD_VX: f0 = I_VXX; break;
+            case SFD_FIELD_VZ: f0 = I_VZX; break;
+            case SFD_FIELD_P: f0 = I_SXXX; break;
+            case SFD_FIELD_SZZ: f0 = I_SZZX; break;
+            default: f0 = I_SXZX; break;
+            }
+            s.nsum = 2;
+            for (int i = 0; i < 2; i++) s.f[i] = F + (f0 + i) * fs;
         } else if (ctx->g.scheme == SFD_VISCOEL_2D) {
             int f0;  // first split part; velocities have two, stresses and memory variables three
             switch (sn.field) {
@@ -541,6 +598,13 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         QArgs q = make_qargs(ctx, k);
         q.slot_to_shot = slots;
         CK(viscoac2d_launch_step(q, act, ctx->stream));
+        *launches += 2;
+        return SFD_OK;
+    }
+    if (ctx->g.scheme == SFD_ELASTIC_2D) {
+        IArgs e = make_iargs(ctx, k);
+        e.slot_to_shot = slots;
+        CK(elastic2d_launch_step(e, act, ctx->stream));
         *launches += 2;
         return SFD_OK;
     }
@@ -655,6 +719,7 @@ int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
     if (ctx->g.scheme == SFD_VISCOAC_2D) return 40;
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
+    if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
     return (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
 }
 
@@ -1123,7 +1188,8 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
 // Without shots the whole grid is one window.
 int q_prepare(sfd_ctx* ctx) {
     const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
-    if ((ctx->g.scheme != SFD_VISCOAC_2D && !elastic) || !ctx->have_model) return SFD_OK;
+    const bool iso = ctx->g.scheme == SFD_ELASTIC_2D;
+    if ((ctx->g.scheme != SFD_VISCOAC_2D && !elastic && !iso) || !ctx->have_model) return SFD_OK;
     const int nz = ctx->g.nz;
     std::vector<std::pair<int, int>> wins;  // (x0, nx)
     std::vector<int> blk(ctx->have_shots ? ctx->nshot : 0);
@@ -1143,15 +1209,30 @@ int q_prepare(sfd_ctx* ctx) {
         start[b] = width;
         width += wins[b].second;
     }
+    if (iso && wins == ctx->prep_wins && ctx->model_gen == ctx->prep_gen && ctx->iso_rgau == ctx->prep_rgau &&
+        width == ctx->q_width) {
+        if (ctx->have_shots) {
+            for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
+            CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
+        }
+        return SFD_OK;
+    }
     std::vector<float> busg((size_t)width * nz), p1((size_t)width * nz), p2((size_t)width * nz);
-    std::vector<std::vector<float>> eq(elastic ? 6 : 0, std::vector<float>((size_t)width * nz));
+    std::vector<std::vector<float>> eq(elastic ? 6 : iso ? 5 : 0, std::vector<float>((size_t)width * nz));
     for (size_t b = 0; b < wins.size(); b++) {
         const size_t off = (size_t)wins[b].first * nz, len = (size_t)wins[b].second * nz;
         std::vector<float> rho(len, ctx->den_c);
         if (!ctx->h_den.empty()) rho.assign(ctx->h_den.begin() + off, ctx->h_den.begin() + off + len);
         const float* qw = ctx->h_q.empty() ? nullptr : ctx->h_q.data() + off;
         const size_t o = (size_t)start[b] * nz;
-        if (elastic) {
+        if (iso) {  // YPUB:323-547 per window, flat surface: itopo = npzn = pml
+            std::vector<float> vs(len, 0.0f);
+            if (!ctx->h_vs.empty()) vs.assign(ctx->h_vs.begin() + off, ctx->h_vs.begin() + off + len);
+            if (!elastic2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(), ctx->g.pml,
+                                   eq[0].data() + o, eq[1].data() + o, eq[2].data() + o, eq[3].data() + o,
+                                   eq[4].data() + o))
+                return set_err(ctx, SFD_ERR_ARG, "zero density in the window at column %d", wins[b].first);
+        } else if (elastic) {
             std::vector<float> vs(len, 0.0f);
             if (!ctx->h_vs.empty()) vs.assign(ctx->h_vs.begin() + off, ctx->h_vs.begin() + off + len);
             const float* qsw = ctx->h_qs.empty() ? nullptr : ctx->h_qs.data() + off;
@@ -1179,19 +1260,64 @@ int q_prepare(sfd_ctx* ctx) {
         return SFD_OK;
     };
     int rc;
-    if ((rc = upload(&ctx->q_busg, busg))) return rc;
+    if (iso) {
+        for (int i = 0; i < 5; i++)
+            if ((rc = upload(&ctx->e_q[i], eq[i]))) return rc;
+        // YPUB:549-634 modipapml on the device: rows z < pml of the five arrays, per window
+        std::vector<int> win(2 * wins.size());
+        for (size_t b = 0; b < wins.size(); b++) {
+            win[2 * b] = start[b];
+            win[2 * b + 1] = wins[b].second;
+        }
+        float* arrs[5];
+        for (int i = 0; i < 5; i++) arrs[i] = ctx->e_q[i] + kModelGhostZ;
+        CK(elastic2d_smooth(arrs, ctx->mpitch, kModelGhostZ, nz, ctx->g.pml, win.data(), (int)wins.size(),
+                            ctx->iso_gc, ctx->iso_rgau, ctx->iso_lo, ctx->iso_hi, ctx->stream));
+    } else if ((rc = upload(&ctx->q_busg, busg))) {
+        return rc;
+    }
     if (elastic) {
         for (int i = 0; i < 6; i++)
             if ((rc = upload(&ctx->e_q[i], eq[i]))) return rc;
-    } else if ((rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2))) {
+    } else if (!iso && ((rc = upload(&ctx->q_p1, p1)) || (rc = upload(&ctx->q_p2, p2)))) {
         return rc;
     }
     if (width != ctx->q_width) ctx->graph_valid = ctx->grad_valid = false;
     ctx->q_width = width;
+    ctx->prep_wins = wins;
+    ctx->prep_gen = ctx->model_gen;
+    ctx->prep_rgau = ctx->iso_rgau;
     if (ctx->have_shots) {
         for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
         CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
     }
+    return SFD_OK;
+}
+
+// Gaussian source stamps of the current shots (QS:1340-1444; YPUB:1429-1466 with the context's
+// rgau), uploaded with the shot descriptors.
+int build_stamps(sfd_ctx* ctx) {
+    const int nz = ctx->g.nz;
+    std::vector<float> stamps;
+    for (int s = 0; s < ctx->nshot; s++) {
+        int box[4];
+        ShotDev& d = ctx->h_shots[s];
+        d.stamp_off = (int)stamps.size();
+        if (ctx->g.scheme == SFD_ELASTIC_2D)
+            elastic2d_stamp(d.nx, nz, d.sx, d.sz, ctx->iso_rgau, ctx->iso_gc, box, &stamps);
+        else
+            viscoac2d_stamp(d.nx, nz, d.sx, d.sz, box, &stamps);
+        d.stamp_x0 = box[0];
+        d.stamp_z0 = box[1];
+        d.stamp_w = box[2];
+        d.stamp_h = box[3];
+    }
+    dfree(ctx->d_stamps);
+    CK(cudaMalloc(&ctx->d_stamps, sizeof(float) * std::max<size_t>(1, stamps.size())));
+    if (!stamps.empty())
+        CK(cudaMemcpy(ctx->d_stamps, stamps.data(), sizeof(float) * stamps.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
+    ctx->graph_valid = false;
     return SFD_OK;
 }
 
@@ -1672,7 +1798,7 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
     if (!g || !out) return SFD_ERR_ARG;
     *out = nullptr;
     if (g->scheme != SFD_ACOUSTIC_2D && g->scheme != SFD_VISCOAC_2D && g->scheme != SFD_ACOUSTIC_3D &&
-        g->scheme != SFD_VISCOEL_2D)
+        g->scheme != SFD_VISCOEL_2D && g->scheme != SFD_ELASTIC_2D)
         return SFD_ERR_ARG;
     const bool is3d = g->scheme == SFD_ACOUSTIC_3D;
     if (g->nx <= 0 || g->nz <= 0 || (is3d ? g->ny <= 0 : g->ny > 1)) return SFD_ERR_ARG;
@@ -1711,6 +1837,17 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
         c->plan.gz = 8;  // RSG halo 5, rounded for float4 staging
         c->plan.stages = 1;
     }
+    if (g->scheme == SFD_ELASTIC_2D) {
+        // the staggered grid of yang_version is 10th order only (a100..a104, YMOD:23-27)
+        if (g->order != 10) return set_err(ctx, SFD_ERR_UNSUPPORTED, "the yang_version scheme is 10th order");
+        if (g->pml < 1) return set_err(ctx, SFD_ERR_ARG, "the yang_version sponge needs pml >= 1 (YPRI:26-29)");
+        c->plan.radius = 5;
+        c->plan.tx = kTileX;
+        c->plan.tz = kTileZ;
+        c->plan.gz = 8;  // staggered reach 5, rounded for float4 staging
+        c->plan.stages = 1;
+        elastic2d_gauss_table(c->iso_rgau, &c->iso_gc, &c->iso_lo, &c->iso_hi);
+    }
     if (g->scheme == SFD_ACOUSTIC_3D) {
         int b0[2], b1[2], b2[2];
         if (!acoustic3d_boxes(R, b0, b1, b2))
@@ -1738,6 +1875,7 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
             if (!(den[i] > 0.0f) || !std::isfinite(den[i]))
                 return set_err(ctx, SFD_ERR_ARG, "den[%zu] = %g is not a positive finite density", i, (double)den[i]);
     CK(cudaSetDevice(ctx->device));
+    ctx->model_gen++;
     ctx->h_vp.assign(vp, vp + n);
     ctx->varden = false;
     ctx->den_c = 2400.0f;
@@ -1784,6 +1922,13 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     } else {
         dfree(ctx->d_den);
     }
+    if (ctx->g.scheme == SFD_ELASTIC_2D) {
+        // YPUB:323-634 per shot window: staggered moduli and buoyancies, smoothed top sponge
+        if (q) return set_err(ctx, SFD_ERR_ARG, "the yang_version scheme has no quality factor");
+        if (!ctx->elastic_call) ctx->h_vs.clear();  // no S waves: vs = 0
+        ctx->have_model = true;
+        if ((urc = q_prepare(ctx))) return urc;
+    }
     if (ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D) {
         // QS:434-551 on the padded grid: averaged density -> buoyancy, Lame and Blanch tau
         if (q)
@@ -1806,7 +1951,8 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
     }
     ctx->have_model = true;
     // source scale factors depend on the model (the viscoacoustic source is a stamp)
-    if (ctx->have_shots && ctx->g.scheme != SFD_VISCOAC_2D && ctx->g.scheme != SFD_VISCOEL_2D) {
+    if (ctx->have_shots && ctx->g.scheme != SFD_VISCOAC_2D && ctx->g.scheme != SFD_VISCOEL_2D &&
+        ctx->g.scheme != SFD_ELASTIC_2D) {
         for (auto& s : ctx->h_shots) {
             const size_t mi = ((size_t)(s.x0 + s.sx) * ctx->g.ny + s.sy) * ctx->g.nz + s.sz;
             const float d = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
@@ -1822,8 +1968,10 @@ int sfd_set_model(sfd_ctx* ctx, const float* vp, const float* den, const float* 
 int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const float* den, const float* qp,
                           const float* qs) {
     if (!ctx || !vp || !vs) return SFD_ERR_ARG;
-    if (ctx->g.scheme != SFD_VISCOEL_2D)
-        return set_err(ctx, SFD_ERR_ARG, "sfd_set_model_elastic applies to SFD_VISCOEL_2D");
+    if (ctx->g.scheme != SFD_VISCOEL_2D && ctx->g.scheme != SFD_ELASTIC_2D)
+        return set_err(ctx, SFD_ERR_ARG, "sfd_set_model_elastic applies to SFD_VISCOEL_2D and SFD_ELASTIC_2D");
+    if (ctx->g.scheme == SFD_ELASTIC_2D && (qp || qs))
+        return set_err(ctx, SFD_ERR_ARG, "the yang_version scheme has no quality factors");
     const size_t n = (size_t)ctx->g.nx * ctx->g.nz;
     for (size_t i = 0; i < n; i++)
         if (!(vs[i] >= 0.0f) || !std::isfinite(vs[i]))
@@ -1846,7 +1994,9 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     if (!ctx || nshot <= 0 || !shots) return SFD_ERR_ARG;
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return set_shots_3d(ctx, nshot, shots);
     const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
-    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D || elastic;  // the Q_forward schemes
+    const bool iso = ctx->g.scheme == SFD_ELASTIC_2D;
+    // the Fortran schemes: in-place split fields, Gaussian source stamps, split cosine sponge
+    const bool visco = ctx->g.scheme == SFD_VISCOAC_2D || elastic || iso;
     if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d is not implemented", ctx->g.scheme);
     CK(cudaSetDevice(ctx->device));
@@ -1961,30 +2111,21 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
     CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));
     CK(cudaMalloc(&ctx->d_rec_nt, rec_bytes));
-    if (elastic) {
+    if (elastic || iso) {
         CK(cudaMalloc(&ctx->d_rec2_tn, rec_bytes));
         CK(cudaMalloc(&ctx->d_rec2_nt, rec_bytes));
     }
-    ctx->state_floats = (elastic ? E_NFIELDS : visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
+    ctx->state_floats = (iso ? I_NFIELDS : elastic ? E_NFIELDS : visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
     CK(cudaMalloc(&ctx->d_src_pre, sizeof(float) * nshot));
     if (visco) {
-        // Gaussian source stamps (QS:1340-1444) and the split cosine sponge tables (QS:555-605)
-        std::vector<float> stamps;
-        for (int s = 0; s < nshot; s++) {
-            int box[4];
-            ctx->h_shots[s].stamp_off = (int)stamps.size();
-            viscoac2d_stamp(ctx->h_shots[s].nx, nz, ctx->h_shots[s].sx, ctx->h_shots[s].sz, box, &stamps);
-            ctx->h_shots[s].stamp_x0 = box[0];
-            ctx->h_shots[s].stamp_z0 = box[1];
-            ctx->h_shots[s].stamp_w = box[2];
-            ctx->h_shots[s].stamp_h = box[3];
-        }
-        if ((rc = up(&ctx->d_stamps, stamps))) return rc;
-        CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * nshot, cudaMemcpyHostToDevice));
+        // Gaussian source stamps (QS:1340-1444, YPUB:1429-1466) and the split cosine sponge tables
+        // (QS:555-605, YPUB:796-849)
+        if ((rc = build_stamps(ctx))) return rc;
         ctx->spg_stride = ctx->g.pml + 1;
         std::vector<float> tab(8 * (size_t)ctx->spg_stride);
-        viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
+        if (iso) elastic2d_sponge_tables(ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
+        else viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
         dfree(ctx->d_spg);
         if ((rc = up(&ctx->d_spg, tab))) return rc;
     } else {
@@ -2123,12 +2264,21 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         for (size_t i = 0; i < n; i++) out[i] = (a[i] + b[i]) + c[i];
         return SFD_OK;
     }
-    if (ctx->g.scheme == SFD_VISCOEL_2D) {
-        // sums of the split parts in the reference's order (QS:1273-1337)
+    if (ctx->g.scheme == SFD_VISCOEL_2D || ctx->g.scheme == SFD_ELASTIC_2D) {
+        // sums of the split parts in the reference's order (QS:1273-1337, YPUB:1410-1426)
         const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
         const int nz = ctx->g.nz;
+        const bool iso = ctx->g.scheme == SFD_ELASTIC_2D;
         int f0;
-        switch (field) {
+        if (iso) switch (field) {
+        case SFD_FIELD_VX: f0 = I_VXX; break;
+        case SFD_FIELD_VZ: f0 = I_VZX; break;
+        case SFD_FIELD_P: f0 = I_SXXX; break;
+        case SFD_FIELD_SZZ: f0 = I_SZZX; break;
+        case SFD_FIELD_SXZ: f0 = I_SXZX; break;
+        default: return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+        }
+        else switch (field) {
         case SFD_FIELD_VX: f0 = E_VXX; break;
         case SFD_FIELD_VZ: f0 = E_VZX; break;
         case SFD_FIELD_P: f0 = E_SXXX; break;
@@ -2137,7 +2287,7 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         case SFD_FIELD_R: f0 = E_RXXX; break;
         default: return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
         }
-        const int np = f0 < E_SXXX ? 2 : 3;
+        const int np = (iso || f0 < E_SXXX) ? 2 : 3;
         const size_t n = (size_t)sd.nx * nz;
         std::vector<float> part(n);
         for (int i = 0; i < np; i++) {
@@ -2167,6 +2317,19 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         for (size_t i = 0; i < a.size(); i++) out[i] = out[i] * a[i];
     }
     return SFD_OK;
+}
+
+int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau) {
+    if (!ctx || rgau < 1 || rgau > 4096) return SFD_ERR_ARG;
+    if (ctx->g.scheme != SFD_ELASTIC_2D)
+        return set_err(ctx, SFD_ERR_ARG, "the Gaussian radius applies to SFD_ELASTIC_2D");
+    if (rgau == ctx->iso_rgau) return SFD_OK;
+    CK(cudaSetDevice(ctx->device));
+    ctx->iso_rgau = rgau;
+    elastic2d_gauss_table(rgau, &ctx->iso_gc, &ctx->iso_lo, &ctx->iso_hi);
+    int rc;
+    if (ctx->have_shots && (rc = build_stamps(ctx))) return rc;
+    return q_prepare(ctx);  // the top sponge's smoothing (no-op without a model)
 }
 
 int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes) {
@@ -2207,7 +2370,7 @@ int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int
     if (ctx->g.scheme == SFD_ACOUSTIC_3D && count > 0)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "snapshots are taken for the 2-D schemes");
     const bool visco = ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D;
-    const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D;
+    const bool elastic = ctx->g.scheme == SFD_VISCOEL_2D || ctx->g.scheme == SFD_ELASTIC_2D;
     if (count > 0 && field != SFD_FIELD_P && field != SFD_FIELD_VX && field != SFD_FIELD_VZ &&
         !(visco && field == SFD_FIELD_R) && !(elastic && (field == SFD_FIELD_SZZ || field == SFD_FIELD_SXZ)))
         return set_err(ctx, SFD_ERR_ARG, "field %d cannot be recorded for this scheme", field);
@@ -2225,12 +2388,14 @@ int sfd_get_records(sfd_ctx* ctx, int field, float* records) {
     if (!ctx || !records) return SFD_ERR_ARG;
     if (!ctx->have_shots) return set_err(ctx, SFD_ERR_STATE, "no shots");
     const bool q = ctx->g.scheme == SFD_VISCOAC_2D || ctx->g.scheme == SFD_VISCOEL_2D;
-    if (!q || (field != SFD_FIELD_SZZ && field != SFD_FIELD_P))
+    const bool iso = ctx->g.scheme == SFD_ELASTIC_2D;
+    if (!(q && (field == SFD_FIELD_SZZ || field == SFD_FIELD_P)) && !(iso && (field == SFD_FIELD_VX || field == SFD_FIELD_VZ)))
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "records of field %d are not recorded for this scheme", field);
     CK(cudaSetDevice(ctx->device));
-    // the time-major records of the last forward, transposed to the output layout: strzz, or
-    // strxx, which only the visco-elastic scheme keeps apart (for vs = 0 both are sigma)
-    const bool sxx = field == SFD_FIELD_P && ctx->g.scheme == SFD_VISCOEL_2D;
+    // the time-major records of the last forward, transposed to the output layout: record1
+    // (strzz; vx for the yang_version scheme) or record2 (strxx, which only the visco-elastic
+    // scheme keeps apart -- for vs = 0 both are sigma; vz for the yang_version scheme)
+    const bool sxx = (field == SFD_FIELD_P && ctx->g.scheme == SFD_VISCOEL_2D) || (iso && field == SFD_FIELD_VZ);
     if (sxx && !ctx->rec2_ready) return set_err(ctx, SFD_ERR_STATE, "no forward has run");
     float* tn = sxx ? ctx->d_rec2_tn : ctx->d_rec_tn;
     float* nt = sxx ? ctx->d_rec2_nt : ctx->d_rec_nt;

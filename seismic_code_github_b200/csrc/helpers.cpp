@@ -84,6 +84,16 @@ int sfd_wavelet(int convention, int nt, float dt, float f0, int delay, float* ou
         }
         return SFD_OK;
     }
+    if (convention == SFD_WAVELET_ISO) {
+        // YPUB:1447-1448, Fortran default reals: it*dt - idecay*dt in single precision, it = 1..nt
+        if (delay < 0) return SFD_ERR_ARG;
+        const float pi = 3.1415926f;
+        for (int j = 0; j < nt; j++) {
+            const float b = pi * f0 * ((float)(j + 1) * dt - (float)delay * dt);
+            out[j] = std::exp(-(b * b)) * (1.0f - 2.0f * (b * b));
+        }
+        return SFD_OK;
+    }
     return SFD_ERR_ARG;
 }
 

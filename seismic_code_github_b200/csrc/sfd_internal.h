@@ -112,6 +112,56 @@ void viscoel2d_prepare(int nx, int nz, const float* vp, const float* vs, const f
                        const float* qs, float f0, float* busg, float* q1, float* q2, float* q3, float* m1, float* m2,
                        float* m3, float* rtau_out);
 
+// Isotropic elastic standard-staggered-grid split fields (elastic2d.cu), in slab order:
+// forward/yang_version_2016_2_2 vxx vxz vzx vzz strxxx strxxz strzzx strzzz strxzx strxzz.
+enum IField { I_VXX, I_VXZ, I_VZX, I_VZZ, I_SXXX, I_SXXZ, I_SZZX, I_SZZZ, I_SXZX, I_SXZZ, I_NFIELDS };
+
+// Arguments of the isotropic elastic kernels (elastic2d.cu): ten in-place split fields.
+struct IArgs {
+    float* f[I_NFIELDS];
+    Layout2D L;
+    int nz, npx, npz;
+    // prepared model (YPUB:323-634), row z = 0 of column 0: busg2e, busg1e, lambmusg, lambsg, musge
+    const float* b2e; const float* b1e; const float* lm2; const float* lam; const float* mue;
+    int mpitch, nx_model;
+    float dt, dtdx, dtdz, dz2;
+    float a[5];
+    const float* spg;                     // spgxn spgxp spgzn' spgzp spg1xn spg2xp spg1zn' spg2zp
+    int spg_stride;
+    const ShotDev* shots;
+    const int* slot_to_shot;
+    const float* wavelets;
+    const float* stamps;
+    const int* rec_x; const int* rec_z;
+    const int* tile_rec_ptr; const int* tile_rec_idx;
+    float* records;                       // vx (record1), [nt][nrec] per shot
+    float* records2;                      // vz (record2)
+    int step;
+};
+cudaError_t elastic2d_launch_step(const IArgs& a, int active, cudaStream_t st);
+// YPUB:323-547 on one window (x-major, z fastest): substagger and the refill of the rows above
+// itopo (0-based rows < itopo - 1 take row itopo - 1); out: busg2e, busg1e, lambmusg, lambsg, musge.
+// Returns false on a zero density (YPUB:370, 400).
+bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, int itopo, float* b2e,
+                       float* b1e, float* lm2, float* lam, float* mue);
+// YPUB:1470-1501: the (2 rgau - 1)^2 Gaussian table (sigma 2 cells), normalised by its sum, in
+// Fortran order gc(idx1, idx2) = out[(idx2 - 1) * w + idx1 - 1]; *lo / *hi: 0-based index range
+// holding every non-zero weight (the same along both axes).
+void elastic2d_gauss_table(int rgau, std::vector<float>* out, int* lo, int* hi);
+// YPUB:1429-1466: the window of the source's Gaussian stamp clipped to the grid, box of
+// non-zero weights (x0, z0, w, h) and the weights (x-major, z fastest).
+void elastic2d_stamp(int nx, int nz, int sx, int sz, int rgau, const std::vector<float>& gc, int* box,
+                     std::vector<float>* out);
+// YPUB:796-849 cosine sponge, with the two top tables shifted for calpmlbclrtb's top loop
+// (YPUB:878-883: row k = 1..npzn takes spgzn(k + 1)).
+void elastic2d_sponge_tables(int np, float dx, float dz, int stride, float* out);
+// YPUB:592-634 on the device: the in-place Gaussian smoothing of rows z < itopo of the five
+// prepared arrays of every window (one sequential chain per array and window, serial order).
+// arrays: five device pointers to row z = 0 of column 0 (column pitch mpitch, `ghost` replicated
+// rows above z = 0, refreshed afterwards); win: nwin (start column, width) pairs.
+cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int nz, int itopo, const int* win_host,
+                             int nwin, const std::vector<float>& gc, int rgau, int lo, int hi, cudaStream_t st);
+
 // Arguments of the viscoacoustic adjoint kernels (q_adjoint2d.cu): adjoint fields in place.
 struct QAdjArgs {
     float* avx; float* avz;               // adjoints of vx, vz
@@ -247,7 +297,7 @@ cudaError_t launch_nan_scan(const float* rec, long long n, int* flag, cudaStream
 
 // ---- wavefield snapshots (snapshots.cu) ----
 struct SnapArgs {
-    const float* f[3];          // field slabs (nsum = 3: summed in order, the viscoacoustic sigma / r)
+    const float* f[3];          // split parts of the field, summed in order (nsum = 1, 2 or 3)
     int nsum;
     Layout2D L;
     int nz, pml;

@@ -24,7 +24,8 @@ __global__ void snapshot_kernel(const __grid_constant__ SnapArgs a) {
         const int x = a.pml + xi, z = a.pml + zi;
         const long long c = base + (long long)x * a.L.pitch + z;
         float v = a.f[0][c];
-        if (a.nsum == 3) v = __fadd_rn(__fadd_rn(v, a.f[1][c]), a.f[2][c]);  // (sx + sz) + sr, QS calsum
+        if (a.nsum >= 2) v = __fadd_rn(v, a.f[1][c]);  // split parts summed in order: x + z (QS, YPUB calu)
+        if (a.nsum == 3) v = __fadd_rn(v, a.f[2][c]);  // (sx + sz) + sr, QS calsum
         if (a.src_pre && x == sd.sx && z == sd.sz && a.step + 1 < sd.nt) v = a.src_pre[shot];
         out[i] = v;
     }

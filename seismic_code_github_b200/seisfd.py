@@ -12,9 +12,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libseisfd.so")
 
 OK, ERR_ARG, ERR_IO, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE = range(9)
-ACOUSTIC_2D, VISCOAC_2D, ACOUSTIC_3D, VISCOEL_2D = 0, 1, 2, 3
+ACOUSTIC_2D, VISCOAC_2D, ACOUSTIC_3D, VISCOEL_2D, ELASTIC_2D = 0, 1, 2, 3, 4
 EXACT, NAN_CHECK = 0x1, 0x2
-WAVELET_AFD, WAVELET_RIC, WAVELET_Q = 0, 1, 2
+WAVELET_AFD, WAVELET_RIC, WAVELET_Q, WAVELET_ISO = 0, 1, 2, 3
 FIELD_P, FIELD_VX, FIELD_VZ, FIELD_VY, FIELD_R, FIELD_SZZ, FIELD_SXZ = 0, 1, 2, 3, 4, 5, 6
 
 _F32P = ctypes.POINTER(ctypes.c_float)
@@ -92,6 +92,7 @@ SIGNATURES = {
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "sfd_set_gauss_radius": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "sfd_set_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int]),
@@ -251,14 +252,16 @@ class Engine:
 
     def set_model_elastic(self, vp: np.ndarray, vs: np.ndarray, den: Optional[np.ndarray] = None,
                           qp: Optional[np.ndarray] = None, qs: Optional[np.ndarray] = None):
-        """P and S velocities, density and quality factors of the visco-elastic scheme."""
+        """P and S velocities, density and quality factors of the visco-elastic scheme (the
+        isotropic elastic scheme takes no quality factors)."""
         arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (vp, vs, den, qp, qs)]
         self._keep_model = tuple(arrs)
         self._check(self._lib.sfd_set_model_elastic(self._h, *[_fp(a) for a in arrs]), "sfd_set_model_elastic")
 
     def records(self, field: int) -> np.ndarray:
-        """Records of one stress component from the last forward: FIELD_SZZ (record1, strzz) or
-        FIELD_P (record2, strxx), in the layout of forward()."""
+        """Records of one component from the last forward, in the layout of forward(): FIELD_SZZ
+        (record1, strzz) or FIELD_P (record2, strxx) for the Q_forward schemes, FIELD_VX (record1)
+        or FIELD_VZ (record2) for the isotropic elastic scheme."""
         out = np.empty(self.record_size(), np.float32)
         self._check(self._lib.sfd_get_records(self._h, field, _fp(out)), "sfd_get_records")
         return out
@@ -323,6 +326,11 @@ class Engine:
 
     def set_checkpoint_interval(self, steps: int):
         self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
+
+    def set_gauss_radius(self, rgau: int):
+        """Half-width of the source / top-sponge Gaussian of the isotropic elastic scheme
+        (YPUB:1470-1501; default 50)."""
+        self._check(self._lib.sfd_set_gauss_radius(self._h, int(rgau)), "sfd_set_gauss_radius")
 
     def set_memory_limit(self, nbytes: int):
         """Device-memory budget of gradient() (0: the free device memory)."""

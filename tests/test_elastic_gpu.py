@@ -1,0 +1,139 @@
+"""GPU isotropic elastic path (SFD_ELASTIC_2D: the abc mode of forward/yang_version_2016_2_2,
+flat surface) through the C ABI, against the FP32 restatement of the Fortran code
+(oracle/iso_oracle.cpp).  The kernels keep the reference's split fields and operation order and
+the top-sponge smoothing runs in the serial order, so both record sets (record1 = vx,
+record2 = vz, YPRI:361-367) must be bit-identical to the restatement; the FP64 restatement gives
+the reported precision error."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from conftest import bits_equal, rel_l2
+from seismic_code_github_b200 import seisfd as S
+
+pytestmark = pytest.mark.gpu
+
+
+def imodel(nx=70, nz=56, seed=0, vs_ratio=1.8):
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz)
+    vp = np.tile(np.where(z < nz // 2, 2000.0, 3000.0), (nx, 1)).astype(np.float32)
+    vp += (40.0 * rng.standard_normal((nx, nz))).astype(np.float32)
+    vs = (vp / vs_ratio).astype(np.float32) if vs_ratio else np.zeros_like(vp)
+    rho = (1900.0 + 300.0 * rng.random((nx, nz))).astype(np.float32)
+    return vp, vs, rho
+
+
+def run_gpu(model, npx, f0, dt, dx, shots_spec, rgau=None, per_shot=False, snap=None):
+    """shots_spec: list of (isxe, isze, nt_total, nrz0, idecay), 1-based padded source cell as in
+    the Fortran; interior model arrays (nx, nz)."""
+    vp, vs, rho = (S.pad_model(a, npx, npx, npx, npx) for a in model)
+    nx, nz = vp.shape
+    e = S.Engine(S.ELASTIC_2D, nx, nz, dx, dx, dt, npx, order=10, f0=f0)
+    if rgau is not None:
+        e.set_gauss_radius(rgau)
+    e.set_model_elastic(vp, vs, rho)
+    shots = []
+    for isxe, isze, ntot, nrz0, idecay in shots_spec:
+        rx = np.arange(npx, nx - npx, dtype=np.int32)
+        rz = np.full_like(rx, npx + nrz0 - 1)
+        shots.append(S.ShotSpec(isxe - 1, isze - 1, rx, rz, S.wavelet(S.WAVELET_ISO, ntot, dt, f0, delay=idecay)))
+    e.set_shots(shots)
+    if snap is not None:
+        e.set_snapshots(0, *snap)
+    r1 = e.forward_per_shot() if per_shot else e.forward()
+    r2 = e.records(S.FIELD_VZ)
+    return e.split_records(r1), e.split_records(r2), e.timing(), e
+
+
+@pytest.mark.parametrize("seed,rgau", [(0, 50), (1, 9)])
+def test_single_shot_bitexact_against_restatement(seed, rgau):
+    model = imodel(seed=seed)
+    npx, f0, dt, dx, nt, idecay = 10, 20.0, 5e-4, 10.0, 160, 40
+    isxe, isze, nrz0 = npx + 25, npx + 4, 1
+    r1, r2, t, e = run_gpu(model, npx, f0, dt, dx, [(isxe, isze, nt + idecay, nrz0, idecay)], rgau=rgau)
+    e.close()
+    kw = dict(nrz0=nrz0, idecay=idecay, rgau=rgau)
+    o1, o2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, isxe, isze, **kw)
+    d1, d2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, isxe, isze, fp64=True, **kw)
+    g1, g2 = r1[0][:, idecay:], r2[0][:, idecay:]
+    print(f"seed {seed}: vx relL2 vs FP32 restatement {rel_l2(g1, o1):.2e}, vs FP64 {rel_l2(g1, d1):.2e}; "
+          f"vz vs FP64 {rel_l2(g2, d2):.2e}; {t['launches']} launches {t['loop_ms']:.2f} ms")
+    assert np.abs(g1).max() > 0 and np.abs(g2).max() > 0
+    assert bits_equal(g1, o1)
+    assert bits_equal(g2, o2)
+
+
+def test_batched_uneven_shots_equal_per_shot_and_restatement():
+    model = imodel(seed=3, nx=80, nz=50, vs_ratio=1.7)
+    npx, f0, dt, dx, rgau = 10, 25.0, 5e-4, 10.0, 12
+    spec = [(npx + 12, npx + 3, 150, 1, 30), (npx + 60, npx + 8, 90, 2, 20), (npx + 40, npx + 20, 120, 1, 40)]
+    full = [(a, b, n + d, c, d) for a, b, n, c, d in spec]
+    b1, b2, _, e = run_gpu(model, npx, f0, dt, dx, full, rgau=rgau)
+    e.close()
+    p1, p2, _, e = run_gpu(model, npx, f0, dt, dx, full, rgau=rgau, per_shot=True)
+    e.close()
+    for i, (isxe, isze, nt, nrz0, idecay) in enumerate(spec):
+        o1, o2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, isxe, isze, nrz0=nrz0, idecay=idecay,
+                                   rgau=rgau)
+        assert bits_equal(b1[i][:, idecay:], o1) and bits_equal(b2[i][:, idecay:], o2), i
+        assert bits_equal(b1[i], p1[i]) and bits_equal(b2[i], p2[i]), i
+
+
+def test_zero_shear_velocity_bitexact():
+    # vs = 0: mu, musg and the harmonic musge (YPUB:449-462 zero branch) vanish
+    model = imodel(seed=4, vs_ratio=0)
+    npx, f0, dt, dx, nt, idecay = 10, 20.0, 5e-4, 10.0, 150, 30
+    r1, r2, _, e = run_gpu(model, npx, f0, dt, dx, [(npx + 20, npx + 5, nt + idecay, 1, idecay)], rgau=20)
+    e.close()
+    o1, o2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, npx + 20, npx + 5, nrz0=1, idecay=idecay, rgau=20)
+    assert np.abs(o1).max() > 0
+    assert bits_equal(r1[0][:, idecay:], o1) and bits_equal(r2[0][:, idecay:], o2)
+
+
+def test_wavefield_readback_and_snapshots():
+    model = imodel(seed=5, nx=40, nz=40)
+    npx, f0, dt, dx, nt, idecay = 8, 20.0, 5e-4, 10.0, 120, 30
+    spec = [(npx + 20, npx + 12, nt + idecay, 3, idecay)]
+    r1, r2, _, e = run_gpu(model, npx, f0, dt, dx, spec, rgau=15, snap=(S.FIELD_VX, nt + idecay - 1, 1, 1))
+    vx = e.wavefield(0, S.FIELD_VX)
+    vz = e.wavefield(0, S.FIELD_VZ)
+    sxz = e.wavefield(0, S.FIELD_SXZ)
+    snap = e.snapshots(0, 0)
+    e.close()
+    _, _, fin = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, npx + 20, npx + 12, nrz0=3, idecay=idecay, rgau=15,
+                               want_final=True)
+    assert np.abs(sxz).max() > 0
+    assert bits_equal(vx, fin)
+    row = npx + 3 - 1
+    assert np.array_equal(r1[0][:, -1], vx[npx:-npx, row]) and np.array_equal(r2[0][:, -1], vz[npx:-npx, row])
+    assert np.array_equal(snap[0], vx[npx:-npx, npx:-npx])
+
+
+def test_gauss_radius_change_reprepares():
+    model = imodel(seed=6, nx=50, nz=40)
+    npx, f0, dt, dx, nt, idecay = 9, 20.0, 5e-4, 10.0, 100, 30
+    spec = [(npx + 25, npx + 3, nt + idecay, 1, idecay)]
+    vp, vs, rho = (S.pad_model(a, npx, npx, npx, npx) for a in model)
+    nx, nz = vp.shape
+    with S.Engine(S.ELASTIC_2D, nx, nz, dx, dx, dt, npx, order=10, f0=f0) as e:
+        e.set_model_elastic(vp, vs, rho)
+        rx = np.arange(npx, nx - npx, dtype=np.int32)
+        e.set_shots([S.ShotSpec(npx + 24, npx + 2, rx, np.full_like(rx, npx), S.wavelet(S.WAVELET_ISO, nt + idecay, dt,
+                                                                                       f0, delay=idecay))])
+        a = e.forward().copy()
+        e.set_gauss_radius(4)  # after the model and the shots: both are re-prepared
+        b = e.forward().copy()
+    o4, _, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, npx + 25, npx + 3, nrz0=1, idecay=idecay, rgau=4)
+    o50, _, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, npx + 25, npx + 3, nrz0=1, idecay=idecay, rgau=50)
+    ntr = nx - 2 * npx
+    assert bits_equal(a.reshape(ntr, -1)[:, idecay:], o50)
+    assert bits_equal(b.reshape(ntr, -1)[:, idecay:], o4)
+
+
+def test_quality_factors_rejected():
+    model = imodel(seed=7, nx=30, nz=30)
+    vp, vs, rho = (S.pad_model(a, 8, 8, 8, 8) for a in model)
+    with S.Engine(S.ELASTIC_2D, vp.shape[0], vp.shape[1], 10.0, 10.0, 5e-4, 8, order=10, f0=20.0) as e:
+        with pytest.raises(RuntimeError):
+            e.set_model_elastic(vp, vs, rho, qp=np.full_like(vp, 50.0))

@@ -72,7 +72,7 @@ def py_prepare(vp, vs, rho, npx, npz, rgau):
     lambmusg[:, NX - 1] = lamb[:, NX - 1] + F(2) * mu[:, NX - 1]
     out = [b2e, b1e, lambmusg, lambsg, musge]
     itopo = npz  # 1-based row itopo = npzn
-    for a in out:  # rows above itopo refilled (YPUB:475-491)
+    for a in out:  # rows above itopo refilled (YPUB:484-501)
         for k in range(itopo - 1, 0, -1):
             a[k - 1] = a[k]
     # Gaussian coefficients (YPUB:1470-1501), sigma = 2

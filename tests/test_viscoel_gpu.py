@@ -105,12 +105,16 @@ def test_wavefield_readback_and_snapshots():
         rx = np.array([20], np.int32)
         e.set_shots([S.ShotSpec(25, 12, rx, rx, S.wavelet(S.WAVELET_Q, 150, dt, f0))])
         e.set_snapshots(0, S.FIELD_SZZ, 149, 1, 1)
+        e.set_snapshots(1, S.FIELD_VX, 149, 1, 1)  # a two-part field: vxx + vxz
         rec = e.forward()
         rec2 = e.records(S.FIELD_P)
         szz = e.wavefield(0, S.FIELD_SZZ)
         sxx = e.wavefield(0, S.FIELD_P)
         sxz = e.wavefield(0, S.FIELD_SXZ)
+        vx = e.wavefield(0, S.FIELD_VX)
         snap = e.snapshots(0, 0)
+        snap_vx = e.snapshots(1, 0)
     assert np.abs(sxz).max() > 0
     assert szz[20, 20] == rec[-1] and sxx[20, 20] == rec2[-1]
     assert np.array_equal(snap[0], szz[npx:-npx, npx:-npx])
+    assert np.array_equal(snap_vx[0], vx[npx:-npx, npx:-npx])
