@@ -148,6 +148,14 @@ int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const 
  * smooth"; default 50).  Re-prepares the model and the source stamps if they are set. */
 int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau);
 
+/* Boundary mode of SFD_ELASTIC_2D (YPRI:190-219 `molmod`).  top = 0: 'abc', the cosine sponge on
+ * all four sides with the top sponge's moduli smoothed (YPRI:234-386; the default).  top >= 1:
+ * 'fsbc', a flat free surface at padded row top - 1 (the reference's itopo = npzn = top,
+ * YPRI:57-230): no top sponge, lower-order z derivatives on the five rows below the surface,
+ * tau_zz = 0 on and above it, the tau_xz image and the extrapolated vz one row above it; the
+ * rows above the surface are air.  Re-prepares the model if it is set. */
+int sfd_set_free_surface(sfd_ctx* ctx, int top);
+
 /* Shots.  Replaces the shot loop QM:124-141 (one launch for all shots instead of one process
  * per shot).  Wavelets and receiver lists are copied; the caller keeps ownership. */
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots);

@@ -1,7 +1,7 @@
 // ORACLE -- test infrastructure only. CPU restatement of the reference's isotropic elastic
-// standard-staggered-grid modelling of one shot (forward/yang_version_2016_2_2, 'abc' mode:
-// cosine sponge on all four sides) for a flat surface, used by tests/ as the checker of the
-// SFD_ELASTIC_2D GPU path.  The reference is Fortran 90 + MPI + OpenMP and cannot be compiled in
+// standard-staggered-grid modelling of one shot (forward/yang_version_2016_2_2, both modes:
+// 'abc', cosine sponge on all four sides, and 'fsbc', free surface on top) for a flat surface,
+// used by tests/ as the checker of the SFD_ELASTIC_2D GPU path.  The reference is Fortran 90 + MPI + OpenMP and cannot be compiled in
 // this environment (no Fortran compiler), so this restatement is not pinned by a run of the
 // reference: "parity unpinned" for this scheme; it is checked by physics properties instead
 // (tests/test_iso_oracle.py).
@@ -20,6 +20,14 @@
 //   YPUB:1095-1157 caluxabs    YPUB:1347-1407 caluzabs    YPUB:1410-1426 calu (sums)
 //   YPUB:1429-1466 addsrc      YPUB:1470-1501 get_gauss_filter_coe
 //   YPRI:234-386   isoewm2dabc (time loop)     YPUB:2-16 get_record (record1 = vx, record2 = vz)
+//   YPRI:57-230    isoewm2dfsbc (time loop, free surface): YPUB:1026-1092 calux and
+//                  YPUB:1160-1343 caluz (rows from itopo; z derivatives of order 8, 6, 4, 2 on the
+//                  five rows nearest the surface, YMOD:7-20), YPUB:901-934 calpmlbclrb (no top
+//                  sponge), YPUB:938-976 calfsbcv, YPUB:978-1007 calfsbcstrzz,
+//                  YPUB:1009-1024 calfsbcstrxz; no smoothing
+//   The free-surface velocity vz(itopo - 1) = vz(itopo) + lambda/(lambda + 2 mu) dx vx is written
+//   into the split parts after calu has summed them (YPRI:141-150), so the stress update reads
+//   it one step later.
 // The split fields also hold a row k = 0 (YPUB:1095 `ux(0:nz,nx)`, loops from itopo - npzn = 0);
 // calu and get_record never read it, so it is not kept here.  Fortran (k, i), k = z, i = x,
 // maps to C index (i-1)*nz + (k-1).
@@ -48,6 +56,9 @@ struct IsoSolver {
     int nx, nz, npxn, npxp, npzn, npzp;
     T dx, dz, dt;
     T a[5];
+    bool fs = false;   // free surface (fsbc mode)
+    int itopo = 1;     // surface row (1-based), flat
+    T cr[6][5] = {};   // cr[M]: coefficients of the M-term staggered derivative (YMOD:7-27)
     Field<T> vx, vz, sxx, szz, sxz;                                     // (-4:nz+5, -4:nx+5)
     Field<T> vxx, vxz, vzx, vzz, sxxx, sxxz, szzx, szzz, sxzx, sxzz;    // (1:nz, 1:nx)
     Field<T> busg1e, busg2e, lambsg, lambmusg, musge;                   // (1:nz, 1:nx)
@@ -60,32 +71,43 @@ struct IsoSolver {
         for (auto* f : {&vxx, &vxz, &vzx, &vzz, &sxxx, &sxxz, &szzx, &szzz, &sxzx, &sxzz}) *f = N();
     }
 
-    // YPUB:1095-1157 (x) and YPUB:1347-1407 (z); flag 0: u(i) - u(i-1) ..., flag 1: u(i+1) - u(i) ...
-    T der(const Field<T>& u, int k, int i, bool xdir, int flag) const {
+    // YPUB:1095-1157 (x) and YPUB:1347-1407 (z); flag 0: u(i) - u(i-1) ..., flag 1: u(i+1) - u(i) ...;
+    // M terms (5 = 10th order; fewer near the free surface, YPUB:1183-1251, 1275-1335)
+    T der(const Field<T>& u, int k, int i, bool xdir, int flag, int M = 5) const {
         auto U = [&](int o) { return xdir ? u(k, i + o) : u(k + o, i); };
         T s = 0;
-        for (int m = 0; m < 5; m++) {
+        for (int m = 0; m < M; m++) {
             const T t = flag == 0 ? U(m) - U(-1 - m) : U(1 + m) - U(-m);
-            s = (m == 0) ? a[0] * t : s + a[m] * t;
+            s = (m == 0) ? cr[M][0] * t : s + cr[M][m] * t;
         }
         return s;
     }
-    // ux(k,i) = ux(k,i) + (dt/dh)*pa(k,i)*(...)
+    // terms of caluz's derivative at row k (YPUB:1160-1343): d = k - itopo from the surface
+    int zterms(int k, int flag) const {
+        if (!fs) return 5;
+        const int d = k - itopo;
+        return flag == 0 ? (d >= 5 ? 5 : (d < 1 ? 1 : d)) : (d >= 4 ? 5 : d + 1);
+    }
+    // ux(k,i) = ux(k,i) + (dt/dh)*pa(k,i)*(...); fsbc: rows from itopo (calux / caluz)
     void update(Field<T>& ux, const Field<T>& u, const Field<T>& pa, bool xdir, int flag) {
         const T c = xdir ? dt / dx : dt / dz;
+        const int k0 = fs ? itopo : 1;
 #pragma omp parallel for schedule(static)
         for (int i = 1; i <= nx; i++)
-            for (int k = 1; k <= nz; k++) ux(k, i) = ux(k, i) + c * pa(k, i) * der(u, k, i, xdir, flag);
+            for (int k = k0; k <= nz; k++)
+                ux(k, i) = ux(k, i) + c * pa(k, i) * der(u, k, i, xdir, flag, xdir ? 5 : zterms(k, flag));
     }
     // YPUB:851-897, flat surface (itopo(i) - npzn = 0); the top loop runs k = 0..npzn with
     // factor spgzn(k + 1), of which rows 1..npzn are kept here
+    // fsbc: YPUB:901-934 calpmlbclrb, left and right from row itopo, no top sponge
     void sponge(Field<T>& ux, Field<T>& uz, const std::vector<T>& sxn, const std::vector<T>& sxp,
                 const std::vector<T>& szn, const std::vector<T>& szp) {
+        const int k0 = fs ? itopo : 1;
         for (int i = 1; i <= npxn + 1; i++)
-            for (int k = 1; k <= nz; k++) ux(k, i) = ux(k, i) * sxn[i - 1];
+            for (int k = k0; k <= nz; k++) ux(k, i) = ux(k, i) * sxn[i - 1];
         for (int i = 1; i <= npxp + 1; i++)
-            for (int k = 1; k <= nz; k++) ux(k, nx - i + 1) = ux(k, nx - i + 1) * sxp[i - 1];
-        for (int i = 1; i <= nx; i++)
+            for (int k = k0; k <= nz; k++) ux(k, nx - i + 1) = ux(k, nx - i + 1) * sxp[i - 1];
+        for (int i = 1; i <= nx && !fs; i++)
             for (int k = 1; k <= npzn; k++) uz(k, i) = uz(k, i) * szn[k];
         for (int i = 1; i <= nx; i++)
             for (int k = 1; k <= npzp + 1; k++) uz(nz - k + 1, i) = uz(nz - k + 1, i) * szp[k - 1];
@@ -95,9 +117,27 @@ struct IsoSolver {
             for (int k = 1; k <= nz; k++) v(k, i) = a_(k, i) + b_(k, i);
     }
 
-    // YPRI:305-359, one step of isoewm2dabc; `src` adds the source to a split stress
+    // YPUB:938-976 calfsbcv on one pair of split parts: vz(izh-1) from vz(izh) and dx vx(izh)
+    void fsbcv(const Field<T>& vxp, Field<T>& vzp) {
+        if (itopo - 1 < 1) return;  // row 0 of the split parts is never read
+        for (int i = 1; i <= nx - 1; i++)
+            vzp(itopo - 1, i) = vzp(itopo, i) + (lambsg(itopo, i) / lambmusg(itopo, i)) * (vxp(itopo, i + 1) - vxp(itopo, i));
+    }
+    // YPUB:978-1007 calfsbcstrzz: rows 0..itopo zero
+    void fsbczz(Field<T>& t) {
+        for (int i = 1; i <= nx; i++)
+            for (int k = 1; k <= itopo; k++) t(k, i) = T(0.0);
+    }
+    // YPUB:1009-1024 calfsbcstrxz: image row above the surface
+    void fsbcxz(Field<T>& t) {
+        if (itopo - 1 < 1) return;
+        for (int i = 1; i <= nx; i++) t(itopo - 1, i) = -t(itopo, i);
+    }
+
+    // YPRI:305-359 (isoewm2dabc) or YPRI:121-196 (isoewm2dfsbc), one step; `src` adds the source
+    // to a split stress
     template <typename Src>
-    void step(Src&& src) {
+    void step(Src&& src, bool src_xx) {
         update(vxx, sxx, busg2e, true, 0);     // xflag 0, strxx
         update(vxz, sxz, busg2e, false, 0);    // zflag 0, strxz
         sponge(vxx, vxz, spgxn, spgxp, spgzn, spgzp);
@@ -106,19 +146,31 @@ struct IsoSolver {
         update(vzz, szz, busg1e, false, 1);    // zflag 1, strzz
         sponge(vzx, vzz, spg1xn, spg2xp, spg1zn, spg2zp);
         sum2(vz, vzx, vzz);
+        if (fs) {
+            fsbcv(vxx, vzx);
+            fsbcv(vxz, vzz);
+        }
         update(sxxx, vx, lambmusg, true, 1);
         update(sxxz, vz, lambsg, false, 0);
         sponge(sxxx, sxxz, spg1xn, spg2xp, spgzn, spgzp);
-        src(sxxx);
+        if (src_xx) src(sxxx);
         sum2(sxx, sxxx, sxxz);
         update(szzx, vx, lambsg, true, 1);
         update(szzz, vz, lambmusg, false, 0);
         sponge(szzx, szzz, spg1xn, spg2xp, spgzn, spgzp);
+        if (fs) {
+            fsbczz(szzz);
+            fsbczz(szzx);
+        }
         src(szzx);
         sum2(szz, szzx, szzz);
         update(sxzx, vz, musge, true, 0);
         update(sxzz, vx, musge, false, 1);
         sponge(sxzx, sxzz, spgxn, spgxp, spg1zn, spg2zp);
+        if (fs) {
+            fsbcxz(sxzx);
+            fsbcxz(sxzz);
+        }
         sum2(sxz, sxzx, sxzz);
     }
 };
@@ -158,7 +210,17 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     // YMOD:23-27, single precision constants
     const float af[5] = {19845.0f / 16384.0f, -735.0f / 8192.0f, 567.0f / 40960.0f, -405.0f / 229376.0f,
                          35.0f / 294912.0f};
-    for (int m = 0; m < 5; m++) S.a[m] = (T)af[m];
+    for (int m = 0; m < 5; m++) S.a[m] = S.cr[5][m] = (T)af[m];
+    // YMOD:7-20 lower orders
+    const float a8[4] = {1225.0f / 1024.0f, -245.0f / 3072.0f, 49.0f / 5120.0f, -5.0f / 7168.0f};
+    const float a6[3] = {75.0f / 64.0f, -25.0f / 384.0f, 3.0f / 640.0f};
+    const float a4[2] = {9.0f / 8.0f, -1.0f / 24.0f};
+    for (int m = 0; m < 4; m++) S.cr[4][m] = (T)a8[m];
+    for (int m = 0; m < 3; m++) S.cr[3][m] = (T)a6[m];
+    for (int m = 0; m < 2; m++) S.cr[2][m] = (T)a4[m];
+    S.cr[1][0] = (T)1.0f;
+    S.fs = c->fsbc != 0;
+    S.itopo = c->npzn;
     if (S.nx < 12 || S.nz < 12) return 1;
     S.alloc();
     const int NX = S.nx, NZ = S.nz;
@@ -259,7 +321,9 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
         for (int i = 1; i <= NX; i++)
             for (int k = itopo; k >= 2; k--) (*f)(k - 1, i) = (*f)(k, i);
     // YPRI:301-302 modipapml, abc mode only
-    for (auto* f : {&S.lambsg, &S.musge, &S.lambmusg, &S.busg1e, &S.busg2e}) gauss_filter(*f, NX, NZ, c->rgau, itopo, gc);
+    if (!S.fs)
+        for (auto* f : {&S.lambsg, &S.musge, &S.lambmusg, &S.busg1e, &S.busg2e})
+            gauss_filter(*f, NX, NZ, c->rgau, itopo, gc);
     // YPUB:796-849 cosine sponge, R = 1e-3
     {
         const T Rr = (T)1.0e-3f;
@@ -325,9 +389,11 @@ int run_iso(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     // YPRI:305-367
     const int nt = c->nt;
     const int kr = itopo + c->nrz0;
+    // YPRI:163-168: in fsbc mode strxx takes the source only below the surface
+    const bool src_xx = !S.fs || isze > itopo;
     for (int it = 1; it <= nt + c->idecay; it++) {
         it_cur = it;
-        S.step(addsrc);
+        S.step(addsrc, src_xx);
         const int iit = it - c->idecay;
         if (iit >= 1) {
             for (int i = 1; i <= nxe; i++) {

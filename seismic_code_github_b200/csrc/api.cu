@@ -118,6 +118,7 @@ struct sfd_ctx {
     // isotropic elastic scheme (yang_version): Gaussian half-width, its table and non-zero range;
     // the prepared model lives in e_q[0..4] (busg2e, busg1e, lambmusg, lambsg, musge)
     int iso_rgau = 50;
+    int iso_top = 0;                // 0: abc mode; >= 1: fsbc mode, free surface at 1-based row iso_top
     std::vector<float> iso_gc;
     int iso_lo = 0, iso_hi = -1;
     long long model_gen = 0;        // bumped by every sfd_set_model
@@ -126,6 +127,7 @@ struct sfd_ctx {
     std::vector<std::pair<int, int>> prep_wins;
     long long prep_gen = -1;
     int prep_rgau = -1;
+    int prep_top = -1;
 
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
@@ -466,6 +468,14 @@ IArgs make_iargs(const sfd_ctx* c, int step) {
     const float af[5] = {19845.0f / 16384.0f, -735.0f / 8192.0f, 567.0f / 40960.0f, -405.0f / 229376.0f,
                          35.0f / 294912.0f};  // YMOD:23-27
     std::memcpy(a.a, af, sizeof(af));
+    // YMOD:7-20: the lower orders caluz uses next to the free surface
+    const float cr[4][4] = {{1.0f, 0.0f, 0.0f, 0.0f},
+                            {9.0f / 8.0f, -1.0f / 24.0f, 0.0f, 0.0f},
+                            {75.0f / 64.0f, -25.0f / 384.0f, 3.0f / 640.0f, 0.0f},
+                            {1225.0f / 1024.0f, -245.0f / 3072.0f, 49.0f / 5120.0f, -5.0f / 7168.0f}};
+    std::memcpy(a.cr, cr, sizeof(cr));
+    a.fs = c->iso_top > 0 ? 1 : 0;
+    a.zs = c->iso_top - 1;
     a.spg = c->d_spg;
     a.spg_stride = c->spg_stride;
     a.shots = c->d_shots;
@@ -604,8 +614,9 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
     if (ctx->g.scheme == SFD_ELASTIC_2D) {
         IArgs e = make_iargs(ctx, k);
         e.slot_to_shot = slots;
-        CK(elastic2d_launch_step(e, act, ctx->stream));
-        *launches += 2;
+        int n = 0;
+        CK(elastic2d_launch_step(e, act, ctx->L.ntx * kTileX, ctx->stream, &n));
+        *launches += n;
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOEL_2D) {
@@ -1210,7 +1221,7 @@ int q_prepare(sfd_ctx* ctx) {
         width += wins[b].second;
     }
     if (iso && wins == ctx->prep_wins && ctx->model_gen == ctx->prep_gen && ctx->iso_rgau == ctx->prep_rgau &&
-        width == ctx->q_width) {
+        ctx->iso_top == ctx->prep_top && width == ctx->q_width) {
         if (ctx->have_shots) {
             for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
             CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
@@ -1225,10 +1236,11 @@ int q_prepare(sfd_ctx* ctx) {
         if (!ctx->h_den.empty()) rho.assign(ctx->h_den.begin() + off, ctx->h_den.begin() + off + len);
         const float* qw = ctx->h_q.empty() ? nullptr : ctx->h_q.data() + off;
         const size_t o = (size_t)start[b] * nz;
-        if (iso) {  // YPUB:323-547 per window, flat surface: itopo = npzn = pml
+        if (iso) {  // YPUB:323-547 per window, flat surface: itopo = npzn (pml, or the free surface's row)
             std::vector<float> vs(len, 0.0f);
             if (!ctx->h_vs.empty()) vs.assign(ctx->h_vs.begin() + off, ctx->h_vs.begin() + off + len);
-            if (!elastic2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(), ctx->g.pml,
+            const int itopo = ctx->iso_top > 0 ? ctx->iso_top : ctx->g.pml;
+            if (!elastic2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(), itopo,
                                    eq[0].data() + o, eq[1].data() + o, eq[2].data() + o, eq[3].data() + o,
                                    eq[4].data() + o))
                 return set_err(ctx, SFD_ERR_ARG, "zero density in the window at column %d", wins[b].first);
@@ -1263,15 +1275,17 @@ int q_prepare(sfd_ctx* ctx) {
     if (iso) {
         for (int i = 0; i < 5; i++)
             if ((rc = upload(&ctx->e_q[i], eq[i]))) return rc;
-        // YPUB:549-634 modipapml on the device: rows z < pml of the five arrays, per window
-        std::vector<int> win(2 * wins.size());
-        for (size_t b = 0; b < wins.size(); b++) {
-            win[2 * b] = start[b];
-            win[2 * b + 1] = wins[b].second;
-        }
+        // YPUB:549-634 modipapml on the device (abc mode only, YPRI:301-302): rows z < pml of the
+        // five arrays, per window
+        std::vector<int> win;
+        if (ctx->iso_top == 0)
+            for (size_t b = 0; b < wins.size(); b++) {
+                win.push_back(start[b]);
+                win.push_back(wins[b].second);
+            }
         float* arrs[5];
         for (int i = 0; i < 5; i++) arrs[i] = ctx->e_q[i] + kModelGhostZ;
-        CK(elastic2d_smooth(arrs, ctx->mpitch, kModelGhostZ, nz, ctx->g.pml, win.data(), (int)wins.size(),
+        CK(elastic2d_smooth(arrs, ctx->mpitch, kModelGhostZ, nz, ctx->g.pml, win.data(), (int)win.size() / 2,
                             ctx->iso_gc, ctx->iso_rgau, ctx->iso_lo, ctx->iso_hi, ctx->stream));
     } else if ((rc = upload(&ctx->q_busg, busg))) {
         return rc;
@@ -1287,6 +1301,7 @@ int q_prepare(sfd_ctx* ctx) {
     ctx->prep_wins = wins;
     ctx->prep_gen = ctx->model_gen;
     ctx->prep_rgau = ctx->iso_rgau;
+    ctx->prep_top = ctx->iso_top;
     if (ctx->have_shots) {
         for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
         CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
@@ -2330,6 +2345,19 @@ int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau) {
     int rc;
     if (ctx->have_shots && (rc = build_stamps(ctx))) return rc;
     return q_prepare(ctx);  // the top sponge's smoothing (no-op without a model)
+}
+
+int sfd_set_free_surface(sfd_ctx* ctx, int top) {
+    if (!ctx || top < 0) return SFD_ERR_ARG;
+    if (ctx->g.scheme != SFD_ELASTIC_2D)
+        return set_err(ctx, SFD_ERR_ARG, "the free surface applies to SFD_ELASTIC_2D");
+    if (top >= ctx->g.nz - ctx->g.pml - 5)
+        return set_err(ctx, SFD_ERR_ARG, "free-surface row %d too deep for nz = %d", top, ctx->g.nz);
+    if (top == ctx->iso_top) return SFD_OK;
+    CK(cudaSetDevice(ctx->device));
+    ctx->iso_top = top;
+    ctx->graph_valid = false;
+    return q_prepare(ctx);  // substagger's refill row and the smoothing follow the mode
 }
 
 int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes) {

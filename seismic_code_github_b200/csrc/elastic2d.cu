@@ -1,6 +1,6 @@
-// Isotropic elastic (P-SV) standard-staggered-grid time step, 10th order: the 'abc' mode of
-// forward/yang_version_2016_2_2 (YPRI:234-386, cosine sponge on all four sides) for a flat
-// surface.  Every field is kept in the reference's split form (x and z parts), ten per cell:
+// Isotropic elastic (P-SV) standard-staggered-grid time step, 10th order: the two modes of
+// forward/yang_version_2016_2_2 for a flat surface -- 'abc' (YPRI:234-386, cosine sponge on all
+// four sides) and 'fsbc' (YPRI:57-230, free surface at row zs, no top sponge).  Every field is kept in the reference's split form (x and z parts), ten per cell:
 //   vxx vxz vzx vzz | strxxx strxxz | strzzx strzzz | strxzx strxzz
 // and one step is two kernels (YPUB = Iso_multishot_fd_subroutine_fsbc_zy_m2_pub.f90):
 //   velocity: strxx, strxz, strzz = sums of their parts (YPUB:1410-1426) on the tile plus halo;
@@ -17,8 +17,18 @@
 // Every multiply and add is rounded separately in the reference's order, so the kernels agree
 // bit for bit with the FP32 restatement in oracle/iso_oracle.cpp.
 //
-// Model preparation (host, per shot window): substagger (YPUB:323-547); then on the device the
-// PML smoothing of modipapml (YPUB:549-634), which overwrites each top-sponge cell with the
+// Free surface (fsbc): rows above zs keep their values; the z derivatives of the five rows from
+// zs down drop to 8th, 6th, 4th and 2nd order (YPUB:1160-1343); left and right sponges act from
+// zs down, the bottom sponge everywhere, no top sponge (YPUB:901-934); strzz parts are zero on
+// rows <= zs after their sponge and before the source (YPUB:978-1007), which enters strxx only for
+// sources below the surface (YPRI:163-168).  After the stress kernel the surface kernel writes
+// the image strxz(zs - 1) = -strxz(zs) (YPUB:1009-1024) and vz(zs - 1) from vz(zs) and dx vx(zs)
+// (YPUB:938-976).  The reference writes that vz after summing the split parts, so its stress
+// update reads it one step later; running the surface kernel after the stress kernel gives the
+// same order.
+//
+// Model preparation (host, per shot window): substagger (YPUB:323-547); then, in abc mode, on the
+// device the PML smoothing of modipapml (YPUB:549-634), which overwrites each top-sponge cell with the
 // Gaussian-weighted sum of its window while later cells read the already smoothed ones: a
 // sequential chain, run as one thread per array and window in the reference's serial order.
 #include <cuda_runtime.h>
@@ -109,9 +119,11 @@ __device__ __forceinline__ float4 dx4(const float* s, int r, int c, const float*
     return acc;
 }
 
-// z derivative (YPUB:1347-1407) of the same four cells: the window z-8 .. z+11 (c = column of z)
-template <int FLAG>
-__device__ __forceinline__ float4 dz4(const float* s, int r, int c, const float* a) {
+// z derivative (YPUB:1347-1407) of the same four cells: the window z-8 .. z+11 (c = column of z).
+// d0: distance of the first cell below the free surface (large without one).  Cells d = 0..4
+// rows below it take the lower orders of caluz (YPUB:1160-1343); the ones above it are not used.
+template <int FLAG, bool FS>
+__device__ __forceinline__ float4 dz4(const float* s, int r, int c, const IArgs& a, int d0) {
     float w[20];
 #pragma unroll
     for (int j = 0; j < 5; j++) {
@@ -121,16 +133,28 @@ __device__ __forceinline__ float4 dz4(const float* s, int r, int c, const float*
     float4 acc;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
+        const int d = d0 + q;
+        const int M = !FS ? 5 : FLAG == 0 ? (d >= 5 ? 5 : (d < 1 ? 1 : d)) : (d >= 4 ? 5 : (d < 0 ? 1 : d + 1));
         float sum = 0.0f;
 #pragma unroll
         for (int m = 0; m < 5; m++) {
+            if (m >= M) break;
+            const float cm = M == 5 ? a.a[m] : a.cr[M - 1 > 0 ? (M == 4 ? 3 : M == 3 ? 2 : 1) : 0][m & 3];
             const int z = 8 + q;  // index of cell q in w
             const float t = FLAG == 0 ? fs(w[z + m], w[z - 1 - m]) : fs(w[z + 1 + m], w[z - m]);
-            sum = (m == 0) ? fm(a[0], t) : fa(sum, fm(a[m], t));
+            sum = (m == 0) ? fm(cm, t) : fa(sum, fm(cm, t));
         }
         cmpr(acc, q) = sum;
     }
     return acc;
+}
+
+// z-part sponge: abc, top then bottom table (YPUB:851-897); fsbc, the bottom table only
+template <bool FS>
+__device__ __forceinline__ float zsp(float u, int z, const IArgs& a, const float* tn, const float* tp) {
+    if (!FS) return xs(u, z, a.nz, a.npz, tn, tp);
+    if (z >= a.nz - a.npz - 1) u = fm(u, tp[a.nz - 1 - z]);
+    return u;
 }
 
 // four cells of a field: one 16-byte access when all four lie inside the grid, else per cell
@@ -148,6 +172,7 @@ __device__ __forceinline__ void st4(float* f, long long c, int nv, const float4&
     for (int q = 0; q < nv; q++) f[c + q] = cmp(v, q);
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(kThreads, 3) iso_velocity_kernel(const __grid_constant__ IArgs a) {
     extern __shared__ __align__(16) float smem[];
     float* sSxx = smem;
@@ -165,6 +190,7 @@ __global__ void __launch_bounds__(kThreads, 3) iso_velocity_kernel(const __grid_
     const int zv = threadIdx.x & 15, z = 4 * zv, gz = t.z0 + z;
     const int nv = min(4, nz - gz);  // cells of the vector inside the grid
     if (nv <= 0) return;             // no barrier follows
+    const int d0 = FS ? gz - a.zs : (1 << 20);
 #pragma unroll 1
     for (int j = 0; j < kItems; j++) {
         const int r = (threadIdx.x >> 4) + 16 * j, gx = t.x0 + r;
@@ -175,29 +201,35 @@ __global__ void __launch_bounds__(kThreads, 3) iso_velocity_kernel(const __grid_
         float4 vzx = ld4(a.f[I_VZX], c, nv), vzz = ld4(a.f[I_VZZ], c, nv);
         const float4 b2 = __ldg(reinterpret_cast<const float4*>(a.b2e + mi));
         const float4 b1 = __ldg(reinterpret_cast<const float4*>(a.b1e + mi));
-        const float4 d_xx = dx4<0>(sSxx, r + H, z + HZ, a.a);   // Dx0 strxx
-        const float4 d_xz = dz4<0>(sSxz, r + H, z + HZ, a.a);   // Dz0 strxz
-        const float4 d_zx = dx4<1>(sSxz, r + H, z + HZ, a.a);   // Dx1 strxz
-        const float4 d_zz = dz4<1>(sSzz, r + H, z + HZ, a.a);   // Dz1 strzz
+        const float4 d_xx = dx4<0>(sSxx, r + H, z + HZ, a.a);      // Dx0 strxx
+        const float4 d_xz = dz4<0, FS>(sSxz, r + H, z + HZ, a, d0);    // Dz0 strxz
+        const float4 d_zx = dx4<1>(sSxz, r + H, z + HZ, a.a);      // Dx1 strxz
+        const float4 d_zz = dz4<1, FS>(sSzz, r + H, z + HZ, a, d0);    // Dz1 strzz
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int zq = min(gz + q, nz - 1);  // cells past nz are computed, not stored
+            const bool below = !FS || gz + q >= a.zs;  // fsbc: rows above the surface keep their values
             // YPRI:310-316: vx parts, sponge spgxn/spgxp (x part), spgzn/spgzp (z part)
-            const float n_xx = fa(cmp(vxx, q), fm(fm(a.dtdx, cmp(b2, q)), cmp(d_xx, q)));
-            const float n_xz = fa(cmp(vxz, q), fm(fm(a.dtdz, cmp(b2, q)), cmp(d_xz, q)));
-            cmpr(vxx, q) = xs(n_xx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
-            cmpr(vxz, q) = xs(n_xz, zq, nz, a.npz, tb + 2 * st, tb + 3 * st);
+            if (below) {
+                const float n_xx = fa(cmp(vxx, q), fm(fm(a.dtdx, cmp(b2, q)), cmp(d_xx, q)));
+                cmpr(vxx, q) = xs(n_xx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
+                cmpr(vxz, q) = fa(cmp(vxz, q), fm(fm(a.dtdz, cmp(b2, q)), cmp(d_xz, q)));
+            }
+            cmpr(vxz, q) = zsp<FS>(cmp(vxz, q), zq, a, tb + 2 * st, tb + 3 * st);
             // YPRI:320-326: vz parts, sponge spg1xn/spg2xp, spg1zn/spg2zp
-            const float n_zx = fa(cmp(vzx, q), fm(fm(a.dtdx, cmp(b1, q)), cmp(d_zx, q)));
-            const float n_zz = fa(cmp(vzz, q), fm(fm(a.dtdz, cmp(b1, q)), cmp(d_zz, q)));
-            cmpr(vzx, q) = xs(n_zx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-            cmpr(vzz, q) = xs(n_zz, zq, nz, a.npz, tb + 6 * st, tb + 7 * st);
+            if (below) {
+                const float n_zx = fa(cmp(vzx, q), fm(fm(a.dtdx, cmp(b1, q)), cmp(d_zx, q)));
+                cmpr(vzx, q) = xs(n_zx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
+                cmpr(vzz, q) = fa(cmp(vzz, q), fm(fm(a.dtdz, cmp(b1, q)), cmp(d_zz, q)));
+            }
+            cmpr(vzz, q) = zsp<FS>(cmp(vzz, q), zq, a, tb + 6 * st, tb + 7 * st);
         }
         st4(a.f[I_VXX], c, nv, vxx); st4(a.f[I_VXZ], c, nv, vxz);
         st4(a.f[I_VZX], c, nv, vzx); st4(a.f[I_VZZ], c, nv, vzz);
     }
 }
 
+template <bool FS>
 __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_constant__ IArgs a) {
     __shared__ __align__(16) float sVx[SMEM];
     __shared__ __align__(16) float sVz[SMEM];
@@ -213,6 +245,8 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
     const float wav = __ldg(a.wavelets + sd.wav_off + a.step);
     const int zv = threadIdx.x & 15, z = 4 * zv, gz = t.z0 + z;
     const int nv = min(4, nz - gz);
+    const int d0 = FS ? gz - a.zs : (1 << 20);
+    const bool src_xx = !FS || sd.sz > a.zs;  // YPRI:163-168
 #pragma unroll 1
     for (int j = 0; j < kItems && nv > 0; j++) {
         const int r = (threadIdx.x >> 4) + 16 * j, gx = t.x0 + r;
@@ -225,10 +259,10 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
         const float4 lm2 = __ldg(reinterpret_cast<const float4*>(a.lm2 + mi));
         const float4 lam = __ldg(reinterpret_cast<const float4*>(a.lam + mi));
         const float4 mue = __ldg(reinterpret_cast<const float4*>(a.mue + mi));
-        const float4 d1 = dx4<1>(sVx, r + H, z + HZ, a.a);   // Dx1 vx
-        const float4 d2 = dz4<0>(sVz, r + H, z + HZ, a.a);   // Dz0 vz
-        const float4 d3 = dx4<0>(sVz, r + H, z + HZ, a.a);   // Dx0 vz
-        const float4 d4 = dz4<1>(sVx, r + H, z + HZ, a.a);   // Dz1 vx
+        const float4 d1 = dx4<1>(sVx, r + H, z + HZ, a.a);       // Dx1 vx
+        const float4 d2 = dz4<0, FS>(sVz, r + H, z + HZ, a, d0);     // Dz0 vz
+        const float4 d3 = dx4<0>(sVz, r + H, z + HZ, a.a);       // Dx0 vz
+        const float4 d4 = dz4<1, FS>(sVx, r + H, z + HZ, a, d0);     // Dz1 vx
         const int bx = gx - sd.stamp_x0;
         const bool xin = bx >= 0 && bx < sd.stamp_w;
 #pragma unroll
@@ -239,17 +273,32 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
             float src = 0.0f;
             if (in_stamp)  // YPUB:1458 wavelet*gc2d*dt/(dz**2)
                 src = __fdiv_rn(fm(fm(wav, __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz)), a.dt), a.dz2);
+            // fsbc: rows above the surface keep their values (calux / caluz start at itopo)
+            const bool below = !FS || gz + q >= a.zs;
+            const bool zero_zz = FS && gz + q <= a.zs;  // YPUB:978-1007, rows <= itopo
             // YPRI:331-338: strxx parts, sponge spg1xn/spg2xp, spgzn/spgzp, then the source
-            float s0 = xs(fa(cmp(v[0], q), fm(fm(a.dtdx, cmp(lm2, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-            const float s1 = xs(fa(cmp(v[1], q), fm(fm(a.dtdz, cmp(lam, q)), cmp(d2, q))), zq, nz, a.npz, tb + 2 * st, tb + 3 * st);
-            if (in_stamp) s0 = fa(src, s0);
-            // YPRI:342-349: strzz parts
-            float s2 = xs(fa(cmp(v[2], q), fm(fm(a.dtdx, cmp(lam, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-            const float s3 = xs(fa(cmp(v[3], q), fm(fm(a.dtdz, cmp(lm2, q)), cmp(d2, q))), zq, nz, a.npz, tb + 2 * st, tb + 3 * st);
+            float s0 = cmp(v[0], q), s1 = cmp(v[1], q), s2 = cmp(v[2], q), s3 = cmp(v[3], q);
+            float s4 = cmp(v[4], q), s5 = cmp(v[5], q);
+            if (below) {
+                s0 = xs(fa(s0, fm(fm(a.dtdx, cmp(lm2, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
+                s1 = fa(s1, fm(fm(a.dtdz, cmp(lam, q)), cmp(d2, q)));
+            }
+            s1 = zsp<FS>(s1, zq, a, tb + 2 * st, tb + 3 * st);
+            if (in_stamp && src_xx) s0 = fa(src, s0);
+            // YPRI:342-349: strzz parts; fsbc: zero on rows <= the surface before the source
+            if (below) {
+                s2 = xs(fa(s2, fm(fm(a.dtdx, cmp(lam, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
+                s3 = fa(s3, fm(fm(a.dtdz, cmp(lm2, q)), cmp(d2, q)));
+            }
+            s3 = zsp<FS>(s3, zq, a, tb + 2 * st, tb + 3 * st);
+            if (zero_zz) s2 = s3 = 0.0f;
             if (in_stamp) s2 = fa(src, s2);
             // YPRI:353-359: strxz parts, sponge spgxn/spgxp, spg1zn/spg2zp
-            const float s4 = xs(fa(cmp(v[4], q), fm(fm(a.dtdx, cmp(mue, q)), cmp(d3, q))), gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
-            const float s5 = xs(fa(cmp(v[5], q), fm(fm(a.dtdz, cmp(mue, q)), cmp(d4, q))), zq, nz, a.npz, tb + 6 * st, tb + 7 * st);
+            if (below) {
+                s4 = xs(fa(s4, fm(fm(a.dtdx, cmp(mue, q)), cmp(d3, q))), gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
+                s5 = fa(s5, fm(fm(a.dtdz, cmp(mue, q)), cmp(d4, q)));
+            }
+            s5 = zsp<FS>(s5, zq, a, tb + 6 * st, tb + 7 * st);
             cmpr(v[0], q) = s0; cmpr(v[1], q) = s1; cmpr(v[2], q) = s2;
             cmpr(v[3], q) = s3; cmpr(v[4], q) = s4; cmpr(v[5], q) = s5;
         }
@@ -266,6 +315,27 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
         const long long o = sd.rec_base + (long long)a.step * sd.nrec + ridx;
         a.records[o] = sVx[rr * SW + rz];
         a.records2[o] = sVz[rr * SW + rz];
+    }
+}
+
+// Free surface, after the stress kernel (one thread per column): the image strxz(zs - 1) =
+// -strxz(zs) of both split parts (YPUB:1009-1024), and vz(zs - 1) = vz(zs) + lambsg/lambmusg
+// (vx(zs, x + 1) - vx(zs, x)) for both pairs of split parts (YPUB:938-976, columns but the last).
+__global__ void iso_surface_kernel(const __grid_constant__ IArgs a) {
+    const int shot = a.slot_to_shot[blockIdx.y];
+    const ShotDev sd = a.shots[shot];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= sd.nx) return;
+    const int zs = a.zs;
+    const long long c = cell(a, shot, x, zs), cu = c - 1;
+    a.f[I_SXZX][cu] = -a.f[I_SXZX][c];
+    a.f[I_SXZZ][cu] = -a.f[I_SXZZ][c];
+    if (x + 1 < sd.nx) {
+        const long long cn = cell(a, shot, x + 1, zs);
+        const long long mi = (long long)min(sd.x0 + x, a.nx_model - 1) * a.mpitch + zs;
+        const float ratio = __fdiv_rn(__ldg(a.lam + mi), __ldg(a.lm2 + mi));
+        a.f[I_VZX][cu] = fa(a.f[I_VZX][c], fm(ratio, fs(a.f[I_VXX][cn], a.f[I_VXX][c])));
+        a.f[I_VZZ][cu] = fa(a.f[I_VZZ][c], fm(ratio, fs(a.f[I_VXZ][cn], a.f[I_VXZ][c])));
     }
 }
 
@@ -352,19 +422,29 @@ __global__ void __launch_bounds__(32) iso_smooth_kernel(const __grid_constant__ 
 
 }  // namespace
 
-cudaError_t elastic2d_launch_step(const IArgs& a, int active, cudaStream_t st) {
+cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaStream_t st, int* launches) {
     dim3 grid(a.L.ntx * a.L.ntz, active);
     const size_t smem = sizeof(float) * 3 * SMEM;
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(iso_velocity_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+        for (auto k : {iso_velocity_kernel<false>, iso_velocity_kernel<true>}) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
         attr = true;
     }
-    iso_velocity_kernel<<<grid, kThreads, smem, st>>>(a);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    iso_stress_kernel<<<grid, kThreads, 0, st>>>(a);
+    *launches = 2;
+    if (a.fs) {
+        iso_velocity_kernel<true><<<grid, kThreads, smem, st>>>(a);
+        iso_stress_kernel<true><<<grid, kThreads, 0, st>>>(a);
+        if (a.zs >= 1) {  // row zs - 1 exists in the grid
+            iso_surface_kernel<<<dim3((nx_max + 127) / 128, active), 128, 0, st>>>(a);
+            *launches = 3;
+        }
+    } else {
+        iso_velocity_kernel<false><<<grid, kThreads, smem, st>>>(a);
+        iso_stress_kernel<false><<<grid, kThreads, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 

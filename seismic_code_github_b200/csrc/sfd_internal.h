@@ -126,6 +126,9 @@ struct IArgs {
     int mpitch, nx_model;
     float dt, dtdx, dtdz, dz2;
     float a[5];
+    float cr[4][4];                       // M-term staggered coefficients, M = 1..4 (YMOD:7-20)
+    int fs;                               // 1: free surface (fsbc mode) at row zs, 0: abc mode
+    int zs;                               // surface row (0-based; the reference's itopo - 1)
     const float* spg;                     // spgxn spgxp spgzn' spgzp spg1xn spg2xp spg1zn' spg2zp
     int spg_stride;
     const ShotDev* shots;
@@ -138,7 +141,9 @@ struct IArgs {
     float* records2;                      // vz (record2)
     int step;
 };
-cudaError_t elastic2d_launch_step(const IArgs& a, int active, cudaStream_t st);
+// One step: the velocity and stress kernels, and in fsbc mode with zs >= 1 the surface kernel
+// (YPUB:938-976 calfsbcv, YPUB:1009-1024 calfsbcstrxz); *launches receives the kernel count.
+cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaStream_t st, int* launches);
 // YPUB:323-547 on one window (x-major, z fastest): substagger and the refill of the rows above
 // itopo (0-based rows < itopo - 1 take row itopo - 1); out: busg2e, busg1e, lambmusg, lambsg, musge.
 // Returns false on a zero density (YPUB:370, 400).

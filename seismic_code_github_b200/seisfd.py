@@ -93,6 +93,7 @@ SIGNATURES = {
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "sfd_set_gauss_radius": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sfd_set_free_surface": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "sfd_set_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int]),
@@ -331,6 +332,11 @@ class Engine:
         """Half-width of the source / top-sponge Gaussian of the isotropic elastic scheme
         (YPUB:1470-1501; default 50)."""
         self._check(self._lib.sfd_set_gauss_radius(self._h, int(rgau)), "sfd_set_gauss_radius")
+
+    def set_free_surface(self, top: int):
+        """Boundary mode of the isotropic elastic scheme: 0 = absorbing on all sides ('abc'),
+        top >= 1 = free surface at padded row top - 1 ('fsbc', the reference's itopo = top)."""
+        self._check(self._lib.sfd_set_free_surface(self._h, int(top)), "sfd_set_free_surface")
 
     def set_memory_limit(self, nbytes: int):
         """Device-memory budget of gradient() (0: the free device memory)."""

@@ -1,5 +1,5 @@
-"""GPU isotropic elastic path (SFD_ELASTIC_2D: the abc mode of forward/yang_version_2016_2_2,
-flat surface) through the C ABI, against the FP32 restatement of the Fortran code
+"""GPU isotropic elastic path (SFD_ELASTIC_2D: the abc and fsbc modes of
+forward/yang_version_2016_2_2, flat surface) through the C ABI, against the FP32 restatement of the Fortran code
 (oracle/iso_oracle.cpp).  The kernels keep the reference's split fields and operation order and
 the top-sponge smoothing runs in the serial order, so both record sets (record1 = vx,
 record2 = vz, YPRI:361-367) must be bit-identical to the restatement; the FP64 restatement gives
@@ -137,3 +137,62 @@ def test_quality_factors_rejected():
     with S.Engine(S.ELASTIC_2D, vp.shape[0], vp.shape[1], 10.0, 10.0, 5e-4, 8, order=10, f0=20.0) as e:
         with pytest.raises(RuntimeError):
             e.set_model_elastic(vp, vs, rho, qp=np.full_like(vp, 50.0))
+
+
+def run_fs(model, npx, top, f0, dt, dx, spec, per_shot=False, mode_flips=False):
+    """fsbc mode: the model padded with `top` rows above (free surface at padded row top - 1)."""
+    vp, vs, rho = (S.pad_model(a, npx, npx, top, npx) for a in model)
+    nx, nz = vp.shape
+    e = S.Engine(S.ELASTIC_2D, nx, nz, dx, dx, dt, npx, order=10, f0=f0)
+    e.set_gauss_radius(20)
+    if mode_flips:  # abc first: the model is prepared twice, the last preparation must win
+        e.set_model_elastic(vp, vs, rho)
+    e.set_free_surface(top)
+    e.set_model_elastic(vp, vs, rho)
+    shots = []
+    for isxe, isze, ntot, nrz0, idecay in spec:
+        rx = np.arange(npx, nx - npx, dtype=np.int32)
+        rz = np.full_like(rx, top + nrz0 - 1)
+        shots.append(S.ShotSpec(isxe - 1, isze - 1, rx, rz, S.wavelet(S.WAVELET_ISO, ntot, dt, f0, delay=idecay)))
+    e.set_shots(shots)
+    r1 = e.forward_per_shot() if per_shot else e.forward()
+    r2 = e.records(S.FIELD_VZ)
+    out = e.split_records(r1), e.split_records(r2), e.timing()
+    vx = e.wavefield(0, S.FIELD_VX)
+    e.close()
+    return out + (vx,)
+
+
+@pytest.mark.parametrize("top,src_depth", [(1, 6), (4, 6), (4, 0)])
+def test_free_surface_bitexact_against_restatement(top, src_depth):
+    # top = 1: the surface is the first row (the image rows fall outside the grid); top = 4: three
+    # air rows, the surface kernel writes row top - 2; src_depth 0: the source on the surface
+    # row, which skips strxx (YPRI:163-168)
+    model = imodel(seed=8, nx=70, nz=50)
+    npx, f0, dt, dx, nt, idecay = 10, 20.0, 5e-4, 10.0, 200, 40
+    isxe, isze, nrz0 = npx + 30, top + src_depth, 2
+    r1, r2, t, vx = run_fs(model, npx, top, f0, dt, dx, [(isxe, isze, nt + idecay, nrz0, idecay)], mode_flips=True)
+    kw = dict(nrz0=nrz0, idecay=idecay, rgau=20, fsbc=True, npz_top=top)
+    o1, o2, fin = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, isxe, isze, want_final=True, **kw)
+    d1, d2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt, npx, npx, isxe, isze, fp64=True, **kw)
+    g1, g2 = r1[0][:, idecay:], r2[0][:, idecay:]
+    print(f"top {top} src {src_depth}: vx relL2 vs FP64 {rel_l2(g1, d1):.2e}, vz {rel_l2(g2, d2):.2e}; "
+          f"{t['launches']} launches")
+    assert np.abs(g2).max() > 0
+    assert bits_equal(g1, o1) and bits_equal(g2, o2)
+    assert bits_equal(vx, fin)
+    steps = nt + idecay
+    assert t["launches"] == steps * (3 if top >= 2 else 2) + 2  # + the two record transposes
+
+
+def test_free_surface_batched_equals_per_shot():
+    model = imodel(seed=9, nx=80, nz=44, vs_ratio=1.7)
+    npx, top, f0, dt, dx = 10, 3, 25.0, 5e-4, 10.0
+    spec = [(npx + 12, top + 3, 140, 1, 30), (npx + 60, top + 9, 90, 3, 20), (npx + 40, top + 1, 120, 2, 40)]
+    b1, b2, _, _ = run_fs(model, npx, top, f0, dt, dx, spec)
+    p1, p2, _, _ = run_fs(model, npx, top, f0, dt, dx, spec, per_shot=True)
+    for i, (isxe, isze, nt, nrz0, idecay) in enumerate(spec):
+        assert bits_equal(b1[i], p1[i]) and bits_equal(b2[i], p2[i]), i
+        o1, o2, _ = ol.iso_forward(*model, dx, dx, dt, f0, nt - idecay, npx, npx, isxe, isze, nrz0=nrz0,
+                                   idecay=idecay, rgau=20, fsbc=True, npz_top=top)
+        assert bits_equal(b1[i][:, idecay:], o1) and bits_equal(b2[i][:, idecay:], o2), i

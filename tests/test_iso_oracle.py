@@ -175,3 +175,23 @@ def test_zero_density_rejected():
     rho[3, 3] = 0.0
     with pytest.raises(ValueError):
         ol.iso_forward(vp, vs, rho, 10.0, 10.0, 1e-3, 20.0, 10, 4, 4, isxe=8, isze=6, rgau=3)
+
+
+def test_free_surface_stable_and_close_to_fp64():
+    """fsbc mode (YPRI:57-230): the restated free surface stays stable over a long record and
+    agrees with its FP64 restatement; before the direct wave reaches the surface the records
+    match the abc mode's to FP32 round-off."""
+    nx, nz = 100, 90
+    vp = np.full((nx, nz), 3000.0, F)
+    vs = (vp / 1.732).astype(F)
+    rho = np.full((nx, nz), 2000.0, F)
+    kw = dict(dx=10.0, dz=10.0, dt=1e-3, f0=20.0, npx=15, npz=15, isxe=15 + 50, nrz0=2, idecay=60, rgau=20)
+    for top in (1, 4):
+        f1, f2, _ = ol.iso_forward(vp, vs, rho, nt=2000, isze=top + 40, npz_top=top, fsbc=True, **kw)
+        peaks = [np.abs(f2[:, i:i + 250]).max() for i in range(0, 2000, 250)]
+        assert peaks[-1] < 1e-4 * peaks[0], peaks
+        d1, d2, _ = ol.iso_forward(vp, vs, rho, nt=300, isze=top + 40, npz_top=top, fsbc=True, fp64=True, **kw)
+        assert rel_l2(f1[:, :300], d1) <= 1e-5 and rel_l2(f2[:, :300], d2) <= 1e-5
+        a1, a2, _ = ol.iso_forward(vp, vs, rho, nt=300, isze=top + 40, npz_top=top, **kw)
+        early = 40  # 40 samples after the Ricker peak: the wave is still 25 cells below the surface
+        assert np.abs(f2[:, :early] - a2[:, :early]).max() <= 1e-5 * np.abs(f2).max()
