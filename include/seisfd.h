@@ -10,6 +10,8 @@
  *   forward/Q_forward/Q_multishot_fd_subroutine_fsbc_zy_rotated.f90         (QS)
  *   tools/ricker.cpp                                                        (RIC)
  *   forward/yang_version_2016_2_2/Iso_multishot_fd_subroutine_fsbc_zy_m2_{pub,pri}.f90 (YPUB, YPRI)
+ *   forward/yang_version_2016_2_2/Iso_multishot_fd_main_fsbc_zy_m2.f90                 (YM)
+ *   forward/yang_version_2016_2_2/Iso_multishot_fd_module_zy_m2.f90                    (YMOD)
  *
  * Conventions (the reference's in-memory and file layouts):
  *   - grids are x-major with z fastest: a[x * nz + z] (AFD:51-100 `P[i][j]`, i = x, j = z;
@@ -148,7 +150,7 @@ int sfd_set_model_elastic(sfd_ctx* ctx, const float* vp, const float* vs, const 
  * smooth"; default 50).  Re-prepares the model and the source stamps if they are set. */
 int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau);
 
-/* Boundary mode of SFD_ELASTIC_2D (YPRI:190-219 `molmod`).  top = 0: 'abc', the cosine sponge on
+/* Boundary mode of SFD_ELASTIC_2D (YM:190-219 `molmod`).  top = 0: 'abc', the cosine sponge on
  * all four sides with the top sponge's moduli smoothed (YPRI:234-386; the default).  top >= 1:
  * 'fsbc', a flat free surface at padded row top - 1 (the reference's itopo = npzn = top,
  * YPRI:57-230): no top sponge, lower-order z derivatives on the five rows below the surface,
@@ -216,12 +218,13 @@ int sfd_get_timing(const sfd_ctx* ctx, sfd_timing* out);
 /* Wavefield snapshots taken inside the forward time loop.  Replaces the Snap.dat / Pall.dat
  * writes of AFD:343-373 and the snapshot files of QM:462-481.  Stream id (0..3) records, after
  * every step k (0-based) with k >= first and (k - first) % every == 0, at most `count` times per
- * shot, the interior (pml <= x < nx_shot - pml, pml <= z < nz - pml) of `field` as the reference
+ * shot, the interior (pml <= x < nx_shot - pml, top <= z < nz - pml; top = pml, or the row
+ * given to sfd_set_free_surface) of `field` as the reference
  * holds it after the step: SFD_FIELD_P (AFD P1 / QS strxx), SFD_FIELD_VX, SFD_FIELD_VZ, and
  * SFD_FIELD_R for the viscoacoustic scheme.  count = 0 removes the stream.  2-D schemes only. */
 int sfd_set_snapshots(sfd_ctx* ctx, int id, int field, int first, int every, int count);
 /* The snapshots of stream id for one shot from the last forward: n x (nx_shot - 2 pml) x
- * (nz - 2 pml) floats, x-major, z fastest; *n_out receives n.  out may be NULL to query n. */
+ * (nz - top - pml) floats, x-major, z fastest; *n_out receives n.  out may be NULL to query n. */
 int sfd_get_snapshots(sfd_ctx* ctx, int id, int shot, float* out, int* n_out);
 
 /* Single-shot 2-D acoustic forward that allocates no device memory.  No counterpart in the
@@ -269,6 +272,26 @@ typedef struct {
     int fdo2, fdo1;
 } sfd_qpar;
 int sfd_qpar_read(const char* path, sfd_qpar* out);
+/* yang_version parameter card (YPUB:48-145): pairs of a label line and a value line, in this
+ * order.  dtsnap: snapshot interval (s); decay: source delay (s), nint(decay/dt) steps before the
+ * first recorded sample; rgau: Gaussian half-width (cells). */
+typedef struct {
+    char molmod[16];                                       /* "abc" or "fsbc" (YM:190-219)     */
+    char vp[256], vs[256], rho[256], topo[256];            /* model files; topo: nx surface depths (m) */
+    char snapx[256], snapz[256];                           /* vx / vz snapshot file prefixes     */
+    char shot1[256], shot2[256], shot3[256], shot4[256];   /* vx parts / vx merged / vz parts / vz merged */
+    int nshot;
+    float offset_min, offset_max;
+    float sx0, sz0, rz0;
+    float dsx;
+    int nx, nz;
+    float dx, dz;
+    int nt;
+    float dt, dtsnap, f0, decay;
+    float pml_xn, pml_xp, pml_zn, pml_zp;                  /* sponge thickness (m)               */
+    int rgau;
+} sfd_isopar;
+int sfd_isopar_read(const char* path, sfd_isopar* out);
 /* Raw little-endian float32 files: models (x-major, z fastest: QS:238-284, tools/get_vel_model.cpp:
  * 50-58), AFD's record / snapshot outputs (AFD:343-393).  append = 1 opens for appending. */
 int sfd_read_floats(const char* path, long long n, float* out);
@@ -279,6 +302,11 @@ int sfd_write_floats(const char* path, const float* data, long long n, int appen
  * Fortran), followed by the trace's nt float32 samples.  traces: [ntr][nt]. */
 int sfd_su_write(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
                  float dt);
+/* The same with header options: SFD_SU_CDP sets cdp as QS:1535 does; yang_version's writer
+ * (YPUB:1533-1604) leaves it 0. */
+#define SFD_SU_CDP 0x1
+int sfd_su_write_ex(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
+                    float dt, int flags);
 /* Concatenate per-shot SU files in order (QS:1550-1624); delete_inputs = 1 removes them as the
  * reference does. */
 int sfd_su_merge(const char* out_path, const char* const* in_paths, int n, int delete_inputs);

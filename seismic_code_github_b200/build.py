@@ -30,7 +30,7 @@ LIB_SOURCES = ["api.cu", "acoustic2d.cu", "acoustic2d_fma.cu", "adjoint2d.cu", "
                "helpers.cpp", "noalloc.cu", "acoustic3d.cu", "snapshots.cu",
                "fileio.cpp"]
 OPTIONAL_SOURCES = []
-PROGRAMS = {"afd_fd": "cli_afd.cpp", "q_forward": "cli_qforward.cpp"}
+PROGRAMS = {"afd_fd": "cli_afd.cpp", "q_forward": "cli_qforward.cpp", "iso_forward": "cli_isoforward.cpp"}
 
 
 def _sources():

@@ -492,12 +492,17 @@ IArgs make_iargs(const sfd_ctx* c, int step) {
     return a;
 }
 
+// First row of the snapshot interior: the top pad (pml; the free surface's pad in fsbc mode).
+int snap_top(const sfd_ctx* ctx) {
+    return (ctx->g.scheme == SFD_ELASTIC_2D && ctx->iso_top > 0) ? ctx->iso_top : ctx->g.pml;
+}
+
 // Size the snapshot buffers for the current shot set; returns true if a buffer moved (the
 // captured time loop holds their addresses).
 bool snap_prepare(sfd_ctx* ctx, int* rc) {
     *rc = SFD_OK;
     bool moved = false;
-    const int pml = ctx->g.pml, nzi = ctx->g.nz - 2 * pml;
+    const int pml = ctx->g.pml, nzi = ctx->g.nz - snap_top(ctx) - pml;
     for (auto& sn : ctx->snaps) {
         sn.ready = false;
         if (sn.count <= 0) continue;
@@ -578,6 +583,7 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         s.L = ctx->L;
         s.nz = ctx->g.nz;
         s.pml = ctx->g.pml;
+        s.ztop = snap_top(ctx);
         s.shots = ctx->d_shots;
         s.slot_to_shot = slots;
         s.step = k;
@@ -2357,6 +2363,7 @@ int sfd_set_free_surface(sfd_ctx* ctx, int top) {
     CK(cudaSetDevice(ctx->device));
     ctx->iso_top = top;
     ctx->graph_valid = false;
+    for (auto& sn : ctx->snaps) sn.ready = false;  // the snapshot interior starts at the new top
     return q_prepare(ctx);  // substagger's refill row and the smoothing follow the mode
 }
 
@@ -2441,8 +2448,8 @@ int sfd_get_snapshots(sfd_ctx* ctx, int id, int shot, float* out, int* n_out) {
     if (n_out) *n_out = sn.taken[shot];
     if (out && sn.taken[shot] > 0) {
         CK(cudaSetDevice(ctx->device));
-        const long long n =
-            (long long)sn.taken[shot] * (ctx->h_shots[shot].nx - 2 * ctx->g.pml) * (ctx->g.nz - 2 * ctx->g.pml);
+        const long long n = (long long)sn.taken[shot] * (ctx->h_shots[shot].nx - 2 * ctx->g.pml) *
+                            (ctx->g.nz - snap_top(ctx) - ctx->g.pml);
         CK(cudaMemcpy(out, sn.d_buf + sn.off[shot], sizeof(float) * n, cudaMemcpyDeviceToHost));
     }
     return SFD_OK;

@@ -1,5 +1,5 @@
-// The reference programs' file contract: the Q_forward parameter card, binary model files and
-// the SU shot records with their merge step.  Used by the afd_fd / q_forward programs and
+// The reference programs' file contract: the Q_forward and yang_version parameter cards, binary
+// model files and the SU shot records with their merge step.  Used by the afd_fd / q_forward programs and
 // exported through the C ABI so that other callers can read and write the same files.
 #include <cerrno>
 #include <cmath>
@@ -130,6 +130,70 @@ int sfd_qpar_read(const char* path, sfd_qpar* p) {
     return SFD_OK;
 }
 
+int sfd_isopar_read(const char* path, sfd_isopar* p) {
+    if (!path || !p) return SFD_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SFD_ERR_IO;
+    std::memset(p, 0, sizeof(*p));
+    std::string label, line;
+    // YPUB:94-115: the mode, ten file names, then the numeric cards, each after one label line
+    int rc = SFD_OK;
+    if (!read_line(f, &label) || !read_line(f, &line)) rc = SFD_ERR_IO;
+    else std::snprintf(p->molmod, sizeof(p->molmod), "%s", strip(line).c_str());
+    char* names[10] = {p->vp, p->vs, p->rho, p->topo, p->snapx, p->snapz, p->shot1, p->shot2, p->shot3, p->shot4};
+    for (int i = 0; i < 10 && rc == SFD_OK; i++) {
+        if (!read_line(f, &label) || !read_line(f, &line)) rc = SFD_ERR_IO;
+        else std::snprintf(names[i], sizeof(p->vp), "%s", strip(line).c_str());
+    }
+    struct Card {
+        int n;
+        double* d[3];
+    };
+    double nshot, omin, omax, sx0, sz0, rz0, dsx, nx, nz, dx, dz, nt, dt, dtsnap, f0, decay, pxn, pxp, pzn, pzp, rgau;
+    // YPUB:116-141
+    const Card cards[] = {{1, {&nshot}},      {2, {&omin, &omax}}, {3, {&sx0, &sz0, &rz0}}, {1, {&dsx}},
+                          {2, {&nx, &nz}},    {2, {&dx, &dz}},     {1, {&nt}},             {2, {&dt, &dtsnap}},
+                          {1, {&f0}},         {1, {&decay}},       {2, {&pxn, &pxp}},      {2, {&pzn, &pzp}},
+                          {1, {&rgau}}};
+    for (const Card& c : cards) {
+        if (rc != SFD_OK) break;
+        if (!read_line(f, &label) || !read_line(f, &line)) {
+            rc = SFD_ERR_IO;
+            break;
+        }
+        const std::vector<double> v = numbers(line);
+        if ((int)v.size() < c.n) {
+            rc = SFD_ERR_ARG;
+            break;
+        }
+        for (int i = 0; i < c.n; i++) *c.d[i] = v[i];
+    }
+    std::fclose(f);
+    if (rc != SFD_OK) return rc;
+    p->nshot = (int)nshot;
+    p->offset_min = (float)omin;
+    p->offset_max = (float)omax;
+    p->sx0 = (float)sx0;
+    p->sz0 = (float)sz0;
+    p->rz0 = (float)rz0;
+    p->dsx = (float)dsx;
+    p->nx = (int)nx;
+    p->nz = (int)nz;
+    p->dx = (float)dx;
+    p->dz = (float)dz;
+    p->nt = (int)nt;
+    p->dt = (float)dt;
+    p->dtsnap = (float)dtsnap;
+    p->f0 = (float)f0;
+    p->decay = (float)decay;
+    p->pml_xn = (float)pxn;
+    p->pml_xp = (float)pxp;
+    p->pml_zn = (float)pzn;
+    p->pml_zp = (float)pzp;
+    p->rgau = (int)rgau;
+    return SFD_OK;
+}
+
 int sfd_read_floats(const char* path, long long n, float* out) {
     if (!path || !out || n < 0) return SFD_ERR_ARG;
     FILE* f = std::fopen(path, "rb");
@@ -150,6 +214,11 @@ int sfd_write_floats(const char* path, const float* data, long long n, int appen
 
 int sfd_su_write(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
                  float dt) {
+    return sfd_su_write_ex(path, traces, ntr, nt, shot_no, isx, ixmin, dx, dt, SFD_SU_CDP);
+}
+
+int sfd_su_write_ex(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
+                    float dt, int flags) {
     if (!path || (!traces && ntr > 0) || ntr < 0 || nt < 1 || nt > 32767 || !(dx > 0) || !(dt > 0))
         return SFD_ERR_ARG;
     FILE* f = std::fopen(path, "wb");
@@ -169,7 +238,7 @@ int sfd_su_write(const char* path, const float* traces, int ntr, int nt, int sho
         const int gx = (int)((float)(ixmin - 1 + i - 1) * dx);
         put32(h, 80, gx);                                            // gx
         put32(h, 36, gx - sx);                                       // offset
-        put32(h, 20, (int)std::lround((float)(gx + sx) / dx) + 1);   // cdp
+        if (flags & SFD_SU_CDP) put32(h, 20, (int)std::lround((float)(gx + sx) / dx) + 1);  // cdp
         if (std::fwrite(h, 1, 240, f) != 240 ||
             std::fwrite(traces + (size_t)(i - 1) * nt, sizeof(float), (size_t)nt, f) != (size_t)nt)
             rc = SFD_ERR_IO;

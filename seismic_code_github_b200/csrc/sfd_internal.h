@@ -306,11 +306,12 @@ struct SnapArgs {
     int nsum;
     Layout2D L;
     int nz, pml;
+    int ztop;                   // first interior row (pml; the free surface's top pad in fsbc mode)
     const ShotDev* shots;
     const int* slot_to_shot;
     const float* src_pre;       // acoustic P: value at the source cell before the next injection
     int step, index;            // step just completed, snapshot number
-    float* out;                 // per shot at shot_off[shot]: [snapshot][nx_shot - 2 pml][nz - 2 pml]
+    float* out;                 // per shot at shot_off[shot]: [snapshot][nx_shot - 2 pml][nz - ztop - pml]
     const long long* shot_off;
 };
 cudaError_t launch_snapshot(const SnapArgs& a, int active, int nx_max, cudaStream_t st);

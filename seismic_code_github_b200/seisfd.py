@@ -52,9 +52,36 @@ def read_qpar(path: str) -> QPar:
     return p
 
 
-def su_write(path: str, traces: np.ndarray, shot_no: int, isx: int, ixmin: int, dx: float, dt: float):
+class IsoPar(ctypes.Structure):
+    """sfd_isopar: the yang_version parameter card."""
+    _fields_ = [("molmod", ctypes.c_char * 16)] + \
+               [(n, ctypes.c_char * 256) for n in ("vp", "vs", "rho", "topo", "snapx", "snapz", "shot1", "shot2",
+                                                   "shot3", "shot4")] + \
+               [("nshot", ctypes.c_int), ("offset_min", ctypes.c_float), ("offset_max", ctypes.c_float),
+                ("sx0", ctypes.c_float), ("sz0", ctypes.c_float), ("rz0", ctypes.c_float), ("dsx", ctypes.c_float),
+                ("nx", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
+                ("nt", ctypes.c_int), ("dt", ctypes.c_float), ("dtsnap", ctypes.c_float), ("f0", ctypes.c_float),
+                ("decay", ctypes.c_float), ("pml_xn", ctypes.c_float), ("pml_xp", ctypes.c_float),
+                ("pml_zn", ctypes.c_float), ("pml_zp", ctypes.c_float), ("rgau", ctypes.c_int)]
+
+
+def read_isopar(path: str) -> IsoPar:
+    p = IsoPar()
+    rc = load().sfd_isopar_read(path.encode(), ctypes.byref(p))
+    if rc:
+        raise SfdError(rc, f"sfd_isopar_read({path})")
+    return p
+
+
+SU_CDP = 0x1
+
+
+def su_write(path: str, traces: np.ndarray, shot_no: int, isx: int, ixmin: int, dx: float, dt: float,
+             flags: int = SU_CDP):
+    """One shot's SU file; flags = SU_CDP sets the cdp header word as QS does, 0 leaves it 0 as
+    the yang_version writer does."""
     tr = np.ascontiguousarray(traces, np.float32)
-    rc = load().sfd_su_write(path.encode(), _fp(tr), tr.shape[0], tr.shape[1], shot_no, isx, ixmin, dx, dt)
+    rc = load().sfd_su_write_ex(path.encode(), _fp(tr), tr.shape[0], tr.shape[1], shot_no, isx, ixmin, dx, dt, flags)
     if rc:
         raise SfdError(rc, f"sfd_su_write({path})")
 
@@ -103,10 +130,13 @@ SIGNATURES = {
                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I32P, _I32P,
                                            ctypes.c_void_p, ctypes.c_void_p]),
     "sfd_qpar_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p]),
+    "sfd_isopar_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p]),
     "sfd_read_floats": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong, _F32P]),
     "sfd_write_floats": (ctypes.c_int, [ctypes.c_char_p, _F32P, ctypes.c_longlong, ctypes.c_int]),
     "sfd_su_write": (ctypes.c_int, [ctypes.c_char_p, _F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_float, ctypes.c_float]),
+    "sfd_su_write_ex": (ctypes.c_int, [ctypes.c_char_p, _F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int]),
     "sfd_su_merge": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int]),
     "sfd_wavelet": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _F32P]),
     "sfd_afd_sponge": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P]),

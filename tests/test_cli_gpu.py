@@ -163,3 +163,63 @@ def test_snapshots_equal_truncated_runs_viscoacoustic():
                 e.forward()
                 full = e.wavefield(0, field)
             assert bits_equal(snap, full[npx:-npx, npx:-npx]), (field, k)
+
+
+@pytest.mark.parametrize("mode", ["abc", "fsbc"])
+def test_iso_forward_program_against_restatement(tmp_path, mode):
+    """iso_forward on a yang_version card of three aperture shots: the merged SU files hold the
+    FP32 restatement's vx / vz traces bit for bit, with YPUB:1555-1596's headers (no cdp); the
+    last snapshot of the last shot equals the restatement's wavefield after that step."""
+    from test_fileio import ISOCARD
+    nx, nz = 120, 80
+    rng = np.random.default_rng(12)
+    z = np.arange(nz)
+    vp = np.tile(np.where(z < 40, 2000.0, 2700.0), (nx, 1)).astype(np.float32)
+    vp += rng.uniform(-50, 50, vp.shape).astype(np.float32)
+    vs = (vp / 1.8).astype(np.float32)
+    rho = (2000.0 + 300.0 * rng.random((nx, nz))).astype(np.float32)
+    for name, a in (("vp", vp), ("vs", vs), ("rho", rho)):
+        a.tofile(tmp_path / f"{name}.bin")
+    np.zeros(nx, np.float32).tofile(tmp_path / "topo.bin")
+    (tmp_path / "snap").mkdir()
+    card = ISOCARD.format(d=str(tmp_path), mode=mode, ztop="90.0" if mode == "abc" else "0000.0", rgau=12)
+    (tmp_path / "iso.par").write_text(card)
+    p = S.read_isopar(str(tmp_path / "iso.par"))
+    run([os.path.join(BIN, "iso_forward"), str(tmp_path / "iso.par"), "--snapshots", str(tmp_path / "snap")],
+        cwd=tmp_path)
+    nint = lambda v: int(np.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
+    np_ = nint(p.pml_xn / p.dx) + 1
+    top = nint(p.pml_zn / p.dz) + 1
+    isx0, isz0, irz0 = nint(p.sx0 / p.dx) + 1, nint(p.sz0 / p.dz) + 1, nint(p.rz0 / p.dz) + 1
+    idecay, idtsnap = nint(p.decay / p.dt), nint(p.dtsnap / p.dt)
+    fs = mode == "fsbc"
+    kw = dict(nrz0=irz0, idecay=idecay, rgau=p.rgau, fsbc=fs, npz_top=top)
+    refs = []
+    for i in range(1, p.nshot + 1):
+        isx = isx0 + nint((i - 1) * p.dsx / p.dx)
+        ixmine, ixmaxe = isx + nint(p.offset_min / p.dx), isx + nint(p.offset_max / p.dx)
+        args = (vp, vs, rho, p.dx, p.dz, p.dt, p.f0)
+        r1, r2, _ = ol.iso_forward(*args, p.nt, np_, np_, isx - ixmine + np_ + 1, isz0 + top, ixmine=ixmine,
+                                   ixmaxe=ixmaxe, **kw)
+        refs.append((isx, ixmine, ixmaxe - ixmine + 1, r1, r2))
+    for stem, which in (("vx", 3), ("vz", 4)):
+        assert not (tmp_path / f"{stem}_tmp1.su").exists()
+        raw = open(tmp_path / f"shot_{stem}.su", "rb").read()
+        off = 0
+        for i, ref in enumerate(refs, start=1):
+            isx, ixmine, nxe = ref[:3]
+            for t in range(nxe):
+                rec = raw[off:off + 240 + 4 * p.nt]
+                off += 240 + 4 * p.nt
+                want = bytearray(expected_header(i, isx, ixmine, p.dx, p.dt, p.nt, t + 1))
+                want[20:24] = b"\0\0\0\0"
+                assert rec[:240] == bytes(want)
+                assert bits_equal(np.frombuffer(rec[240:], np.float32), ref[which][t]), (stem, i, t)
+        assert off == len(raw)
+    # snapshots of the last shot: vx after step it = k * idtsnap (YPRI:212-224)
+    isx, ixmine, nxe = refs[-1][:3]
+    last = idtsnap * ((p.nt + idecay) // idtsnap)
+    snap = read(tmp_path / "snap" / f"vx_{last}", (nxe, nz))
+    _, _, fin = ol.iso_forward(vp, vs, rho, p.dx, p.dz, p.dt, p.f0, last - idecay, np_, np_, isx - ixmine + np_ + 1,
+                               isz0 + top, ixmine=ixmine, ixmaxe=ixmine + nxe - 1, want_final=True, **kw)
+    assert bits_equal(snap, fin[np_:np_ + nxe, top:top + nz])

@@ -1,6 +1,7 @@
 """CPU checks of the file contract helpers (seismic_code_github_b200/csrc/fileio.cpp): the
-Q_forward parameter card reader (QS:121-234), the SU shot writer (QS:1476-1546), the merge
-(QS:1550-1624) and the raw float32 files.  The expected SU headers are built here from the
+Q_forward parameter card reader (QS:121-234), the yang_version card reader (YPUB:48-145), the SU
+shot writer (QS:1476-1546, and YPUB:1533-1604 without the cdp word), the merge (QS:1550-1624)
+and the raw float32 files.  The expected SU headers are built here from the
 Fortran statements of QS:1502-1533 with numpy float32 arithmetic."""
 import os
 import struct
@@ -148,6 +149,96 @@ def test_raw_float_files(tmp_path):
     assert lib.sfd_read_floats(p, 18, S._fp(np.empty(18, np.float32))) == S.ERR_IO
 
 
+ISOCARD = """!*Modeling mode:fsbc(free surface bc).or.abc(absorbing bc)*!
+{mode}
+!*P-wave velocity filename*!
+{d}/vp.bin
+!*S-wave velocity filename*!
+{d}/vs.bin
+!*Density velocity filename*!
+{d}/rho.bin
+!*Topography velocity filename*!
+{d}/topo.bin
+!*Vx snapshot  filename*!
+{d}/snap/vx_
+!*Vz snapshot filename*!
+{d}/snap/vz_
+!*NO.1 shot record filename(tmp)*!
+{d}/vx_tmp
+!*NO.2 shot record filename(all)*!
+{d}/shot_vx
+!*NO.3 shot record filename(tmp)*!
+{d}/vz_tmp
+!*NO.4 shot record filename(all)*!
+{d}/shot_vz
+!*nshot(samples)*!
+3
+!*offset_min,offset_max*!
+-150.0  250.0
+!*sx0,sz0,rz0(m)*!
+200.0 30.0 10.0
+!*dsx(m)*!
+50.0
+!*nx_v,nz_v(samples)*!
+120 80
+!*dx_v,dz_v(m)*!
+10.0 10.0
+!*nt(samples)*!
+300
+!*dt(s),desnap(s)*!
+0.0005 0.025
+!*f0(Hz)*!
+20.0
+!*decay(s) recommending decay=(1.2/f0)s*!
+0.02
+!*pml_thick x left and right direction(m)*!
+90.0 90.0
+!*pml_thick z up and down direction(m)*!
+{ztop} 90.0
+!*rad of gauss smooth*!
+{rgau}
+"""
+
+
+def test_yang_parameter_card(tmp_path):
+    p = tmp_path / "iso.par"
+    p.write_text(ISOCARD.format(d=str(tmp_path), mode="fsbc", ztop="0000.0", rgau=12))
+    q = S.read_isopar(str(p))
+    assert q.molmod.decode() == "fsbc" and q.topo.decode() == f"{tmp_path}/topo.bin"
+    assert q.snapz.decode() == f"{tmp_path}/snap/vz_" and q.shot4.decode() == f"{tmp_path}/shot_vz"
+    assert (q.nshot, q.nx, q.nz, q.nt, q.rgau) == (3, 120, 80, 300, 12)
+    assert (q.offset_min, q.offset_max, q.sx0, q.sz0, q.rz0, q.dsx) == (-150.0, 250.0, 200.0, 30.0, 10.0, 50.0)
+    assert np.float32(q.dt) == np.float32(0.0005) and np.float32(q.dtsnap) == np.float32(0.025)
+    assert (q.f0, np.float32(q.decay)) == (20.0, np.float32(0.02))
+    assert (q.pml_xn, q.pml_xp, q.pml_zn, q.pml_zp) == (90.0, 90.0, 0.0, 90.0)
+
+
+def test_reference_yang_parameter_card():
+    """The card shipped with the reference (forward/yang_version_2016_2_2/iso_2d_modelling_sin_test.par)."""
+    path = "/root/reference/forward/yang_version_2016_2_2/iso_2d_modelling_sin_test.par"
+    if not os.path.exists(path):
+        pytest.skip("reference tree not present")
+    q = S.read_isopar(path)
+    assert q.molmod.decode() == "fsbc" and q.shot1.decode().endswith("/vx_tmp")
+    assert (q.nshot, q.nx, q.nz, q.nt, q.rgau) == (1, 501, 401, 3001, 50)
+    assert (q.offset_min, q.offset_max, q.sx0, q.dsx, q.dx, q.f0) == (-1250.0, 1250.0, 1250.0, 100.0, 5.0, 25.0)
+    assert np.float32(q.decay) == np.float32(0.048) and np.float32(q.dtsnap) == np.float32(0.01)
+    assert (q.pml_xn, q.pml_xp, q.pml_zn, q.pml_zp) == (1000.0, 1000.0, 0.0, 1000.0)
+
+
+def test_su_without_cdp(tmp_path):
+    nt, ntr = 21, 5
+    tr = np.random.default_rng(1).standard_normal((ntr, nt)).astype(np.float32)
+    path = str(tmp_path / "shot3.su")
+    S.su_write(path, tr, 3, 40, 12, 5.0, 0.001, flags=0)
+    raw = open(path, "rb").read()
+    for i in range(1, ntr + 1):
+        rec = raw[(i - 1) * (240 + 4 * nt):i * (240 + 4 * nt)]
+        want = bytearray(expected_header(3, 40, 12, 5.0, 0.001, nt, i))
+        want[20:24] = b"\0\0\0\0"  # YPUB:1555-1572 never sets cdp
+        assert rec[:240] == bytes(want), i
+
+
 def test_programs_are_built():
-    for name in ("afd_fd", "q_forward"):
+    for name in ("afd_fd", "q_forward", "iso_forward"):
         assert os.access(os.path.join(ROOT, "seismic_code_github_b200", "bin", name), os.X_OK)
