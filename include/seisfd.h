@@ -158,6 +158,16 @@ int sfd_set_gauss_radius(sfd_ctx* ctx, int rgau);
  * rows above the surface are air.  Re-prepares the model if it is set. */
 int sfd_set_free_surface(sfd_ctx* ctx, int top);
 
+/* Topography of SFD_ELASTIC_2D: itopo[x] for every padded model column x, the reference's 1-based
+ * surface row itopoe = nint(topo/dz) + npzn (YPUB:270-272); NULL restores the flat surface (pml in
+ * abc mode, the sfd_set_free_surface row in fsbc mode).  In abc mode column x is updated from
+ * padded row itopo[x] - pml - 1 down, with the top sponge on the pml + 1 rows from there
+ * (YPUB:1095-1407, 851-897), and itopo[x] >= pml; in fsbc mode the free surface lies at row
+ * itopo[x] - 1 of column x.  The smoothed rows (abc), the rows refilled by substagger and the
+ * source condition (YPRI:163-168) follow it; receivers are placed by the caller.  Re-prepares
+ * the model if it is set. */
+int sfd_set_topography(sfd_ctx* ctx, const int* itopo);
+
 /* Shots.  Replaces the shot loop QM:124-141 (one launch for all shots instead of one process
  * per shot).  Wavelets and receiver lists are copied; the caller keeps ownership. */
 int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots);

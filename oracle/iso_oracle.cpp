@@ -1,7 +1,7 @@
 // ORACLE -- test infrastructure only. CPU restatement of the reference's isotropic elastic
 // standard-staggered-grid modelling of one shot (forward/yang_version_2016_2_2, both modes:
-// 'abc', cosine sponge on all four sides, and 'fsbc', free surface on top) for a flat surface,
-// used by tests/ as the checker of the SFD_ELASTIC_2D GPU path.  The reference is Fortran 90 + MPI + OpenMP and cannot be compiled in
+// 'abc', cosine sponge on all four sides, and 'fsbc', free surface on top), flat or with
+// topography, used by tests/ as the checker of the SFD_ELASTIC_2D GPU path.  The reference is Fortran 90 + MPI + OpenMP and cannot be compiled in
 // this environment (no Fortran compiler), so this restatement is not pinned by a run of the
 // reference: "parity unpinned" for this scheme; it is checked by physics properties instead
 // (tests/test_iso_oracle.py).
@@ -28,9 +28,12 @@
 //   The free-surface velocity vz(itopo - 1) = vz(itopo) + lambda/(lambda + 2 mu) dx vx is written
 //   into the split parts after calu has summed them (YPRI:141-150), so the stress update reads
 //   it one step later.
-// The split fields also hold a row k = 0 (YPUB:1095 `ux(0:nz,nx)`, loops from itopo - npzn = 0);
-// calu and get_record never read it, so it is not kept here.  Fortran (k, i), k = z, i = x,
+// Topography: itopo(i) = nint(topo/dz) + npzn per window column (YPUB:270-272); every loop
+// bound, sponge row, surface row, the source condition and the receiver row follow it.
+// The split fields also hold a row k = 0 (YPUB:1095 `ux(0:nz,nx)`, abc loops from itopo - npzn,
+// which is 0 for a flat surface); calu and get_record never read it, so it is not kept here.  Fortran (k, i), k = z, i = x,
 // maps to C index (i-1)*nz + (k-1).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -57,7 +60,7 @@ struct IsoSolver {
     T dx, dz, dt;
     T a[5];
     bool fs = false;   // free surface (fsbc mode)
-    int itopo = 1;     // surface row (1-based), flat
+    std::vector<int> itopo;  // itopo(i), i = 1..nx: surface row (1-based) per column
     T cr[6][5] = {};   // cr[M]: coefficients of the M-term staggered derivative (YMOD:7-27)
     Field<T> vx, vz, sxx, szz, sxz;                                     // (-4:nz+5, -4:nx+5)
     Field<T> vxx, vxz, vzx, vzz, sxxx, sxxz, szzx, szzz, sxzx, sxzz;    // (1:nz, 1:nx)
@@ -82,33 +85,35 @@ struct IsoSolver {
         }
         return s;
     }
-    // terms of caluz's derivative at row k (YPUB:1160-1343): d = k - itopo from the surface
-    int zterms(int k, int flag) const {
+    // terms of caluz's derivative at row k of column i (YPUB:1160-1343): d rows below the surface
+    int zterms(int k, int i, int flag) const {
         if (!fs) return 5;
-        const int d = k - itopo;
+        const int d = k - itopo[i];
         return flag == 0 ? (d >= 5 ? 5 : (d < 1 ? 1 : d)) : (d >= 4 ? 5 : d + 1);
     }
-    // ux(k,i) = ux(k,i) + (dt/dh)*pa(k,i)*(...); fsbc: rows from itopo (calux / caluz)
+    // first updated row of column i: itopo (calux / caluz) or itopo - npzn (caluxabs /
+    // caluzabs; row 0 is not kept)
+    int krow(int i) const { return fs ? itopo[i] : std::max(itopo[i] - npzn, 1); }
+    // ux(k,i) = ux(k,i) + (dt/dh)*pa(k,i)*(...)
     void update(Field<T>& ux, const Field<T>& u, const Field<T>& pa, bool xdir, int flag) {
         const T c = xdir ? dt / dx : dt / dz;
-        const int k0 = fs ? itopo : 1;
 #pragma omp parallel for schedule(static)
         for (int i = 1; i <= nx; i++)
-            for (int k = k0; k <= nz; k++)
-                ux(k, i) = ux(k, i) + c * pa(k, i) * der(u, k, i, xdir, flag, xdir ? 5 : zterms(k, flag));
+            for (int k = krow(i); k <= nz; k++)
+                ux(k, i) = ux(k, i) + c * pa(k, i) * der(u, k, i, xdir, flag, xdir ? 5 : zterms(k, i, flag));
     }
-    // YPUB:851-897, flat surface (itopo(i) - npzn = 0); the top loop runs k = 0..npzn with
-    // factor spgzn(k + 1), of which rows 1..npzn are kept here
+    // YPUB:851-897: left and right from the first updated row; the top loop runs
+    // k = itopo - npzn .. itopo with factor spgzn(k - (itopo - npzn) + 1) (rows >= 1 kept here).
     // fsbc: YPUB:901-934 calpmlbclrb, left and right from row itopo, no top sponge
     void sponge(Field<T>& ux, Field<T>& uz, const std::vector<T>& sxn, const std::vector<T>& sxp,
                 const std::vector<T>& szn, const std::vector<T>& szp) {
-        const int k0 = fs ? itopo : 1;
         for (int i = 1; i <= npxn + 1; i++)
-            for (int k = k0; k <= nz; k++) ux(k, i) = ux(k, i) * sxn[i - 1];
+            for (int k = krow(i); k <= nz; k++) ux(k, i) = ux(k, i) * sxn[i - 1];
         for (int i = 1; i <= npxp + 1; i++)
-            for (int k = k0; k <= nz; k++) ux(k, nx - i + 1) = ux(k, nx - i + 1) * sxp[i - 1];
+            for (int k = krow(nx - i + 1); k <= nz; k++) ux(k, nx - i + 1) = ux(k, nx - i + 1) * sxp[i - 1];
         for (int i = 1; i <= nx && !fs; i++)
-            for (int k = 1; k <= npzn; k++) uz(k, i) = uz(k, i) * szn[k];
+            for (int k = std::max(itopo[i] - npzn, 1); k <= itopo[i]; k++)
+                uz(k, i) = uz(k, i) * szn[k - (itopo[i] - npzn)];
         for (int i = 1; i <= nx; i++)
             for (int k = 1; k <= npzp + 1; k++) uz(nz - k + 1, i) = uz(nz - k + 1, i) * szp[k - 1];
     }
@@ -117,21 +122,24 @@ struct IsoSolver {
             for (int k = 1; k <= nz; k++) v(k, i) = a_(k, i) + b_(k, i);
     }
 
-    // YPUB:938-976 calfsbcv on one pair of split parts: vz(izh-1) from vz(izh) and dx vx(izh)
+    // YPUB:938-976 calfsbcv on one pair of split parts: vz(izh-1) from vz(izh) and dx vx(izh),
+    // izh = itopo(ix) for both columns ix and ix + 1 (row 0 of the split parts is never read)
     void fsbcv(const Field<T>& vxp, Field<T>& vzp) {
-        if (itopo - 1 < 1) return;  // row 0 of the split parts is never read
-        for (int i = 1; i <= nx - 1; i++)
-            vzp(itopo - 1, i) = vzp(itopo, i) + (lambsg(itopo, i) / lambmusg(itopo, i)) * (vxp(itopo, i + 1) - vxp(itopo, i));
+        for (int i = 1; i <= nx - 1; i++) {
+            const int h = itopo[i];
+            if (h - 1 < 1) continue;
+            vzp(h - 1, i) = vzp(h, i) + (lambsg(h, i) / lambmusg(h, i)) * (vxp(h, i + 1) - vxp(h, i));
+        }
     }
     // YPUB:978-1007 calfsbcstrzz: rows 0..itopo zero
     void fsbczz(Field<T>& t) {
         for (int i = 1; i <= nx; i++)
-            for (int k = 1; k <= itopo; k++) t(k, i) = T(0.0);
+            for (int k = 1; k <= itopo[i]; k++) t(k, i) = T(0.0);
     }
     // YPUB:1009-1024 calfsbcstrxz: image row above the surface
     void fsbcxz(Field<T>& t) {
-        if (itopo - 1 < 1) return;
-        for (int i = 1; i <= nx; i++) t(itopo - 1, i) = -t(itopo, i);
+        for (int i = 1; i <= nx; i++)
+            if (itopo[i] - 1 >= 1) t(itopo[i] - 1, i) = -t(itopo[i], i);
     }
 
     // YPRI:305-359 (isoewm2dabc) or YPRI:121-196 (isoewm2dfsbc), one step; `src` adds the source
@@ -175,13 +183,13 @@ struct IsoSolver {
     }
 };
 
-// YPUB:592-634, serial order: rows k = 1..itopo of every column, each replaced by the weighted
-// sum of its (2 rgau - 1)^2 window as it stands at that moment
+// YPUB:592-634, serial order: rows k = 1..itopo(i) of every column, each replaced by the
+// weighted sum of its (2 rgau - 1)^2 window as it stands at that moment
 template <typename T>
-void gauss_filter(Field<T>& u, int nx, int nz, int rgau, int itopo, const Field<T>& gc) {
+void gauss_filter(Field<T>& u, int nx, int nz, int rgau, const std::vector<int>& itopo, const Field<T>& gc) {
     const int w = 2 * rgau - 1;
     for (int i = 1; i <= nx; i++)
-        for (int k = 1; k <= itopo; k++) {
+        for (int k = 1; k <= itopo[i]; k++) {
             T s = 0;
             int idx2 = 1;
             for (int n = i - (rgau - 1); n <= i + (rgau - 1); n++) {
@@ -220,11 +228,10 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     for (int m = 0; m < 2; m++) S.cr[2][m] = (T)a4[m];
     S.cr[1][0] = (T)1.0f;
     S.fs = c->fsbc != 0;
-    S.itopo = c->npzn;
     if (S.nx < 12 || S.nz < 12) return 1;
     S.alloc();
     const int NX = S.nx, NZ = S.nz;
-    const int itopo = c->npzn;  // flat surface: nint(0/dz) + npzn (YPUB:271)
+
     // YPUB:210-266 window and edge padding
     Field<T> vpe(1, NZ, 1, NX), vse(1, NZ, 1, NX), rhoe(1, NZ, 1, NX);
     auto in = [&](const float* m, int k, int i) { return (T)m[(size_t)(i - 1) * nz_m + (k - 1)]; };
@@ -247,6 +254,23 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
             for (int i = 1; i <= c->npxn; i++) (*f)(k, i) = (*f)(k, c->npxn + 1);
         for (int k = 1; k <= NZ; k++)
             for (int i = c->npxn + nxe + 1; i <= NX; i++) (*f)(k, i) = (*f)(k, c->npxn + nxe);
+    }
+    // YPUB:216-272 surface: topoe of the window (edge columns repeated), itopoe = nint(topoe/dz) + npzn
+    {
+        std::vector<float> topoe(NX + 1, 0.0f);
+        for (int i = 1; i <= nxe; i++) {
+            int io = i + c->ixmine;
+            if (io < 1) io = 1;
+            if (io > nx_m) io = nx_m;
+            topoe[i + c->npxn] = c->topo ? c->topo[io - 1] : 0.0f;
+        }
+        for (int i = 1; i <= c->npxn; i++) topoe[i] = topoe[c->npxn + 1];
+        for (int i = c->npxn + nxe + 1; i <= NX; i++) topoe[i] = topoe[c->npxn + nxe];
+        S.itopo.assign(NX + 1, 0);
+        for (int i = 1; i <= NX; i++) {
+            S.itopo[i] = (int)std::lround(topoe[i] / (float)c->dz) + c->npzn;
+            if (S.itopo[i] < (S.fs ? 1 : c->npzn) || S.itopo[i] > NZ - c->npzp - 6) return 3;
+        }
     }
     // YPUB:1470-1501 Gaussian coefficients, sigma = 2.0 cells, (2 rgau - 1)^2 window, normalised
     const T pi = (T)3.1415926f;
@@ -319,11 +343,11 @@ int prepare(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     // are carried further)
     for (auto* f : {&S.lambsg, &S.lambmusg, &S.musge, &S.busg1e, &S.busg2e})
         for (int i = 1; i <= NX; i++)
-            for (int k = itopo; k >= 2; k--) (*f)(k - 1, i) = (*f)(k, i);
+            for (int k = S.itopo[i]; k >= 2; k--) (*f)(k - 1, i) = (*f)(k, i);
     // YPRI:301-302 modipapml, abc mode only
     if (!S.fs)
         for (auto* f : {&S.lambsg, &S.musge, &S.lambmusg, &S.busg1e, &S.busg2e})
-            gauss_filter(*f, NX, NZ, c->rgau, itopo, gc);
+            gauss_filter(*f, NX, NZ, c->rgau, S.itopo, gc);
     // YPUB:796-849 cosine sponge, R = 1e-3
     {
         const T Rr = (T)1.0e-3f;
@@ -361,7 +385,6 @@ int run_iso(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     const int rc = prepare(c, vp_in, vs_in, rho_in, S, gc);
     if (rc) return rc;
     const int NX = S.nx, NZ = S.nz, nxe = c->ixmaxe - c->ixmine + 1;
-    const int itopo = c->npzn;
     const T pi = (T)3.1415926f;
     // YPUB:1429-1466 addsrc: the (2 rgau - 1)^2 window around the source; cells with an exact zero
     // weight are left out (adding a zero leaves u unchanged)
@@ -388,15 +411,16 @@ int run_iso(const OracleIsoCfg* c, const float* vp_in, const float* vs_in, const
     };
     // YPRI:305-367
     const int nt = c->nt;
-    const int kr = itopo + c->nrz0;
+
     // YPRI:163-168: in fsbc mode strxx takes the source only below the surface
-    const bool src_xx = !S.fs || isze > itopo;
+    const bool src_xx = !S.fs || isze > S.itopo[isxe];
     for (int it = 1; it <= nt + c->idecay; it++) {
         it_cur = it;
         S.step(addsrc, src_xx);
         const int iit = it - c->idecay;
         if (iit >= 1) {
             for (int i = 1; i <= nxe; i++) {
+                const int kr = S.itopo[i + c->npxn] + c->nrz0;  // YPUB:13 itopo(i+npxn)+nrz0
                 if (rec1) rec1[(size_t)(i - 1) * nt + (iit - 1)] = S.vx(kr, i + c->npxn);
                 if (rec2) rec2[(size_t)(i - 1) * nt + (iit - 1)] = S.vz(kr, i + c->npxn);
             }

@@ -60,7 +60,9 @@ typedef struct {
     int nrz0;                      // receiver row offset below itopo, nint(rz0/dz) + 1
     int idecay;                    // nint(decay/dt): steps before the first recorded sample
     int rgau;                      // Gaussian window half-width (2 rgau - 1 cells), the .par's rgau
-    int fsbc;                      // 0: 'abc' mode; 1: 'fsbc' mode, free surface at row npzn (1-based)
+    int fsbc;                      // 0: 'abc' mode; 1: 'fsbc' mode, free surface at row itopo (1-based)
+    const float* topo;             // surface depth (m) per model column (nx values), NULL: flat;
+                                   // itopo = nint(topo/dz) + npzn per window column (YPUB:270-272)
 } OracleIsoCfg;
 // the five arrays of the time loop after substagger and the PML smoothing (YPUB:323-634):
 // busg2e, busg1e, lambmusg, lambsg, musge, each [NX][NZ] of the padded window

@@ -181,16 +181,17 @@ class OracleIsoCfg(ctypes.Structure):
                 ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int), ("npxn", ctypes.c_int),
                 ("npxp", ctypes.c_int), ("npzn", ctypes.c_int), ("npzp", ctypes.c_int), ("ixmine", ctypes.c_int),
                 ("ixmaxe", ctypes.c_int), ("isxe", ctypes.c_int), ("isze", ctypes.c_int), ("nrz0", ctypes.c_int),
-                ("idecay", ctypes.c_int), ("rgau", ctypes.c_int), ("fsbc", ctypes.c_int)]
+                ("idecay", ctypes.c_int), ("rgau", ctypes.c_int), ("fsbc", ctypes.c_int), ("topo", _F32P)]
 
 
 def iso_forward(vp, vs, rho, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz0=1, idecay=0, rgau=50, ixmine=None,
-                ixmaxe=None, fp64=False, want_final=False, fsbc=False, npz_top=None):
+                ixmaxe=None, fp64=False, want_final=False, fsbc=False, npz_top=None, topo=None):
     """Restated yang_version isotropic elastic modelling, abc mode, flat surface
     (oracle/iso_oracle.cpp).  Model arrays are the interior (nx, nz) float32 x-major arrays; npx /
     npz are the sponge cells on both sides (npxn = npxp, npzn = npzp; npz_top overrides npzn, the
-    1-based surface row itopo of the fsbc mode); source and receiver row 1-based as in the
-    Fortran.  Returns (record1 = vx, record2 = vz, final vx or None), records [nxe][nt]."""
+    1-based surface row itopo of the fsbc mode); topo: surface depth (m) per model column (None:
+    flat); source row 1-based as in the Fortran (isz + itopoe(isxe)), receivers at
+    itopo(i) + nrz0.  Returns (record1 = vx, record2 = vz, final vx or None), records [nxe][nt]."""
     L = lib()
     if not hasattr(L, "_iso_sig"):
         tp = ctypes.POINTER(OracleIsoCfg)
@@ -203,8 +204,9 @@ def iso_forward(vp, vs, rho, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz0=1, i
     ixmaxe = nx - 1 if ixmaxe is None else ixmaxe
     nxe = ixmaxe - ixmine + 1
     top = npz if npz_top is None else npz_top
+    topo_a = None if topo is None else np.ascontiguousarray(topo, np.float32)
     cfg = OracleIsoCfg(nx, nz, dx, dz, dt, f0, nt, npx, npx, top, npz, ixmine, ixmaxe, isxe, isze, nrz0, idecay, rgau,
-                       1 if fsbc else 0)
+                       1 if fsbc else 0, _p(topo_a))
     dt_ = np.float64 if fp64 else np.float32
     tp = _F64P if fp64 else _F32P
     r1 = np.zeros((nxe, nt), dt_)

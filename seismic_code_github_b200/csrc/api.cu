@@ -118,7 +118,10 @@ struct sfd_ctx {
     // isotropic elastic scheme (yang_version): Gaussian half-width, its table and non-zero range;
     // the prepared model lives in e_q[0..4] (busg2e, busg1e, lambmusg, lambsg, musge)
     int iso_rgau = 50;
-    int iso_top = 0;                // 0: abc mode; >= 1: fsbc mode, free surface at 1-based row iso_top
+    int iso_top = 0;                // 0: abc mode; >= 1: fsbc mode, top pad of iso_top rows (flat: itopo)
+    std::vector<int> h_itopo;       // itopo per padded model column (sfd_set_topography); empty: flat
+    int* d_itopo = nullptr;         // ... per prepared-model column
+    long long topo_gen = 0;         // bumped by every sfd_set_topography
     std::vector<float> iso_gc;
     int iso_lo = 0, iso_hi = -1;
     long long model_gen = 0;        // bumped by every sfd_set_model
@@ -128,6 +131,7 @@ struct sfd_ctx {
     long long prep_gen = -1;
     int prep_rgau = -1;
     int prep_top = -1;
+    long long prep_topo_gen = -1;
 
     // gradient (sized on first use for the current shot set)
     int ckpt_interval = 0;
@@ -284,7 +288,7 @@ sfd_ctx::~sfd_ctx() {
     if (device >= 0) cudaSetDevice(device);
     free_shot_buffers(this);
     dfree(d_vp); dfree(d_den); dfree(d_q); dfree(d_flag); dfree(d_err);
-    dfree(q_busg); dfree(q_p1); dfree(q_p2); dfree(d_spg);
+    dfree(q_busg); dfree(q_p1); dfree(q_p2); dfree(d_spg); dfree(d_itopo);
     for (auto& p : e_q) dfree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -475,7 +479,7 @@ IArgs make_iargs(const sfd_ctx* c, int step) {
                             {1225.0f / 1024.0f, -245.0f / 3072.0f, 49.0f / 5120.0f, -5.0f / 7168.0f}};
     std::memcpy(a.cr, cr, sizeof(cr));
     a.fs = c->iso_top > 0 ? 1 : 0;
-    a.zs = c->iso_top - 1;
+    a.itopo = c->d_itopo;
     a.spg = c->d_spg;
     a.spg_stride = c->spg_stride;
     a.shots = c->d_shots;
@@ -1227,12 +1231,27 @@ int q_prepare(sfd_ctx* ctx) {
         width += wins[b].second;
     }
     if (iso && wins == ctx->prep_wins && ctx->model_gen == ctx->prep_gen && ctx->iso_rgau == ctx->prep_rgau &&
-        ctx->iso_top == ctx->prep_top && width == ctx->q_width) {
+        ctx->iso_top == ctx->prep_top && ctx->topo_gen == ctx->prep_topo_gen && width == ctx->q_width) {
         if (ctx->have_shots) {
             for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
             CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
         }
         return SFD_OK;
+    }
+    // yang_version surface rows per prepared column: the topography's itopo, or flat (the top pad:
+    // pml in abc mode, the free surface's row in fsbc mode); YPUB:270-272
+    std::vector<int> itopo(iso ? width : 0);
+    if (iso) {
+        const int flat = ctx->iso_top > 0 ? ctx->iso_top : ctx->g.pml;
+        const int lo = ctx->iso_top > 0 ? 1 : ctx->g.pml, hi = nz - ctx->g.pml - 6;
+        for (size_t b = 0; b < wins.size(); b++)
+            for (int c = 0; c < wins[b].second; c++) {
+                const int v = ctx->h_itopo.empty() ? flat : ctx->h_itopo[wins[b].first + c];
+                if (v < lo || v > hi)
+                    return set_err(ctx, SFD_ERR_ARG, "surface row %d of column %d outside [%d, %d]", v,
+                                   wins[b].first + c, lo, hi);
+                itopo[start[b] + c] = v;
+            }
     }
     std::vector<float> busg((size_t)width * nz), p1((size_t)width * nz), p2((size_t)width * nz);
     std::vector<std::vector<float>> eq(elastic ? 6 : iso ? 5 : 0, std::vector<float>((size_t)width * nz));
@@ -1245,8 +1264,8 @@ int q_prepare(sfd_ctx* ctx) {
         if (iso) {  // YPUB:323-547 per window, flat surface: itopo = npzn (pml, or the free surface's row)
             std::vector<float> vs(len, 0.0f);
             if (!ctx->h_vs.empty()) vs.assign(ctx->h_vs.begin() + off, ctx->h_vs.begin() + off + len);
-            const int itopo = ctx->iso_top > 0 ? ctx->iso_top : ctx->g.pml;
-            if (!elastic2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(), itopo,
+            if (!elastic2d_prepare(wins[b].second, nz, ctx->h_vp.data() + off, vs.data(), rho.data(),
+                                   itopo.data() + start[b],
                                    eq[0].data() + o, eq[1].data() + o, eq[2].data() + o, eq[3].data() + o,
                                    eq[4].data() + o))
                 return set_err(ctx, SFD_ERR_ARG, "zero density in the window at column %d", wins[b].first);
@@ -1281,6 +1300,9 @@ int q_prepare(sfd_ctx* ctx) {
     if (iso) {
         for (int i = 0; i < 5; i++)
             if ((rc = upload(&ctx->e_q[i], eq[i]))) return rc;
+        if (width != ctx->q_width) dfree(ctx->d_itopo);
+        if (!ctx->d_itopo) CK(cudaMalloc(&ctx->d_itopo, sizeof(int) * width));
+        CK(cudaMemcpy(ctx->d_itopo, itopo.data(), sizeof(int) * width, cudaMemcpyHostToDevice));
         // YPUB:549-634 modipapml on the device (abc mode only, YPRI:301-302): rows z < pml of the
         // five arrays, per window
         std::vector<int> win;
@@ -1291,7 +1313,7 @@ int q_prepare(sfd_ctx* ctx) {
             }
         float* arrs[5];
         for (int i = 0; i < 5; i++) arrs[i] = ctx->e_q[i] + kModelGhostZ;
-        CK(elastic2d_smooth(arrs, ctx->mpitch, kModelGhostZ, nz, ctx->g.pml, win.data(), (int)win.size() / 2,
+        CK(elastic2d_smooth(arrs, ctx->mpitch, kModelGhostZ, nz, ctx->d_itopo, win.data(), (int)win.size() / 2,
                             ctx->iso_gc, ctx->iso_rgau, ctx->iso_lo, ctx->iso_hi, ctx->stream));
     } else if ((rc = upload(&ctx->q_busg, busg))) {
         return rc;
@@ -1308,6 +1330,7 @@ int q_prepare(sfd_ctx* ctx) {
     ctx->prep_gen = ctx->model_gen;
     ctx->prep_rgau = ctx->iso_rgau;
     ctx->prep_top = ctx->iso_top;
+    ctx->prep_topo_gen = ctx->topo_gen;
     if (ctx->have_shots) {
         for (int s = 0; s < ctx->nshot; s++) ctx->h_shots[s].x0 = start[blk[s]];
         CK(cudaMemcpy(ctx->d_shots, ctx->h_shots.data(), sizeof(ShotDev) * ctx->nshot, cudaMemcpyHostToDevice));
@@ -2145,8 +2168,7 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         if ((rc = build_stamps(ctx))) return rc;
         ctx->spg_stride = ctx->g.pml + 1;
         std::vector<float> tab(8 * (size_t)ctx->spg_stride);
-        if (iso) elastic2d_sponge_tables(ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
-        else viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
+        viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
         dfree(ctx->d_spg);
         if ((rc = up(&ctx->d_spg, tab))) return rc;
     } else {
@@ -2365,6 +2387,24 @@ int sfd_set_free_surface(sfd_ctx* ctx, int top) {
     ctx->graph_valid = false;
     for (auto& sn : ctx->snaps) sn.ready = false;  // the snapshot interior starts at the new top
     return q_prepare(ctx);  // substagger's refill row and the smoothing follow the mode
+}
+
+int sfd_set_topography(sfd_ctx* ctx, const int* itopo) {
+    if (!ctx) return SFD_ERR_ARG;
+    if (ctx->g.scheme != SFD_ELASTIC_2D) return set_err(ctx, SFD_ERR_ARG, "topography applies to SFD_ELASTIC_2D");
+    if (itopo) {
+        for (int x = 0; x < ctx->g.nx; x++)
+            if (itopo[x] < 1 || itopo[x] > ctx->g.nz - ctx->g.pml - 6)
+                return set_err(ctx, SFD_ERR_ARG, "itopo[%d] = %d outside [1, %d]", x, itopo[x],
+                               ctx->g.nz - ctx->g.pml - 6);
+        ctx->h_itopo.assign(itopo, itopo + ctx->g.nx);
+    } else {
+        ctx->h_itopo.clear();
+    }
+    CK(cudaSetDevice(ctx->device));
+    ctx->topo_gen++;
+    ctx->graph_valid = false;
+    return q_prepare(ctx);  // the refill rows, the smoothing rows and the kernels follow the surface
 }
 
 int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes) {

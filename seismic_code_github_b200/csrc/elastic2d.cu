@@ -17,7 +17,10 @@
 // Every multiply and add is rounded separately in the reference's order, so the kernels agree
 // bit for bit with the FP32 restatement in oracle/iso_oracle.cpp.
 //
-// Free surface (fsbc): rows above zs keep their values; the z derivatives of the five rows from
+// The surface row is per column: itopo(x) (1-based, the reference's itopoe), from a topography or
+// flat.  abc mode updates the rows from t0 = itopo - npz - 1 (0-based) down, with the top sponge
+// on rows t0 .. t0 + npz taking spgzn(z - t0 + 1) (YPUB:851-897); a flat surface has t0 = -1.
+// Free surface (fsbc, zs = itopo - 1): rows above zs keep their values; the z derivatives of the five rows from
 // zs down drop to 8th, 6th, 4th and 2nd order (YPUB:1160-1343); left and right sponges act from
 // zs down, the bottom sponge everywhere, no top sponge (YPUB:901-934); strzz parts are zero on
 // rows <= zs after their sponge and before the source (YPUB:978-1007), which enters strxx only for
@@ -149,10 +152,11 @@ __device__ __forceinline__ float4 dz4(const float* s, int r, int c, const IArgs&
     return acc;
 }
 
-// z-part sponge: abc, top then bottom table (YPUB:851-897); fsbc, the bottom table only
+// z-part sponge: abc, the top table on rows t0 .. t0 + npz then the bottom table (YPUB:851-897);
+// fsbc, the bottom table only (YPUB:901-934)
 template <bool FS>
-__device__ __forceinline__ float zsp(float u, int z, const IArgs& a, const float* tn, const float* tp) {
-    if (!FS) return xs(u, z, a.nz, a.npz, tn, tp);
+__device__ __forceinline__ float zsp(float u, int z, int t0, const IArgs& a, const float* tn, const float* tp) {
+    if (!FS && z >= t0 && z <= t0 + a.npz) u = fm(u, tn[z - t0]);
     if (z >= a.nz - a.npz - 1) u = fm(u, tp[a.nz - 1 - z]);
     return u;
 }
@@ -190,13 +194,16 @@ __global__ void __launch_bounds__(kThreads, 3) iso_velocity_kernel(const __grid_
     const int zv = threadIdx.x & 15, z = 4 * zv, gz = t.z0 + z;
     const int nv = min(4, nz - gz);  // cells of the vector inside the grid
     if (nv <= 0) return;             // no barrier follows
-    const int d0 = FS ? gz - a.zs : (1 << 20);
 #pragma unroll 1
     for (int j = 0; j < kItems; j++) {
         const int r = (threadIdx.x >> 4) + 16 * j, gx = t.x0 + r;
         if (gx >= nx) break;
         const long long c = cell(a, t.shot, gx, gz);
-        const long long mi = (long long)min(t.sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
+        const int mc = min(t.sd.x0 + gx, a.nx_model - 1);
+        const long long mi = (long long)mc * a.mpitch + gz;
+        // first updated row: zs = itopo - 1 (fsbc) or t0 = itopo - npz - 1 (abc)
+        const int top = __ldg(a.itopo + mc) - (FS ? 1 : a.npz + 1);
+        const int d0 = FS ? gz - top : (1 << 20);
         float4 vxx = ld4(a.f[I_VXX], c, nv), vxz = ld4(a.f[I_VXZ], c, nv);
         float4 vzx = ld4(a.f[I_VZX], c, nv), vzz = ld4(a.f[I_VZZ], c, nv);
         const float4 b2 = __ldg(reinterpret_cast<const float4*>(a.b2e + mi));
@@ -208,21 +215,21 @@ __global__ void __launch_bounds__(kThreads, 3) iso_velocity_kernel(const __grid_
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int zq = min(gz + q, nz - 1);  // cells past nz are computed, not stored
-            const bool below = !FS || gz + q >= a.zs;  // fsbc: rows above the surface keep their values
+            const bool below = gz + q >= top;  // rows above the first updated row keep their values
             // YPRI:310-316: vx parts, sponge spgxn/spgxp (x part), spgzn/spgzp (z part)
             if (below) {
                 const float n_xx = fa(cmp(vxx, q), fm(fm(a.dtdx, cmp(b2, q)), cmp(d_xx, q)));
                 cmpr(vxx, q) = xs(n_xx, gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
                 cmpr(vxz, q) = fa(cmp(vxz, q), fm(fm(a.dtdz, cmp(b2, q)), cmp(d_xz, q)));
             }
-            cmpr(vxz, q) = zsp<FS>(cmp(vxz, q), zq, a, tb + 2 * st, tb + 3 * st);
+            cmpr(vxz, q) = zsp<FS>(cmp(vxz, q), zq, top, a, tb + 2 * st, tb + 3 * st);
             // YPRI:320-326: vz parts, sponge spg1xn/spg2xp, spg1zn/spg2zp
             if (below) {
                 const float n_zx = fa(cmp(vzx, q), fm(fm(a.dtdx, cmp(b1, q)), cmp(d_zx, q)));
                 cmpr(vzx, q) = xs(n_zx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
                 cmpr(vzz, q) = fa(cmp(vzz, q), fm(fm(a.dtdz, cmp(b1, q)), cmp(d_zz, q)));
             }
-            cmpr(vzz, q) = zsp<FS>(cmp(vzz, q), zq, a, tb + 6 * st, tb + 7 * st);
+            cmpr(vzz, q) = zsp<FS>(cmp(vzz, q), zq, top, a, tb + 6 * st, tb + 7 * st);
         }
         st4(a.f[I_VXX], c, nv, vxx); st4(a.f[I_VXZ], c, nv, vxz);
         st4(a.f[I_VZX], c, nv, vzx); st4(a.f[I_VZZ], c, nv, vzz);
@@ -245,14 +252,17 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
     const float wav = __ldg(a.wavelets + sd.wav_off + a.step);
     const int zv = threadIdx.x & 15, z = 4 * zv, gz = t.z0 + z;
     const int nv = min(4, nz - gz);
-    const int d0 = FS ? gz - a.zs : (1 << 20);
-    const bool src_xx = !FS || sd.sz > a.zs;  // YPRI:163-168
+    // YPRI:163-168: in fsbc mode strxx takes the source only below the surface at the source column
+    const bool src_xx = !FS || sd.sz + 1 > __ldg(a.itopo + min(sd.x0 + sd.sx, a.nx_model - 1));
 #pragma unroll 1
     for (int j = 0; j < kItems && nv > 0; j++) {
         const int r = (threadIdx.x >> 4) + 16 * j, gx = t.x0 + r;
         if (gx >= nx) break;
         const long long c = cell(a, t.shot, gx, gz);
-        const long long mi = (long long)min(sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
+        const int mc = min(sd.x0 + gx, a.nx_model - 1);
+        const long long mi = (long long)mc * a.mpitch + gz;
+        const int top = __ldg(a.itopo + mc) - (FS ? 1 : a.npz + 1);  // zs (fsbc) or t0 (abc)
+        const int d0 = FS ? gz - top : (1 << 20);
         float4 v[6];  // strxxx strxxz strzzx strzzz strxzx strxzz
 #pragma unroll
         for (int k = 0; k < 6; k++) v[k] = ld4(a.f[I_SXXX + k], c, nv);
@@ -273,9 +283,10 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
             float src = 0.0f;
             if (in_stamp)  // YPUB:1458 wavelet*gc2d*dt/(dz**2)
                 src = __fdiv_rn(fm(fm(wav, __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz)), a.dt), a.dz2);
-            // fsbc: rows above the surface keep their values (calux / caluz start at itopo)
-            const bool below = !FS || gz + q >= a.zs;
-            const bool zero_zz = FS && gz + q <= a.zs;  // YPUB:978-1007, rows <= itopo
+            // rows above the first updated row keep their values (the loops start at itopo or
+            // itopo - npzn)
+            const bool below = gz + q >= top;
+            const bool zero_zz = FS && gz + q <= top;  // YPUB:978-1007, rows <= itopo
             // YPRI:331-338: strxx parts, sponge spg1xn/spg2xp, spgzn/spgzp, then the source
             float s0 = cmp(v[0], q), s1 = cmp(v[1], q), s2 = cmp(v[2], q), s3 = cmp(v[3], q);
             float s4 = cmp(v[4], q), s5 = cmp(v[5], q);
@@ -283,14 +294,14 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
                 s0 = xs(fa(s0, fm(fm(a.dtdx, cmp(lm2, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
                 s1 = fa(s1, fm(fm(a.dtdz, cmp(lam, q)), cmp(d2, q)));
             }
-            s1 = zsp<FS>(s1, zq, a, tb + 2 * st, tb + 3 * st);
+            s1 = zsp<FS>(s1, zq, top, a, tb + 2 * st, tb + 3 * st);
             if (in_stamp && src_xx) s0 = fa(src, s0);
             // YPRI:342-349: strzz parts; fsbc: zero on rows <= the surface before the source
             if (below) {
                 s2 = xs(fa(s2, fm(fm(a.dtdx, cmp(lam, q)), cmp(d1, q))), gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
                 s3 = fa(s3, fm(fm(a.dtdz, cmp(lm2, q)), cmp(d2, q)));
             }
-            s3 = zsp<FS>(s3, zq, a, tb + 2 * st, tb + 3 * st);
+            s3 = zsp<FS>(s3, zq, top, a, tb + 2 * st, tb + 3 * st);
             if (zero_zz) s2 = s3 = 0.0f;
             if (in_stamp) s2 = fa(src, s2);
             // YPRI:353-359: strxz parts, sponge spgxn/spgxp, spg1zn/spg2zp
@@ -298,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
                 s4 = xs(fa(s4, fm(fm(a.dtdx, cmp(mue, q)), cmp(d3, q))), gx, nx, a.npx, tb + 0 * st, tb + 1 * st);
                 s5 = fa(s5, fm(fm(a.dtdz, cmp(mue, q)), cmp(d4, q)));
             }
-            s5 = zsp<FS>(s5, zq, a, tb + 6 * st, tb + 7 * st);
+            s5 = zsp<FS>(s5, zq, top, a, tb + 6 * st, tb + 7 * st);
             cmpr(v[0], q) = s0; cmpr(v[1], q) = s1; cmpr(v[2], q) = s2;
             cmpr(v[3], q) = s3; cmpr(v[4], q) = s4; cmpr(v[5], q) = s5;
         }
@@ -318,7 +329,7 @@ __global__ void __launch_bounds__(kThreads, 3) iso_stress_kernel(const __grid_co
     }
 }
 
-// Free surface, after the stress kernel (one thread per column): the image strxz(zs - 1) =
+// Free surface, after the stress kernel (one thread per column, zs = itopo(x) - 1): the image strxz(zs - 1) =
 // -strxz(zs) of both split parts (YPUB:1009-1024), and vz(zs - 1) = vz(zs) + lambsg/lambmusg
 // (vx(zs, x + 1) - vx(zs, x)) for both pairs of split parts (YPUB:938-976, columns but the last).
 __global__ void iso_surface_kernel(const __grid_constant__ IArgs a) {
@@ -326,13 +337,15 @@ __global__ void iso_surface_kernel(const __grid_constant__ IArgs a) {
     const ShotDev sd = a.shots[shot];
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= sd.nx) return;
-    const int zs = a.zs;
+    const int mc = min(sd.x0 + x, a.nx_model - 1);
+    const int zs = __ldg(a.itopo + mc) - 1;
+    if (zs < 1) return;  // the row above the surface is the split fields' unused row 0
     const long long c = cell(a, shot, x, zs), cu = c - 1;
     a.f[I_SXZX][cu] = -a.f[I_SXZX][c];
     a.f[I_SXZZ][cu] = -a.f[I_SXZZ][c];
     if (x + 1 < sd.nx) {
         const long long cn = cell(a, shot, x + 1, zs);
-        const long long mi = (long long)min(sd.x0 + x, a.nx_model - 1) * a.mpitch + zs;
+        const long long mi = (long long)mc * a.mpitch + zs;
         const float ratio = __fdiv_rn(__ldg(a.lam + mi), __ldg(a.lm2 + mi));
         a.f[I_VZX][cu] = fa(a.f[I_VZX][c], fm(ratio, fs(a.f[I_VXX][cn], a.f[I_VXX][c])));
         a.f[I_VZZ][cu] = fa(a.f[I_VZZ][c], fm(ratio, fs(a.f[I_VXZ][cn], a.f[I_VXZ][c])));
@@ -352,7 +365,8 @@ struct SmoothArgs {
     float* arr[5];
     const int* win;   // nwin (start column, width) pairs
     const int* rng;   // per table column idx2: first and last row idx1 with a non-zero weight
-    int nwin, mpitch, ghost, nz, itopo, rgau, lo, hi;
+    const int* itopo; // per prepared column: rows z < itopo are smoothed
+    int nwin, mpitch, ghost, nz, rgau, lo, hi;
     const float* gc;
 };
 
@@ -361,10 +375,11 @@ __global__ void __launch_bounds__(32) iso_smooth_kernel(const __grid_constant__ 
     const int t = blockIdx.x, lane = threadIdx.x;
     const int b = t / 5;
     float* u = s.arr[t - 5 * b] + (long long)s.win[2 * b] * s.mpitch;
+    const int* itopo = s.itopo + s.win[2 * b];
     const int nxw = s.win[2 * b + 1];
     const int w = 2 * s.rgau - 1, r1 = s.rgau - 1;
     for (int i = 0; i < nxw; i++)
-        for (int k = 0; k < s.itopo; k++) {
+        for (int k = 0, kn = min(itopo[i], s.nz); k < kn; k++) {
             const int nlo = max(i - r1 + s.lo, 0), nhi = min(i - r1 + s.hi, nxw - 1);
             // lane L forms the products of columns nlo + L and nlo + L + 32; their offsets in the
             // loop order come from a warp prefix sum of the column lengths
@@ -437,10 +452,8 @@ cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaSt
     if (a.fs) {
         iso_velocity_kernel<true><<<grid, kThreads, smem, st>>>(a);
         iso_stress_kernel<true><<<grid, kThreads, 0, st>>>(a);
-        if (a.zs >= 1) {  // row zs - 1 exists in the grid
-            iso_surface_kernel<<<dim3((nx_max + 127) / 128, active), 128, 0, st>>>(a);
-            *launches = 3;
-        }
+        iso_surface_kernel<<<dim3((nx_max + 127) / 128, active), 128, 0, st>>>(a);
+        *launches = 3;
     } else {
         iso_velocity_kernel<false><<<grid, kThreads, smem, st>>>(a);
         iso_stress_kernel<false><<<grid, kThreads, 0, st>>>(a);
@@ -448,9 +461,10 @@ cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int nz, int itopo, const int* win_host,
-                             int nwin, const std::vector<float>& gc, int rgau, int lo, int hi, cudaStream_t st) {
-    if (nwin <= 0 || itopo <= 0) return cudaSuccess;
+cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int nz, const int* itopo_dev,
+                             const int* win_host, int nwin, const std::vector<float>& gc, int rgau, int lo, int hi,
+                             cudaStream_t st) {
+    if (nwin <= 0) return cudaSuccess;
     SmoothArgs s{};
     for (int i = 0; i < 5; i++) s.arr[i] = arrays[i];
     const int w = 2 * rgau - 1;
@@ -481,7 +495,7 @@ cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int 
         s.mpitch = mpitch;
         s.ghost = ghost;
         s.nz = nz;
-        s.itopo = std::min(itopo, nz);
+        s.itopo = itopo_dev;
         s.rgau = rgau;
         s.lo = lo;
         s.hi = hi;
@@ -505,8 +519,8 @@ cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int 
     return e;
 }
 
-bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, int itopo, float* b2e,
-                       float* b1e, float* lm2, float* lam, float* mue) {
+bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, const int* itopo,
+                       float* b2e, float* b1e, float* lm2, float* lam, float* mue) {
     const size_t n = (size_t)nx * nz;
     auto at = [nz](int k, int i) { return (size_t)i * nz + k; };  // Fortran (k, i), 0-based
     std::vector<float> mu(n), lamb(n), busg1(n, 0.0f), busg2(n), musg(n);
@@ -558,7 +572,7 @@ bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const f
     // YPUB:484-501: rows above itopo (1-based) take row itopo's values
     for (float* f : {b2e, b1e, lm2, lam, mue})
         for (int i = 0; i < nx; i++)
-            for (int k = std::min(itopo, nz) - 1; k >= 1; k--) f[at(k - 1, i)] = f[at(k, i)];
+            for (int k = std::min(itopo[i], nz) - 1; k >= 1; k--) f[at(k - 1, i)] = f[at(k, i)];
     return true;
 }
 
@@ -605,15 +619,6 @@ void elastic2d_stamp(int nx, int nz, int sx, int sz, int rgau, const std::vector
     box[0] = xlo; box[1] = zlo; box[2] = xhi - xlo + 1; box[3] = zhi - zlo + 1;
     for (int x = xlo; x <= xhi; x++)
         for (int z = zlo; z <= zhi; z++) out->push_back(gc[(size_t)(x - sx + r1) * w + (z - sz + r1)]);
-}
-
-void elastic2d_sponge_tables(int np, float dx, float dz, int stride, float* out) {
-    viscoac2d_sponge_tables(np, np, dx, dz, stride, out);  // YPUB:796-849 = the same cosine profiles
-    for (int t : {2, 6}) {
-        float* f = out + t * stride;
-        for (int z = 0; z < np; z++) f[z] = f[z + 1];
-        f[np] = 1.0f;
-    }
 }
 
 }  // namespace sfd

@@ -127,9 +127,10 @@ struct IArgs {
     float dt, dtdx, dtdz, dz2;
     float a[5];
     float cr[4][4];                       // M-term staggered coefficients, M = 1..4 (YMOD:7-20)
-    int fs;                               // 1: free surface (fsbc mode) at row zs, 0: abc mode
-    int zs;                               // surface row (0-based; the reference's itopo - 1)
-    const float* spg;                     // spgxn spgxp spgzn' spgzp spg1xn spg2xp spg1zn' spg2zp
+    int fs;                               // 1: free surface (fsbc mode), 0: abc mode
+    const int* itopo;                     // per prepared-model column: the reference's itopo (1-based
+                                          // surface row; abc updates from row itopo - npz - 1, 0-based)
+    const float* spg;                     // spgxn spgxp spgzn spgzp spg1xn spg2xp spg1zn spg2zp
     int spg_stride;
     const ShotDev* shots;
     const int* slot_to_shot;
@@ -141,14 +142,14 @@ struct IArgs {
     float* records2;                      // vz (record2)
     int step;
 };
-// One step: the velocity and stress kernels, and in fsbc mode with zs >= 1 the surface kernel
-// (YPUB:938-976 calfsbcv, YPUB:1009-1024 calfsbcstrxz); *launches receives the kernel count.
+// One step: the velocity and stress kernels, and in fsbc mode the surface kernel (YPUB:938-976
+// calfsbcv, YPUB:1009-1024 calfsbcstrxz); *launches receives the kernel count.
 cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaStream_t st, int* launches);
 // YPUB:323-547 on one window (x-major, z fastest): substagger and the refill of the rows above
-// itopo (0-based rows < itopo - 1 take row itopo - 1); out: busg2e, busg1e, lambmusg, lambsg, musge.
-// Returns false on a zero density (YPUB:370, 400).
-bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, int itopo, float* b2e,
-                       float* b1e, float* lm2, float* lam, float* mue);
+// itopo(x) (0-based rows < itopo - 1 take row itopo - 1); out: busg2e, busg1e, lambmusg, lambsg,
+// musge.  Returns false on a zero density (YPUB:370, 400).
+bool elastic2d_prepare(int nx, int nz, const float* vp, const float* vs, const float* rho, const int* itopo,
+                       float* b2e, float* b1e, float* lm2, float* lam, float* mue);
 // YPUB:1470-1501: the (2 rgau - 1)^2 Gaussian table (sigma 2 cells), normalised by its sum, in
 // Fortran order gc(idx1, idx2) = out[(idx2 - 1) * w + idx1 - 1]; *lo / *hi: 0-based index range
 // holding every non-zero weight (the same along both axes).
@@ -157,15 +158,14 @@ void elastic2d_gauss_table(int rgau, std::vector<float>* out, int* lo, int* hi);
 // non-zero weights (x0, z0, w, h) and the weights (x-major, z fastest).
 void elastic2d_stamp(int nx, int nz, int sx, int sz, int rgau, const std::vector<float>& gc, int* box,
                      std::vector<float>* out);
-// YPUB:796-849 cosine sponge, with the two top tables shifted for calpmlbclrtb's top loop
-// (YPUB:878-883: row k = 1..npzn takes spgzn(k + 1)).
-void elastic2d_sponge_tables(int np, float dx, float dz, int stride, float* out);
-// YPUB:592-634 on the device: the in-place Gaussian smoothing of rows z < itopo of the five
+// YPUB:592-634 on the device: the in-place Gaussian smoothing of rows z < itopo(x) of the five
 // prepared arrays of every window (one sequential chain per array and window, serial order).
 // arrays: five device pointers to row z = 0 of column 0 (column pitch mpitch, `ghost` replicated
-// rows above z = 0, refreshed afterwards); win: nwin (start column, width) pairs.
-cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int nz, int itopo, const int* win_host,
-                             int nwin, const std::vector<float>& gc, int rgau, int lo, int hi, cudaStream_t st);
+// rows above z = 0, refreshed afterwards); itopo_dev: per prepared column; win: nwin (start
+// column, width) pairs.
+cudaError_t elastic2d_smooth(float* const arrays[5], int mpitch, int ghost, int nz, const int* itopo_dev,
+                             const int* win_host, int nwin, const std::vector<float>& gc, int rgau, int lo, int hi,
+                             cudaStream_t st);
 
 // Arguments of the viscoacoustic adjoint kernels (q_adjoint2d.cu): adjoint fields in place.
 struct QAdjArgs {

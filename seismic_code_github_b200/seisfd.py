@@ -121,6 +121,7 @@ SIGNATURES = {
     "sfd_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "sfd_set_gauss_radius": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_set_free_surface": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sfd_set_topography": (ctypes.c_int, [ctypes.c_void_p, _I32P]),
     "sfd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "sfd_set_snapshots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int]),
@@ -367,6 +368,15 @@ class Engine:
         """Boundary mode of the isotropic elastic scheme: 0 = absorbing on all sides ('abc'),
         top >= 1 = free surface at padded row top - 1 ('fsbc', the reference's itopo = top)."""
         self._check(self._lib.sfd_set_free_surface(self._h, int(top)), "sfd_set_free_surface")
+
+    def set_topography(self, itopo):
+        """Surface row per padded model column for the isotropic elastic scheme (the reference's
+        1-based itopoe = nint(topo/dz) + npzn); None restores the flat surface."""
+        if itopo is None:
+            self._check(self._lib.sfd_set_topography(self._h, None), "sfd_set_topography")
+            return
+        a = np.ascontiguousarray(itopo, np.int32)
+        self._check(self._lib.sfd_set_topography(self._h, a.ctypes.data_as(_I32P)), "sfd_set_topography")
 
     def set_memory_limit(self, nbytes: int):
         """Device-memory budget of gradient() (0: the free device memory)."""
