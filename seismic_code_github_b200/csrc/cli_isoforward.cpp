@@ -17,8 +17,11 @@
 // where <name> is the last path component of the card's snapx / snapz prefix (YPRI:212-224,
 // YPUB:20-44).  The reference writes them for the shots of MPI rank 0 into the card's
 // directories.
-// Limits of this engine, reported as errors: a flat surface only (the topography file must be all
-// zeros), one sponge width for the left, right and bottom sides (and the top in abc mode).
+// The topography file gives each model column's surface depth; every window column gets
+// itopoe = nint(topoe/dz) + npzn (YPUB:216-272, pads repeat the window's edge columns), the
+// source sits at isz + itopoe(isxe) and trace i records row itopoe(i + npxn) + nrz0 (YPUB:2-16).
+// Limit of this engine, reported as an error: one sponge width for the left, right and bottom
+// sides (and the top in abc mode).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -103,9 +106,6 @@ int main(int argc, char** argv) {
         if ((rc = sfd_read_floats(strip(files[f]).c_str(), (long long)nm, arrays[f]->data())))
             return fail(files[f], rc, nullptr);
     if ((rc = sfd_read_floats(strip(p.topo).c_str(), nx, topo.data()))) return fail(p.topo, rc, nullptr);
-    for (int i = 0; i < nx; i++)
-        if (nint(topo[i] / p.dz) != 0)  // YPUB:271 itopoe = nint(topo/dz) + npzn
-            return fail("topography (this engine models a flat surface)", SFD_ERR_UNSUPPORTED, nullptr);
     const int nt_run = p.nt + idecay;
     std::vector<float> w(nt_run);
     if ((rc = sfd_wavelet(SFD_WAVELET_ISO, nt_run, p.dt, p.f0, idecay, w.data()))) return fail("wavelet", rc, nullptr);
@@ -142,6 +142,7 @@ int main(int argc, char** argv) {
     }
     const size_t nme = (size_t)width * nzea;
     std::vector<float> vpe(nme), vse(nme), rhoe(nme);
+    std::vector<int> itopoe(width);  // YPUB:270-272 per padded window column
     for (size_t b = 0; b < blocks.size(); b++) {
         const int ixmine = blocks[b].first, nxe = blocks[b].second, nxea = nxe + 2 * np;
         for (int c = 0; c < nxea; c++) {
@@ -150,6 +151,7 @@ int main(int argc, char** argv) {
             const int i = c < np ? 1 : (c >= np + nxe ? nxe : c - np + 1);
             int i_ori = i + ixmine;
             i_ori = i_ori < 1 ? 1 : (i_ori > nx ? nx : i_ori);
+            itopoe[block_x0[b] + c] = nint(topo[i_ori - 1] / p.dz) + top;
             for (int k = 0; k < nzea; k++) {
                 const int kz = k < top ? 0 : (k >= top + nz ? nz - 1 : k - top);
                 const size_t src = (size_t)(i_ori - 1) * nz + kz, dst = (size_t)(block_x0[b] + c) * nzea + k;
@@ -175,20 +177,25 @@ int main(int argc, char** argv) {
     if ((rc = sfd_create(&g, device, &ctx))) return fail("sfd_create", rc, ctx);
     if ((rc = sfd_set_gauss_radius(ctx, p.rgau))) return fail("sfd_set_gauss_radius", rc, ctx);
     if (fsbc && (rc = sfd_set_free_surface(ctx, top))) return fail("sfd_set_free_surface", rc, ctx);
+    if ((rc = sfd_set_topography(ctx, itopoe.data()))) return fail("sfd_set_topography", rc, ctx);
     if ((rc = sfd_set_model_elastic(ctx, vpe.data(), vse.data(), rhoe.data(), nullptr, nullptr)))
         return fail("sfd_set_model_elastic", rc, ctx);
     std::vector<sfd_shot> desc(p.nshot);
     std::vector<std::vector<int>> rx(p.nshot), rz(p.nshot);
     for (int i = 0; i < p.nshot; i++) {
         const ShotInfo& s = shots[i];
-        // YPUB:276-277: isxe = isx - ixmine + npxn + 1, isze = isz + itopoe (flat: isz0 + npzn)
+        // YPUB:276-277: isxe = isx - ixmine + npxn + 1, isze = isz + itopoe(isxe)
+        const int* it = itopoe.data() + block_x0[s.block];
         desc[i].sx = s.isx - s.ixmine + np;
-        desc[i].sz = isz0 + top - 1;
+        desc[i].sz = isz0 + it[desc[i].sx] - 1;
         desc[i].nt = nt_run;
-        // YPUB:2-16: receivers at row itopoe + irz0 of every window column
+        // YPUB:2-16: receivers at row itopoe(i + npxn) + irz0 of every window column
         rx[i].resize(s.nxe);
-        rz[i].assign(s.nxe, top + irz0 - 1);
-        for (int c = 0; c < s.nxe; c++) rx[i][c] = np + c;
+        rz[i].resize(s.nxe);
+        for (int c = 0; c < s.nxe; c++) {
+            rx[i][c] = np + c;
+            rz[i][c] = it[np + c] + irz0 - 1;
+        }
         desc[i].nrec = s.nxe;
         desc[i].rec_x = rx[i].data();
         desc[i].rec_z = rz[i].data();

@@ -165,11 +165,12 @@ def test_snapshots_equal_truncated_runs_viscoacoustic():
             assert bits_equal(snap, full[npx:-npx, npx:-npx]), (field, k)
 
 
-@pytest.mark.parametrize("mode", ["abc", "fsbc"])
-def test_iso_forward_program_against_restatement(tmp_path, mode):
-    """iso_forward on a yang_version card of three aperture shots: the merged SU files hold the
-    FP32 restatement's vx / vz traces bit for bit, with YPUB:1555-1596's headers (no cdp); the
-    last snapshot of the last shot equals the restatement's wavefield after that step."""
+@pytest.mark.parametrize("mode,hilly", [("abc", False), ("fsbc", False), ("abc", True), ("fsbc", True)])
+def test_iso_forward_program_against_restatement(tmp_path, mode, hilly):
+    """iso_forward on a yang_version card of three aperture shots, flat or with topography: the
+    merged SU files hold the FP32 restatement's vx / vz traces bit for bit, with YPUB:1555-1596's
+    headers (no cdp); the last snapshot of the last shot equals the restatement's wavefield after
+    that step."""
     from test_fileio import ISOCARD
     nx, nz = 120, 80
     rng = np.random.default_rng(12)
@@ -180,7 +181,9 @@ def test_iso_forward_program_against_restatement(tmp_path, mode):
     rho = (2000.0 + 300.0 * rng.random((nx, nz))).astype(np.float32)
     for name, a in (("vp", vp), ("vs", vs), ("rho", rho)):
         a.tofile(tmp_path / f"{name}.bin")
-    np.zeros(nx, np.float32).tofile(tmp_path / "topo.bin")
+    x = np.arange(nx)
+    topo = (10.0 * np.round(2 + 1.5 * np.cos(x / 10.0))).astype(np.float32) if hilly else np.zeros(nx, np.float32)
+    topo.tofile(tmp_path / "topo.bin")
     (tmp_path / "snap").mkdir()
     card = ISOCARD.format(d=str(tmp_path), mode=mode, ztop="90.0" if mode == "abc" else "0000.0", rgau=12)
     (tmp_path / "iso.par").write_text(card)
@@ -193,15 +196,17 @@ def test_iso_forward_program_against_restatement(tmp_path, mode):
     isx0, isz0, irz0 = nint(p.sx0 / p.dx) + 1, nint(p.sz0 / p.dz) + 1, nint(p.rz0 / p.dz) + 1
     idecay, idtsnap = nint(p.decay / p.dt), nint(p.dtsnap / p.dt)
     fs = mode == "fsbc"
-    kw = dict(nrz0=irz0, idecay=idecay, rgau=p.rgau, fsbc=fs, npz_top=top)
+    kw = dict(nrz0=irz0, idecay=idecay, rgau=p.rgau, fsbc=fs, npz_top=top, topo=topo)
+    itopo_at = lambda col: nint(float(np.float32(topo[min(max(col, 1), nx) - 1]) / np.float32(p.dz))) + top
     refs = []
     for i in range(1, p.nshot + 1):
         isx = isx0 + nint((i - 1) * p.dsx / p.dx)
         ixmine, ixmaxe = isx + nint(p.offset_min / p.dx), isx + nint(p.offset_max / p.dx)
         args = (vp, vs, rho, p.dx, p.dz, p.dt, p.f0)
-        r1, r2, _ = ol.iso_forward(*args, p.nt, np_, np_, isx - ixmine + np_ + 1, isz0 + top, ixmine=ixmine,
+        isze = isz0 + itopo_at(isx + 1)  # isz + itopoe(isxe): window column isxe reads model column isx + 1
+        r1, r2, _ = ol.iso_forward(*args, p.nt, np_, np_, isx - ixmine + np_ + 1, isze, ixmine=ixmine,
                                    ixmaxe=ixmaxe, **kw)
-        refs.append((isx, ixmine, ixmaxe - ixmine + 1, r1, r2))
+        refs.append((isx, ixmine, ixmaxe - ixmine + 1, r1, r2, isze))
     for stem, which in (("vx", 3), ("vz", 4)):
         assert not (tmp_path / f"{stem}_tmp1.su").exists()
         raw = open(tmp_path / f"shot_{stem}.su", "rb").read()
@@ -221,5 +226,5 @@ def test_iso_forward_program_against_restatement(tmp_path, mode):
     last = idtsnap * ((p.nt + idecay) // idtsnap)
     snap = read(tmp_path / "snap" / f"vx_{last}", (nxe, nz))
     _, _, fin = ol.iso_forward(vp, vs, rho, p.dx, p.dz, p.dt, p.f0, last - idecay, np_, np_, isx - ixmine + np_ + 1,
-                               isz0 + top, ixmine=ixmine, ixmaxe=ixmine + nxe - 1, want_final=True, **kw)
+                               refs[-1][5], ixmine=ixmine, ixmaxe=ixmine + nxe - 1, want_final=True, **kw)
     assert bits_equal(snap, fin[np_:np_ + nxe, top:top + nz])
