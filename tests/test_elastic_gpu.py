@@ -236,3 +236,34 @@ def test_topography_bitexact_against_restatement(fsbc, top):
     # the flat run records at the same (topography-following) receivers: compare with the flat
     # restatement's wavefield there is not possible through records, so check it differs
     assert not np.array_equal(f1, r1)
+
+
+def test_elastic_options_validate_their_arguments():
+    """The elastic scheme's options reject what the kernels cannot model, with SFD_ERR_ARG, and
+    leave the context usable."""
+    model = imodel(seed=11, nx=40, nz=30)
+    npx = 8
+    vp, vs, rho = (S.pad_model(a, npx, npx, npx, npx) for a in model)
+    nx, nz = vp.shape
+    with S.Engine(S.ELASTIC_2D, nx, nz, 10.0, 10.0, 5e-4, npx, order=10, f0=20.0) as e:
+        e.set_model_elastic(vp, vs, rho)
+        for bad in (lambda: e.set_gauss_radius(0),
+                    lambda: e.set_free_surface(-1),
+                    lambda: e.set_free_surface(nz),  # too deep for the bottom sponge and stencil
+                    lambda: e.set_topography(np.full(nx, 0, np.int32)),
+                    lambda: e.set_topography(np.full(nx, nz, np.int32))):
+            with pytest.raises(S.SfdError) as ex:
+                bad()
+            assert ex.value.status == S.ERR_ARG
+        # abc mode needs itopo >= pml (its first updated row is itopo - pml - 1)
+        with pytest.raises(S.SfdError):
+            e.set_topography(np.full(nx, npx - 1, np.int32))
+        e.set_topography(None)
+        rx = np.arange(npx, nx - npx, dtype=np.int32)
+        e.set_shots([S.ShotSpec(20, 12, rx, np.full_like(rx, npx), S.wavelet(S.WAVELET_ISO, 60, 5e-4, 20.0, delay=20))])
+        assert np.abs(e.forward()).max() > 0
+    with S.Engine(S.ACOUSTIC_2D, nx, nz, 10.0, 10.0, 5e-4, npx, order=8) as a:
+        for bad in (lambda: a.set_gauss_radius(10), lambda: a.set_free_surface(1),
+                    lambda: a.set_topography(np.full(nx, 9, np.int32))):
+            with pytest.raises(S.SfdError):
+                bad()
