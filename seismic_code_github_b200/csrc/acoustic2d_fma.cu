@@ -599,8 +599,15 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
 
     // which tile t is: shot, tile index within the shot, origin; false if beyond the aperture
     auto locate = [&](int t, int& shot, int& tile, int& x0, int& z0) -> bool {
-        const int slot = t / per_shot;
-        tile = t - slot * per_shot;
+        int slot, k;
+        if (a.tile_major) {
+            k = t / active;
+            slot = t - k * active;
+        } else {
+            slot = t / per_shot;
+            k = t - slot * per_shot;
+        }
+        tile = a.tile_order ? __ldg(a.tile_order + k) : k;
         shot = a.slot_to_shot[slot];
         const int tx_i = tile / a.L.ntz;
         x0 = tx_i * T::TX;

@@ -66,6 +66,8 @@ struct sfd_ctx {
     int* d_rec_z = nullptr;
     int* d_trp = nullptr;      // per-tile receiver CSR pointers
     int* d_tri = nullptr;      // per-tile receiver indices
+    int* d_torder = nullptr;   // FMA kernel's forward tile order: interior tiles, then edge tiles
+    int tile_major = 1;        // forward steps of the FMA kernel: tile-major over d_torder
     float* d_rec_tn = nullptr; // [nt][nrec] per shot
     float* d_rec_nt = nullptr; // [nrec][nt] per shot (output layout)
     float* d_state = nullptr;  // 6 fields: p0 p1 vx0 vx1 vz0 vz1, each nshot * shot_stride
@@ -256,7 +258,7 @@ float sponge3(const sfd_grid& g, int x, int y, int z) {
 
 void free_shot_buffers(sfd_ctx* c) {
     dfree(c->d_shots); dfree(c->d_slot); dfree(c->d_ident); dfree(c->d_wav);
-    dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri); dfree(c->d_rec_y);
+    dfree(c->d_rec_x); dfree(c->d_rec_z); dfree(c->d_trp); dfree(c->d_tri); dfree(c->d_torder); dfree(c->d_rec_y);
     dfree(c->d_rec_tn); dfree(c->d_rec_nt); dfree(c->d_state); dfree(c->d_stamps); dfree(c->d_src_pre);
     dfree(c->d_rec2_tn); dfree(c->d_rec2_nt);
     c->rec2_ready = false;
@@ -345,6 +347,8 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.rec_z = c->d_rec_z;
     a.tile_rec_ptr = c->d_trp;
     a.tile_rec_idx = c->d_tri;
+    a.tile_major = c->tile_major;
+    a.tile_order = c->tile_major ? c->d_torder : nullptr;
     a.records = c->d_rec_tn;
     a.tm_p = c->tmaps[i];
     a.tm_vx = c->tmaps[2 + i];
@@ -965,6 +969,8 @@ Acou2DArgs make_adj_args(const sfd_ctx* ctx, const GradRange& r, int k, const fl
     a.tm_vx = ctx->adj_tmaps[2 + i];
     a.tm_vz = ctx->adj_tmaps[4 + i];
     a.slot_to_shot = r.slots;
+    a.tile_major = 0;
+    a.tile_order = nullptr;
     a.records = nullptr;
     a.src_pre = nullptr;
     a.div_out = nullptr;
@@ -2112,6 +2118,27 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         }
         trp.push_back((int)tri.size());
     }
+    // Tile order of the FMA kernel's forward steps: CTAs are numbered tile-major (the active
+    // shots' copies of one tile are consecutive) over a tile order that puts the tiles whose
+    // stencil reaches neither the sponge nor a grid edge (the kernel's interior body) first and
+    // the edge tiles after them, so that nearly all CTAs resident at one time run the same code
+    // path.  On 64 shots of 612 x 2148 this is 3% faster than shot-major numbering in natural
+    // order; either change alone gains nothing.  The adjoint steps keep shot-major natural order,
+    // and SFD_TILE_MAJOR=0 in the environment selects it for the forward steps too.
+    std::vector<int> torder;
+    {
+        const int R = ctx->radius, RQ = (R + 3) & ~3, E = std::max(ctx->g.pml, R);
+        int nxs = 0;
+        for (const auto& d : hs) nxs = std::max(nxs, d.nx);
+        for (int pass = 0; pass < 2; pass++)
+            for (int t = 0; t < ntiles; t++) {
+                const int x0 = (t / L.ntz) * L.tx, z0 = (t % L.ntz) * L.tz;
+                const bool inner = x0 - R >= E && x0 + L.tx + R <= nxs - E && z0 - RQ >= E && z0 + L.tz + RQ <= nz - E;
+                if (inner == (pass == 0)) torder.push_back(t);
+            }
+        ctx->tile_major = 1;
+        if (const char* env = std::getenv("SFD_TILE_MAJOR")) ctx->tile_major = std::atoi(env) != 0;
+    }
     // source scale ((dt * DEN) * Vp) in float, AFD:250
     for (auto& d : hs) {
         if (ctx->have_model) {
@@ -2150,7 +2177,7 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
     int rc;
     if ((rc = up(&ctx->d_shots, hs)) || (rc = up(&ctx->d_slot, order)) || (rc = up(&ctx->d_ident, ident)) ||
         (rc = up(&ctx->d_wav, wav)) || (rc = up(&ctx->d_rec_x, rx)) || (rc = up(&ctx->d_rec_z, rz)) ||
-        (rc = up(&ctx->d_trp, trp)) || (rc = up(&ctx->d_tri, tri)))
+        (rc = up(&ctx->d_trp, trp)) || (rc = up(&ctx->d_tri, tri)) || (rc = up(&ctx->d_torder, torder)))
         return rc;
     const size_t rec_bytes = sizeof(float) * std::max<long long>(1, rec_total);
     CK(cudaMalloc(&ctx->d_rec_tn, rec_bytes));

@@ -241,6 +241,11 @@ struct Acou2DArgs {
     const int* rec_x; const int* rec_z;
     const int* tile_rec_ptr;   // per shot: ntiles + 1 offsets into tile_rec_idx
     const int* tile_rec_idx;   // receiver index within the shot
+    // FMA kernel's CTA numbering: tile_major 0 = CTA t takes position k = t % T of slot t / T
+    // (T tiles per shot), 1 = position k = t / active of slot t % active; position k is tile
+    // tile_order[k] (tile k when tile_order is NULL)
+    int tile_major;
+    const int* tile_order;
     float* records;            // [nt][nrec] per shot at ShotDev::rec_base
     int step;
     float* div_out;            // optional: D = rdx S-x Vx + rdz S-z Vz of this step (field layout)

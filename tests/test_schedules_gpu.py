@@ -4,12 +4,14 @@ tuner picks the faster schedule at run time; SFD_FMA_STAGES forces one, so each 
 must stay within the forward tolerance of the oracle restatement (relative L2 <= 1e-5), at every
 order, with variable density, on sponge-free interior tiles and for uneven shots, and carry the
 adjoint gradient to within 1e-4 of the FP64 adjoint oracle (the gradient's forward and its
-recomputation run under the forced schedule)."""
+recomputation run under the forced schedule).  Forward steps number their CTAs tile-major by
+default (SFD_TILE_MAJOR=0 selects shot-major); every case runs under both numberings, and the
+two must give the same bits."""
 import numpy as np
 import pytest
 
 import oracle_lib as ol
-from conftest import rel_l2
+from conftest import bits_equal, rel_l2
 from seismic_code_github_b200 import seisfd as S
 from seismic_code_github_b200 import workloads as W
 
@@ -19,10 +21,12 @@ TOL_FWD = 1e-5
 SCHEDULES = [1, 2]
 
 
-@pytest.fixture(params=SCHEDULES)
+@pytest.fixture(params=[(s, m) for s in SCHEDULES for m in (1, 0)], ids=lambda p: f"s{p[0]}-tm{p[1]}")
 def schedule(request, monkeypatch):
-    monkeypatch.setenv("SFD_FMA_STAGES", str(request.param))
-    return request.param
+    s, m = request.param
+    monkeypatch.setenv("SFD_FMA_STAGES", str(s))
+    monkeypatch.setenv("SFD_TILE_MAJOR", str(m))
+    return s
 
 
 @pytest.mark.parametrize("order", [16, 10, 8, 4, 2])
@@ -43,19 +47,24 @@ def test_all_orders_variable_density(schedule, order):
     assert err <= TOL_FWD
 
 
-def test_interior_tiles_uneven_shots(schedule):
+def uneven_shots_case():
     NX, NZ, PML = 300, 200, 20
     v = W.layered_model(NX, NZ, 5, 1800.0, 3500.0, seed=5, anomalies=2, radius=12.0, amp=250.0, dx=10.0)
     vp = W.pad_edges(v, PML, PML)
     den = np.full_like(vp, 2200.0)
     rx = np.arange(PML, vp.shape[0] - PML, dtype=np.int32)
     rz = np.full_like(rx, PML + 2)
-    shots, refs = [], []
+    shots = []
     for i, (sx, sz, nt) in enumerate(((PML + 40, PML + 3, 260), (PML + 150, PML + 100, 200), (PML + 290, PML + 5, 130))):
         w = S.wavelet(S.WAVELET_RIC, nt, 1e-3, 20.0 + i, 50)
         shots.append(S.ShotSpec(sx, sz, rx, rz, w))
-        ref, _, _ = ol.afd_forward(vp.shape[0], vp.shape[1], PML, nt, 10.0, 10.0, 1e-3, vp, den, w, sx, sz, rx, rz)
-        refs.append(ref)
+    return vp, den, PML, shots
+
+
+def test_interior_tiles_uneven_shots(schedule):
+    vp, den, PML, shots = uneven_shots_case()
+    refs = [ol.afd_forward(vp.shape[0], vp.shape[1], PML, s.nt, 10.0, 10.0, 1e-3, vp, den, s.wavelet, s.sx, s.sz,
+                           s.rec_x, s.rec_z)[0] for s in shots]
     with S.Engine(S.ACOUSTIC_2D, vp.shape[0], vp.shape[1], 10.0, 10.0, 1e-3, PML, order=16) as e:
         e.set_model(vp, den)
         e.set_shots(shots)
@@ -89,3 +98,21 @@ def test_gradient_against_fp64_adjoint(schedule):
     err = rel_l2(g, g64)
     print(f"schedule {schedule}: gradient relL2 vs FP64 adjoint {err:.2e}")
     assert err <= 1e-4 and abs(misfit - J) <= 1e-3 * J
+
+
+def test_tile_numbering_gives_identical_bits(monkeypatch):
+    """Tile-major and shot-major CTA numbering visit the same tiles with the same arithmetic: the
+    records of a multi-shot forward and the batched gradient agree bit for bit."""
+    vp, den, PML, shots = uneven_shots_case()
+    out = {}
+    for m in (1, 0):
+        monkeypatch.setenv("SFD_TILE_MAJOR", str(m))
+        with S.Engine(S.ACOUSTIC_2D, vp.shape[0], vp.shape[1], 10.0, 10.0, 1e-3, PML, order=16) as e:
+            e.set_model(vp, den)
+            e.set_shots(shots)
+            rec = e.forward().copy()
+            e.set_model((vp * 1.01).astype(np.float32), den)
+            J, g, _ = e.gradient(rec)
+        out[m] = (rec, J, g)
+    assert bits_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] and bits_equal(out[0][2], out[1][2])
