@@ -111,6 +111,14 @@ __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, 
         : "memory");
 }
 
+// L2 prefetch of a box (no shared-memory destination, no completion to wait for); the
+// coordinates follow the rules of tma_load_3d
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     unsigned ok;
     asm volatile(
@@ -630,6 +638,15 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
         tma_load_3d(st + T::OFF_VX, &a.tm_vx, gz + z0, gx + x0 - R, shot, bar);
         tma_load_3d(st + T::OFF_VZ, &a.tm_vz, gz + z0 - T::RQ, gx + x0, shot, bar);
     };
+    // thread 0: prefetch the three boxes of tile t into L2 (for the CTA that will take tile t)
+    auto prefetch = [&](int t) {
+        int shot, tile, x0, z0;
+        if (!locate(t, shot, tile, x0, z0)) return;
+        const int gx = a.L.gx, gz = a.L.gz;
+        tma_prefetch_3d(&a.tm_p, gz + z0 - T::HZ, gx + x0 - T::HX, shot);
+        tma_prefetch_3d(&a.tm_vx, gz + z0, gx + x0 - R, shot);
+        tma_prefetch_3d(&a.tm_vz, gz + z0 - T::RQ, gx + x0, shot);
+    };
 
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sptr(bars)) : "memory");
@@ -638,6 +655,8 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
     }
     __syncthreads();
     if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+    if (NST == 1 && tid == 0 && a.l2_ahead > 0 && (int)blockIdx.x + a.l2_ahead < total)
+        prefetch(blockIdx.x + a.l2_ahead);
 
     unsigned phase = 0;  // bit s: parity of the next completion of stage s's barrier
     for (int i = 0;; i++) {

@@ -68,6 +68,7 @@ struct sfd_ctx {
     int* d_tri = nullptr;      // per-tile receiver indices
     int* d_torder = nullptr;   // FMA kernel's forward tile order: interior tiles, then edge tiles
     int tile_major = 1;        // forward steps of the FMA kernel: tile-major over d_torder
+    int l2_ahead = 0;          // FMA kernel, one tile per CTA: L2 prefetch distance in CTAs
     float* d_rec_tn = nullptr; // [nt][nrec] per shot
     float* d_rec_nt = nullptr; // [nrec][nt] per shot (output layout)
     float* d_state = nullptr;  // 6 fields: p0 p1 vx0 vx1 vz0 vz1, each nshot * shot_stride
@@ -349,6 +350,7 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.tile_rec_idx = c->d_tri;
     a.tile_major = c->tile_major;
     a.tile_order = c->tile_major ? c->d_torder : nullptr;
+    a.l2_ahead = c->l2_ahead;
     a.records = c->d_rec_tn;
     a.tm_p = c->tmaps[i];
     a.tm_vx = c->tmaps[2 + i];
@@ -2138,6 +2140,16 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
             }
         ctx->tile_major = 1;
         if (const char* env = std::getenv("SFD_TILE_MAJOR")) ctx->tile_major = std::atoi(env) != 0;
+    }
+    // Each CTA of the one-tile-per-CTA schedule prefetches into L2 the boxes of the CTA one wave
+    // of resident CTAs (two per SM) later, so that its TMA loads find them in L2 rather than in
+    // HBM.  SFD_L2_AHEAD in the environment sets another distance (0: no prefetch).
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        ctx->l2_ahead = 2 * sms;
+        if (const char* env = std::getenv("SFD_L2_AHEAD")) ctx->l2_ahead = std::max(0, std::atoi(env));
     }
     // source scale ((dt * DEN) * Vp) in float, AFD:250
     for (auto& d : hs) {

@@ -246,6 +246,8 @@ struct Acou2DArgs {
     // tile_order[k] (tile k when tile_order is NULL)
     int tile_major;
     const int* tile_order;
+    int l2_ahead;              // one-tile-per-CTA schedule: CTA t prefetches CTA t + l2_ahead's
+                               // boxes into L2 (0: no prefetch)
     float* records;            // [nt][nrec] per shot at ShotDev::rec_base
     int step;
     float* div_out;            // optional: D = rdx S-x Vx + rdz S-z Vz of this step (field layout)
