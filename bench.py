@@ -439,6 +439,48 @@ def measure_elastic(args, dev):
     return out
 
 
+def measure_vti(args, dev):
+    """The VTI modeller's .par geometry (de-multiple/convolution_srm/vti_qa_2d_c3_demo1): 64 shots
+    of 600 traces on a seeded synthetic 300 x 300 VTI model, batched in one launch per time step
+    (the fused u / q step of csrc/vti2d.cu, reference operation order).  The record length is cut
+    from the card's 10000 to 2000 samples; the per-step cost does not depend on it.  The CPU figure
+    is the restated modeller (oracle/vti_oracle.cpp, OpenMP) on one shot."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.vti_card(nshot=args.vti_nshot, nt=args.vti_nt)
+    args_ = (c["vz"], c["eps"], c["delta"], c["dx"], c["dz"], c["dt"], c["f0"], c["nt"], c["bounds"])
+    S.vti_forward(*args_, c["shots"][:1], device=dev)  # warm-up (module load)
+    ms, t = [], None
+    for _ in range(args.vti_steps):
+        _, t = S.vti_forward(*args_, c["shots"], device=dev)
+        ms.append(t["loop_ms"])
+    pts = t["point_updates"]
+    gpts = pts / (float(np.median(ms)) / 1e3) / 1e9
+    nxl, nxr, nzu, nzd = c["bounds"]
+    nx = 600 + nxl + nxr - 2
+    nz = c["vz"].shape[1] + nzu + nzd - 2
+    out = {"workload": f"VTI pseudo-acoustic (vti_qa_2d_modelling_new.par geometry): 300x300 model, {nz}x{nx} "
+                       f"grid per shot, {len(c['shots'])} shots of 600 traces, nt {c['nt']} (+ source delay steps)",
+           "gpts_per_s": gpts, "shots_per_s": len(c["shots"]) / (float(np.median(ms)) / 1e3),
+           "loop_ms": float(np.median(ms)), "launches": t["launches"], "total_ms": t["total_ms"],
+           "bytes_per_point": 36, "hbm_frac_of_measured": 36 * gpts / read_peaks()[0],
+           "parity": "bit-exact vs FP32 restatement (tests/test_vti_gpu.py)"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as ol
+        steps = args.vti_cpu_steps
+        sh = c["shots"][len(c["shots"]) // 2]
+        t0 = time.perf_counter()
+        ol.vti_forward(c["vz"], c["eps"], c["delta"], c["dx"], c["dz"], c["dt"], c["f0"], steps, c["bounds"], *sh)
+        wall = time.perf_counter() - t0
+        nwt = int(round(2 * 0.07 / c["dt"])) + 1
+        out["cpu_baseline"] = {"value": nx * nz * (steps + (nwt - 1) // 2) / max(wall, 1e-9) / 1e9, "unit": "Gpts/s",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"restated VTI modeller (oracle/vti_oracle.cpp, OpenMP) on one shot, "
+                                         f"{steps} record samples plus the source delay steps"}
+    return out
+
+
 def measure_q_gradient(args, dev):
     """Config-3 geometry: the viscoacoustic gradient d misfit / d vp and d misfit / d (1/Q) of 16
     shots (uneven record lengths), observed data from the Q field scaled by 0.8, batched (one
@@ -701,6 +743,8 @@ def run_ours(args, world, rank, local):
         line["viscoelastic"] = measure_viscoelastic(args, dev)
     if world == 1 and args.el_steps > 0:
         line["elastic"] = measure_elastic(args, dev)
+    if world == 1 and args.vti_steps > 0:
+        line["vti"] = measure_vti(args, dev)
     if world == 1 and args.qg_steps > 0:
         line["viscoacoustic_gradient"] = measure_q_gradient(args, dev)
     if world == 1 and args.d3_steps > 0:
@@ -739,6 +783,10 @@ def main():
     ap.add_argument("--d3-cpu-steps", type=int, default=3)
     ap.add_argument("--e-steps", type=int, default=1, help="timed visco-elastic forwards (0 = skip)")
     ap.add_argument("--el-steps", type=int, default=1, help="timed isotropic elastic forwards (0 = skip)")
+    ap.add_argument("--vti-steps", type=int, default=1, help="timed VTI surveys (0 = skip)")
+    ap.add_argument("--vti-nshot", type=int, default=64)
+    ap.add_argument("--vti-nt", type=int, default=2000)
+    ap.add_argument("--vti-cpu-steps", type=int, default=60)
     ap.add_argument("--qg-steps", type=int, default=1, help="timed viscoacoustic gradients (0 = skip)")
     ap.add_argument("--qg-nshot", type=int, default=16)
     ap.add_argument("--qg-nt-scale", type=float, default=1.0)

@@ -321,6 +321,36 @@ int sfd_su_write_ex(const char* path, const float* traces, int ntr, int nt, int 
  * reference does. */
 int sfd_su_merge(const char* out_path, const char* const* in_paths, int n, int delete_inputs);
 
+/* ---- VTI pseudo-acoustic modeller (de-multiple/convolution_srm/vti_qa_2d_c3_demo1) ----
+ * The coupled u / q second-order system with 10th-order second derivatives inside and split PML
+ * fields on the four sides (VTI_multishot_qacoustic_fd_subroutine_c3.f90 = VS, main program VM).
+ * One call runs every shot of a survey, batched in one launch per time step; it replaces the shot
+ * loop of multi_shot_modelling (VM:12-180) and single_shot_modelling (VM:190-560), whose .par
+ * card gives these fields (VS:342-425).  Grid numbers are the reference's, 1-based: nsx, nsz0 and
+ * nrz0 as VM:145-147 and 158 compute them, xmin / xmax the shot's aperture columns (VM:162-163).
+ * Model arrays are [nx_v][nz_v], x-major (z fastest), host pointers.  records (host) receives
+ * [shot][xmax - xmin + 1][nt]: u on the receiver row (VM:446-453).  Every shot must have the same
+ * xmax - xmin.  Orders: explicit 10, pml_1st 9 or 10, pml_2nd 10 (the stencils are written out
+ * with five coefficients, VS:511-551); nx_bound_r and nz_bound_d >= 2 (VM:248-249). */
+typedef struct {
+    int nx_v, nz_v;        /* model grid                                                      */
+    float dx, dz, dt, f0;  /* metres, seconds, Hz                                             */
+    int nt;                /* record length                                                   */
+    int nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d;  /* PML cells, nint(thickness / dx) (VM:136-141) */
+    int order_explicit, order_pml_1st, order_pml_2nd;
+} sfd_vti_par;
+
+typedef struct {
+    int nsx, nsz0, nrz0;   /* source column and row, receiver row                             */
+    int xmin, xmax;        /* aperture: record columns xmin + 1 .. xmax + 1 of the model (VS:300) */
+} sfd_vti_shot;
+
+/* FD coefficients of coefficient_2nd (first = 0, order/2 values) or coefficient_1st (first = 1,
+ * (order+1)/2 values), VS:1264-1472, as the modeller computes them in single precision. */
+int sfd_vti_coefficients(int order, int first, float* out);
+int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilon, const float* delta, int nshot,
+                    const sfd_vti_shot* shots, int device, float* records, sfd_timing* timing);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,22 @@ typedef struct {
     const float* topo;             // surface depth (m) per model column (nx values), NULL: flat;
                                    // itopo = nint(topo/dz) + npzn per window column (YPUB:270-272)
 } OracleIsoCfg;
+// VTI pseudo-acoustic modeller (de-multiple/convolution_srm/vti_qa_2d_c3_demo1): the reference's
+// parameters of one shot.  Model arrays [nx_v][nz_v] x-major; grid numbers 1-based as in the
+// Fortran (nsx, nsz0 and nrz0 from VM:145-147, xmin / xmax the shot's aperture columns, VM:162-163);
+// record[trace][nt] for the xmax - xmin + 1 traces.
+typedef struct {
+    int nx_v, nz_v, nt;
+    float dx, dz, dt, f0;
+    int nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d;  // PML cells (VM:136-141)
+    int order_explicit, order_pml_1st, order_pml_2nd;    // 10, 9 or 10, 10
+    int nsx, nsz0, nrz0, xmin, xmax;
+} OracleVtiCfg;
+// the FD coefficients of VS:1264-1472 (first = 0: coefficient_2nd(order), 1: coefficient_1st)
+int oracle_vti_coef_f32(int order, int first, float* out);
+int oracle_vti_coef_f64(int order, int first, double* out);
+int oracle_vti_f32(const OracleVtiCfg* c, const float* vz, const float* eps, const float* delta, float* record);
+int oracle_vti_f64(const OracleVtiCfg* c, const float* vz, const float* eps, const float* delta, double* record);
 // the five arrays of the time loop after substagger and the PML smoothing (YPUB:323-634):
 // busg2e, busg1e, lambmusg, lambsg, musge, each [NX][NZ] of the padded window
 int oracle_iso_prepare_f32(const OracleIsoCfg* c, const float* vp, const float* vs, const float* rho, float* out);

@@ -219,6 +219,50 @@ def iso_forward(vp, vs, rho, dx, dz, dt, f0, nt, npx, npz, isxe, isze, nrz0=1, i
     return r1, r2, fin
 
 
+class OracleVtiCfg(ctypes.Structure):
+    _fields_ = [("nx_v", ctypes.c_int), ("nz_v", ctypes.c_int), ("nt", ctypes.c_int), ("dx", ctypes.c_float),
+                ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nx_bound_l", ctypes.c_int),
+                ("nx_bound_r", ctypes.c_int), ("nz_bound_u", ctypes.c_int), ("nz_bound_d", ctypes.c_int),
+                ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int),
+                ("nsx", ctypes.c_int), ("nsz0", ctypes.c_int), ("nrz0", ctypes.c_int), ("xmin", ctypes.c_int),
+                ("xmax", ctypes.c_int)]
+
+
+def vti_coefficients(order, first, fp64=False):
+    """The FD coefficients of coefficient_2nd (first = 0) / coefficient_1st (first = 1)
+    (oracle/vti_oracle.cpp, VS:1264-1472)."""
+    L = lib()
+    k = (order + 1) // 2 if first else order // 2
+    out = np.zeros(k, np.float64 if fp64 else np.float32)
+    fn = L.oracle_vti_coef_f64 if fp64 else L.oracle_vti_coef_f32
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, _F64P if fp64 else _F32P]
+    if fn(order, 1 if first else 0, _p(out, _F64P if fp64 else _F32P)) != 0:
+        raise ValueError("unsupported order")
+    return out
+
+
+def vti_forward(vz, eps, delta, dx, dz, dt, f0, nt, bounds, nsx, nsz0, nrz0, xmin, xmax, orders=(10, 9, 10),
+                fp64=False):
+    """Restated VTI pseudo-acoustic modelling of one shot (oracle/vti_oracle.cpp).  Model arrays
+    (nx_v, nz_v) float32 x-major; bounds = (nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d) in
+    cells; nsx, nsz0, nrz0, xmin, xmax the reference's 1-based grid numbers.  Returns the record
+    [xmax - xmin + 1][nt] (u on the receiver row)."""
+    L = lib()
+    if not hasattr(L, "_vti_sig"):
+        tp = ctypes.POINTER(OracleVtiCfg)
+        L.oracle_vti_f32.argtypes = [tp, _F32P, _F32P, _F32P, _F32P]
+        L.oracle_vti_f64.argtypes = [tp, _F32P, _F32P, _F32P, _F64P]
+        L._vti_sig = True
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (vz, eps, delta)]
+    nx_v, nz_v = arrs[0].shape
+    cfg = OracleVtiCfg(nx_v, nz_v, nt, dx, dz, dt, f0, *bounds, *orders, nsx, nsz0, nrz0, xmin, xmax)
+    rec = np.zeros((xmax - xmin + 1, nt), np.float64 if fp64 else np.float32)
+    fn = L.oracle_vti_f64 if fp64 else L.oracle_vti_f32
+    if fn(ctypes.byref(cfg), *[_p(a) for a in arrs], _p(rec, _F64P if fp64 else _F32P)) != 0:
+        raise ValueError("oracle_vti rejected the configuration")
+    return rec
+
+
 class OracleAfd3Cfg(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("pml", ctypes.c_int),
                 ("nt", ctypes.c_int), ("radius", ctypes.c_int), ("dx", ctypes.c_float), ("dy", ctypes.c_float),

@@ -1,0 +1,426 @@
+// 2-D VTI pseudo-acoustic modelling for sm_100a: the coupled u / q second-order system of
+// de-multiple/convolution_srm/vti_qa_2d_c3_demo1 (VS = VTI_multishot_qacoustic_fd_subroutine_c3.f90,
+// VM = VTI_multishot_qacoustic_fd_main_c3.f90), every shot of a call in one launch per time step.
+//
+// Per time step the reference calls extrapolation_one_step_1 (new u from the current u and q,
+// VS:432-960) and then extrapolation_one_step_2 (new q from the current u and q, VS:965-1258).
+// Neither reads what the other writes -- step 2 takes the current u, not the new one -- so one
+// kernel does both: each thread owns one cell of one shot, reads the current u and q through
+// the 10th-order cross stencils (L1-cached, the cross of 21 + 21 values), updates the split PML
+// fields of its cell in place and writes the new u and q into the slots of the old ones.  The
+// operation order is the reference's as written, every multiply, add and divide rounded
+// separately (__fmul_rn, __fadd_rn, __fdiv_rn, __fsqrt_rn), so the records equal the FP32
+// restatement in oracle/vti_oracle.cpp bit for bit.  A one-thread-per-shot kernel adds the source
+// to the current u before each step (VM:420-424, 468-472); the receiver row is written by the
+// step kernel's threads on that row.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "seisfd.h"
+
+namespace {
+
+constexpr int kBX = 32, kBZ = 8;
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+struct VtiDev {
+    // per shot: fields u[2], q[2] (pitch x (nz + 10), cell (i, j) 1-based at (j+4)*pitch + i+4),
+    // model vz, eps, delta in the same layout, x-strip PML fields (nxl+nxr) x nz of u (4 pairs)
+    // and q (3 pairs), z-strip PML fields nx x (nzu+nzd) of u (4 pairs)
+    float* base;
+    long long field, shot_stride;  // floats per field slab, per shot
+    long long xs, zs;              // floats per x strip, per z strip
+    int pitch, nx, nz, nxl, nxr, nzu, nzd, range, nt;
+    float dx, dz, dt, L;
+    float cE[5], c2[5], c1[5];
+    const int* src;        // per shot: source cell i, j
+    const int* rrow;       // per shot: receiver row and whether it is the row-6 fallback
+    float* records;        // [shot][range][nt]
+};
+
+// one shot's arrays, by arithmetic on VtiDev::base (no pointer tables: the slot indices are
+// run-time values)
+struct VtiSlab {
+    float* p;
+    long long field, xs, zs;
+    __device__ float* u(int b) const { return p + b * field; }
+    __device__ float* q(int b) const { return p + (2 + b) * field; }
+    __device__ const float* vz() const { return p + 4 * field; }
+    __device__ const float* ep() const { return p + 5 * field; }
+    __device__ const float* de() const { return p + 6 * field; }
+    __device__ float* ux(int k, int b) const { return p + 7 * field + (2 * k + b) * xs; }
+    __device__ float* qx(int k, int b) const { return p + 7 * field + (8 + 2 * k + b) * xs; }
+    __device__ float* uz(int k, int b) const { return p + 7 * field + 14 * xs + (2 * k + b) * zs; }
+};
+
+__device__ __forceinline__ VtiSlab slab(const VtiDev& a, int s) {
+    return VtiSlab{a.base + (long long)s * a.shot_stride, a.field, a.xs, a.zs};
+}
+
+// second-derivative sum of VS:511-525: (c1 (f+1 + f-1 - 2 f0) + ... + c5 (...)) / h**2
+__device__ __forceinline__ float d2(const float* f, long long c, long long st, const float* cf, float h) {
+    const float two_f0 = fm(2.0f, __ldg(f + c));
+    float s = fm(cf[0], fs(fa(__ldg(f + c + st), __ldg(f + c - st)), two_f0));
+#pragma unroll
+    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(fa(__ldg(f + c + m * st), __ldg(f + c - m * st)), two_f0)));
+    return fd(s, fm(h, h));
+}
+// first-derivative sum of VS:567-578: (p1 (f+1 - f-1) + ... + p5 (...)) / h
+__device__ __forceinline__ float d1(const float* f, long long c, long long st, const float* cf, float h) {
+    float s = fm(cf[0], fs(__ldg(f + c + st), __ldg(f + c - st)));
+#pragma unroll
+    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(__ldg(f + c + m * st), __ldg(f + c - m * st))));
+    return fd(s, h);
+}
+
+// the split PML recurrences of one boundary cell (VS:651-663, 840-858): a1 (second-derivative
+// part), t2 (first-derivative part with the damping derivative), a2; k2s2 = speed^2 dt^2 (s2 h^2)
+// and k2dd = speed^2 dt^2 dd (s1 h), both formed by the caller in the reference's order
+__device__ __forceinline__ void pml_cell(float d, float dt, float h, float* a1, const float* a1o, float* t2,
+                                         const float* t2o, float* a2, const float* a2o, long long x, float k2s2,
+                                         float k2dd) {
+    const float h2 = fm(h, h);
+    const float d2dt = fm(fm(2.0f, d), dt);
+    const float P = fs(fa(fm(2.0f, h2), fm(d2dt, h2)), fm(fm(fm(d, d), h2), fm(dt, dt)));
+    const float Den = fa(h2, fm(d2dt, h2));
+    const float n1 = fd(fa(fs(fm(a1o[x], P), fm(h2, a1[x])), k2s2), Den);
+    const float P2 = fs(fa(fm(2.0f, h), fm(d2dt, h)), fm(fm(fm(dt, dt), h), fm(d, d)));
+    const float Den2 = fa(h, fm(d2dt, h));
+    const float nt = fd(fs(fs(fm(t2o[x], P2), fm(h, t2[x])), k2dd), Den2);
+    a1[x] = n1;
+    t2[x] = nt;
+    a2[x] = fa(fm(a2o[x], fs(1.0f, fm(d, dt))), fm(nt, dt));
+}
+
+__global__ void vti_inject_kernel(VtiDev a, int cu, float w) {
+    const int s = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    const VtiSlab p = slab(a, s);
+    const long long c = (long long)(a.src[2 * s + 1] + 4) * a.pitch + (a.src[2 * s] + 4);
+    p.u(cu)[c] = fa(p.u(cu)[c], w);
+}
+
+__global__ void __launch_bounds__(kBX * kBZ) vti_step_kernel(VtiDev a, int cu, int iit) {
+    const int i = blockIdx.x * kBX + threadIdx.x + 1, j = blockIdx.y * kBZ + threadIdx.y + 1, s = blockIdx.z;
+    if (i > a.nx || j > a.nz) return;
+    const int ou = 1 - cu;
+    const VtiSlab p = slab(a, s);
+    const long long c = (long long)(j + 4) * a.pitch + (i + 4), P = a.pitch;
+    const float* U = p.u(cu);
+    const float* Q = p.q(cu);
+    const float v = p.vz()[c], de = p.de()[c], ep = p.ep()[c];
+    const float dt = a.dt, dx = a.dx, dz = a.dz, L = a.L;
+    const int nx = a.nx, nz = a.nz, nxl = a.nxl, nxr = a.nxr, nzu = a.nzu, nzd = a.nzd;
+    const bool xin = i > nxl && i < nx - nxr + 1;
+    float un, qn;
+
+    // ---- extrapolation_one_step_1 (VS:432-960): new u ----
+    if (xin && j > nzu && j < nz - nzd + 1) {
+        const float sxu = d2(U, c, 1, a.cE, dx), szu = d2(U, c, P, a.cE, dz), sxq = d2(Q, c, 1, a.cE, dx);
+        un = fa(fs(fm(2.0f, U[c]), p.u(ou)[c]), fm(fm(fm(dt, dt), fm(v, v)), fa(fm(fa(1.0f, fm(2.0f, de)), fa(sxu, sxq)), szu)));
+    } else if (!xin) {
+        const bool left = i <= nxl;
+        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
+        const float vx = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, ep))));
+        float s1 = d1(U, c, 1, a.c1, dx);
+        const float s1q = d1(Q, c, 1, a.c1, dx);
+        float s2 = d2(U, c, 1, a.c2, dx);
+        const float sz2 = d2(U, c, P, a.c2, dz);
+        const float s2q = d2(Q, c, 1, a.c2, dx);
+        s1 = fa(s1, s1q);
+        s2 = fa(s2, s2q);
+        const float axis = fm((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
+        const float thick = fm((float)(left ? nxl : nxr), dx);
+        const int is = left ? i : i - (nx - nxr) + nxl;
+        const float A = fd(fm(3.0f, vx), fm(2.0f, thick));
+        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
+        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
+        const long long x = (long long)(j - 1) * (nxl + nxr) + (is - 1);
+        const float k2 = fm(fm(vn, vn), fm(dt, dt));
+        pml_cell(d, dt, dx, p.ux(0, ou), p.ux(0, cu), p.ux(2, ou), p.ux(2, cu), p.ux(1, ou), p.ux(1, cu), x,
+                 fm(k2, fm(s2, fm(dx, dx))), fm(fm(k2, dd), fm(s1, dx)));
+        float* a3 = p.ux(3, ou);
+        const float* a3o = p.ux(3, cu);
+        const float n3 = fa(fs(fm(2.0f, a3o[x]), a3[x]), fd(fm(fm(fm(v, v), fm(dt, dt)), fm(sz2, fm(dz, dz))), fm(dz, dz)));
+        a3[x] = n3;
+        un = fa(fa(p.ux(0, ou)[x], p.ux(1, ou)[x]), n3);
+    } else {
+        const bool top = j <= nzu;
+        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
+        const float sz1 = d1(U, c, P, a.c1, dx);  // divided by dx as written (VS:796, 880)
+        const float sx2 = d2(U, c, 1, a.c2, dx);
+        const float sz2 = d2(U, c, P, a.c2, dz);
+        const float sx2q = d2(Q, c, 1, a.c2, dx);
+        const float axis = fm((float)(top ? j - (nzu + 1) : j - (nz - nzd)), dz);
+        const float thick = fm((float)(top ? nzu : nzd), dz);
+        const int js = top ? j : j - (nz - nzd) + nzu;
+        const float A = fd(fm(3.0f, v), fm(2.0f, thick));
+        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
+        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
+        const long long z = (long long)(js - 1) * nx + (i - 1);
+        const float k2 = fm(fm(v, v), fm(dt, dt));
+        pml_cell(d, dt, dz, p.uz(0, ou), p.uz(0, cu), p.uz(2, ou), p.uz(2, cu), p.uz(1, ou), p.uz(1, cu), z,
+                 fm(k2, fm(sz2, fm(dz, dz))), fm(fm(k2, dd), fm(sz1, dz)));
+        float* a3 = p.uz(3, ou);
+        const float* a3o = p.uz(3, cu);
+        const float n3 = fa(fs(fm(2.0f, a3o[z]), a3[z]), fm(fm(fm(vn, vn), fm(dt, dt)), fa(sx2, sx2q)));
+        a3[z] = n3;
+        un = fa(fa(p.uz(0, ou)[z], p.uz(1, ou)[z]), n3);
+    }
+
+    // ---- extrapolation_one_step_2 (VS:965-1258): new q from the current u ----
+    if (xin) {
+        const float sxu = d2(U, c, 1, a.cE, dx), sxq = d2(Q, c, 1, a.cE, dx);
+        qn = fa(fs(fm(2.0f, Q[c]), p.q(ou)[c]), fm(fm(fm(dt, dt), fm(v, v)), fm(fm(2.0f, fs(ep, de)), fa(sxq, sxu))));
+    } else {
+        const bool left = i <= nxl;
+        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
+        const float vx = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, ep))));
+        float s1 = d1(Q, c, 1, a.c1, dx);
+        const float s1u = d1(U, c, 1, a.c1, dx);
+        float s2 = d2(Q, c, 1, a.c2, dx);
+        const float s2u = d2(U, c, 1, a.c2, dx);
+        s1 = fa(s1, s1u);
+        s2 = fa(s2, s2u);
+        const float axis = fm((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
+        const float thick = fm((float)(left ? nxl : nxr), dx);
+        const int is = left ? i : i - (nx - nxr) + nxl;
+        const float A = fd(fm(3.0f, vx), fm(2.0f, thick));
+        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
+        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
+        const long long x = (long long)(j - 1) * (nxl + nxr) + (is - 1);
+        const float k2 = fm(fs(fm(vx, vx), fm(vn, vn)), fm(dt, dt));
+        pml_cell(d, dt, dx, p.qx(0, ou), p.qx(0, cu), p.qx(2, ou), p.qx(2, cu), p.qx(1, ou), p.qx(1, cu), x,
+                 fm(k2, fm(s2, fm(dx, dx))), fm(fm(k2, dd), fm(s1, dx)));
+        qn = fa(p.qx(0, ou)[x], p.qx(1, ou)[x]);
+    }
+    p.u(ou)[c] = un;
+    p.q(ou)[c] = qn;
+
+    // ---- recording (VM:446-453, 494-501): new u on the receiver row ----
+    const int rr = a.rrow[2 * s], low = a.rrow[2 * s + 1];
+    if (j == rr && i > nxl && i <= nxl + a.range && iit <= a.nt && ((!low && iit >= 1) || (low && iit > 1)))
+        a.records[((long long)s * a.range + (i - nxl - 1)) * a.nt + (iit - 1)] = un;
+}
+
+// coefficient_2nd / coefficient_1st (VS:1264-1472): a(i,j) = i^p / p! (p = 2j or 2j-1) inverted
+// by successive Sherman-Morrison updates of the identity; coefficient(i) = 0.5 inv(a)(1, i)
+int coefficients(int order, int first, float* out) {
+    const int k = first ? (order + 1) / 2 : order / 2;
+    if (k < 1 || k > 8) return SFD_ERR_ARG;
+    float a[64], inv[64], temp[8], col[8], outer[64], upd[64];
+    for (int i = 1; i <= k; i++)
+        for (int j = 1; j <= k; j++) {
+            const int pw = first ? 2 * j - 1 : 2 * j;
+            float num = 1.0f, fact = 1.0f;
+            for (int m = 0; m < pw; m++) num = num * (float)i;
+            for (int m = 1; m <= pw; m++) fact = fact * (float)m;
+            a[(i - 1) * k + (j - 1)] = num / fact;
+        }
+    for (int q = 0; q < k * k; q++) inv[q] = 0.0f;
+    for (int d = 0; d < k; d++) inv[d * k + d] = 1.0f;
+    for (int i = 0; i < k; i++) {
+        for (int c = 0; c < k; c++) temp[c] = a[i * k + c];
+        temp[i] = temp[i] - 1.0f;
+        float den = 0.0f;
+        for (int r = 0; r < k; r++) den = den + temp[r] * inv[r * k + i];
+        den = den + 1.0f;
+        for (int r = 0; r < k; r++) col[r] = inv[r * k + i];
+        for (int r = 0; r < k; r++)
+            for (int c = 0; c < k; c++) outer[r * k + c] = col[r] * temp[c];
+        for (int r = 0; r < k; r++)
+            for (int c = 0; c < k; c++) {
+                float s = 0.0f;
+                for (int m = 0; m < k; m++) s = s + outer[r * k + m] * inv[m * k + c];
+                upd[r * k + c] = s / den;
+            }
+        for (int q = 0; q < k * k; q++) inv[q] = inv[q] - upd[q];
+    }
+    for (int i = 0; i < k; i++) {
+        float s = 0.0f;
+        for (int m = 0; m < k; m++) s = s + inv[m] * (m == i ? 0.5f : 0.0f);
+        out[i] = s;
+    }
+    return SFD_OK;
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int sfd_vti_coefficients(int order, int first, float* out) {
+    if (!out) return SFD_ERR_ARG;
+    return coefficients(order, first, out);
+}
+
+int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilon, const float* delta, int nshot,
+                    const sfd_vti_shot* shots, int device, float* records, sfd_timing* timing) {
+    const auto t_start = std::chrono::steady_clock::now();
+    if (!par || !vz || !epsilon || !delta || !shots || !records || nshot < 1) return SFD_ERR_ARG;
+    const sfd_vti_par& c = *par;
+    if (c.nx_v < 1 || c.nz_v < 1 || c.nt < 1 || !(c.dx > 0) || !(c.dz > 0) || !(c.dt > 0)) return SFD_ERR_ARG;
+    if (c.order_explicit != 10 || c.order_pml_2nd != 10 || (c.order_pml_1st != 9 && c.order_pml_1st != 10))
+        return SFD_ERR_UNSUPPORTED;  // the stencils are written out with five coefficients (VS:511-551)
+    if (c.nx_bound_l < 0 || c.nz_bound_u < 0 || c.nx_bound_r < 2 || c.nz_bound_d < 2) return SFD_ERR_ARG;
+    const int range = shots[0].xmax - shots[0].xmin + 1;
+    if (range < 1) return SFD_ERR_ARG;
+    for (int s = 0; s < nshot; s++)
+        if (shots[s].xmax - shots[s].xmin + 1 != range) return SFD_ERR_ARG;  // one grid for the batch
+    const int nxl = c.nx_bound_l, nxr = c.nx_bound_r, nzu = c.nz_bound_u, nzd = c.nz_bound_d;
+    const int nx = range + nxl + nxr - 2, nz = c.nz_v + nzu + nzd - 2;  // VM:248-249
+    if (nx <= 10 || nz <= 10) return SFD_ERR_ARG;
+
+    VtiDev a{};
+    a.nx = nx; a.nz = nz; a.nxl = nxl; a.nxr = nxr; a.nzu = nzu; a.nzd = nzd; a.range = range; a.nt = c.nt;
+    a.dx = c.dx; a.dz = c.dz; a.dt = c.dt;
+    a.L = std::log(1.0f / 1.0e-3f);  // log(1/R), R = 1.0E-3 (VS:14)
+    if (coefficients(10, 0, a.cE) || coefficients(c.order_pml_2nd, 0, a.c2) || coefficients(c.order_pml_1st, 1, a.c1))
+        return SFD_ERR_ARG;
+    a.pitch = (nx + 10 + 31) / 32 * 32;
+    a.field = (long long)a.pitch * (nz + 10);
+    a.xs = (long long)(nxl + nxr) * nz;
+    a.zs = (long long)nx * (nzu + nzd);
+    a.shot_stride = 7 * a.field + 14 * a.xs + 8 * a.zs;
+    a.shot_stride = (a.shot_stride + 31) / 32 * 32;
+
+    // per-shot windows (get_currshot_parameters, VS:268-338, and VM:405-408), source cells and
+    // receiver rows
+    std::vector<float> host((size_t)nshot * 3 * a.field, 0.0f);
+    std::vector<int> src(2 * nshot), rrow(2 * nshot);
+    for (int s = 0; s < nshot; s++) {
+        const sfd_vti_shot& sh = shots[s];
+        float* hv = host.data() + (size_t)s * 3 * a.field;
+        float* he = hv + a.field;
+        float* hd = he + a.field;
+        auto C = [&](int i, int j) { return (size_t)(j + 4) * a.pitch + (i + 4); };
+        for (int i = 1; i <= range; i++) {
+            int io = i + sh.xmin;
+            io = io < 1 ? 1 : (io > c.nx_v ? c.nx_v : io);
+            for (int j = 1; j <= c.nz_v; j++) {
+                const size_t m = (size_t)(io - 1) * c.nz_v + (j - 1);
+                hv[C(i + nxl, nzu + j)] = vz[m];
+                he[C(i + nxl, nzu + j)] = epsilon[m];
+                hd[C(i + nxl, nzu + j)] = delta[m];
+            }
+        }
+        for (int j = 1; j <= nzu; j++)
+            for (int i = 1; i <= nx; i++) hv[C(i, j)] = hv[C(i, nzu + 1)];
+        for (int j = nzu + c.nz_v + 1; j <= nz; j++)
+            for (int i = 1; i <= nx; i++) hv[C(i, j)] = hv[C(i, nzu + c.nz_v)];
+        for (int j = 1; j <= nz; j++)
+            for (int i = 1; i <= nxl; i++) hv[C(i, j)] = hv[C(nxl + 1, j)];
+        for (int j = 1; j <= nz; j++)
+            for (int i = nxl + range + 1; i <= nx; i++) hv[C(i, j)] = hv[C(nxl + range, j)];
+        for (int j = 1; j <= sh.nsz0 + nzu + 6 && j <= nz; j++)
+            for (int i = 1; i <= nx; i++) he[C(i, j)] = hd[C(i, j)] = 0.0f;
+        for (int j = 1; j <= nz; j++)
+            for (int i = 1; i <= nx; i++)
+                if (!(hv[C(i, j)] > 0.0f) || !std::isfinite(hv[C(i, j)]) || !std::isfinite(he[C(i, j)]) ||
+                    !std::isfinite(hd[C(i, j)]) || !(1.0f + 2.0f * he[C(i, j)] >= 0.0f) ||
+                    !(1.0f + 2.0f * hd[C(i, j)] >= 0.0f))
+                    return SFD_ERR_ARG;
+        src[2 * s] = sh.nsx - sh.xmin + nxl;  // VS:294-295
+        src[2 * s + 1] = sh.nsz0 + nzu;
+        if (src[2 * s] < 1 || src[2 * s] > nx || src[2 * s + 1] < 1 || src[2 * s + 1] > nz) return SFD_ERR_ARG;
+        const int r = sh.nrz0 + nzu;
+        rrow[2 * s] = r >= 6 ? r : 6;
+        rrow[2 * s + 1] = r >= 6 ? 0 : 1;
+        if (rrow[2 * s] > nz) return SFD_ERR_ARG;
+    }
+
+    // source samples (VM:420-424): exp(-(pi f0 (it - 0.07/dt) dt)^2) (1 - 2 (...)^2), it <= nwt
+    const int nwt = (int)std::lround((double)((2.0f * 0.07f) / c.dt)) + 1;
+    const int half = (int)std::lround((double)(nwt - 1) / 2.0);
+    const int NT = c.nt + half;
+    std::vector<float> w(nwt + 1, 0.0f);
+    for (int it = 1; it <= nwt; it++) {
+        const float b = ((3.1415926f * c.f0) * ((float)it - (0.07f / c.dt))) * c.dt;
+        w[it] = std::exp(-(b * b)) * (1.0f - 2.0f * (b * b));
+    }
+
+    if (cudaSetDevice(device) != cudaSuccess) return SFD_ERR_CUDA;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return SFD_ERR_CUDA;
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{st};
+    DevBuf<float> state, recs;
+    DevBuf<int> dsrc, drow;
+    const size_t total = (size_t)nshot * a.shot_stride;
+    const size_t rec_n = (size_t)nshot * range * c.nt;
+    if (state.alloc(total) != cudaSuccess || recs.alloc(rec_n) != cudaSuccess || dsrc.alloc(2 * nshot) != cudaSuccess ||
+        drow.alloc(2 * nshot) != cudaSuccess) {
+        cudaGetLastError();
+        return SFD_ERR_NOMEM;
+    }
+    long long h2d = 0;
+    if (cudaMemsetAsync(state.p, 0, total * sizeof(float), st) != cudaSuccess ||
+        cudaMemsetAsync(recs.p, 0, rec_n * sizeof(float), st) != cudaSuccess)
+        return SFD_ERR_CUDA;
+    for (int s = 0; s < nshot; s++) {
+        if (cudaMemcpyAsync(state.p + (size_t)s * a.shot_stride + 4 * a.field, host.data() + (size_t)s * 3 * a.field,
+                            3 * a.field * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return SFD_ERR_CUDA;
+        h2d += 3 * a.field * (long long)sizeof(float);
+    }
+    if (cudaMemcpyAsync(dsrc.p, src.data(), 2 * nshot * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(drow.p, rrow.data(), 2 * nshot * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return SFD_ERR_CUDA;
+    a.base = state.p; a.src = dsrc.p; a.rrow = drow.p; a.records = recs.p;
+
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const dim3 grid((nx + kBX - 1) / kBX, (nz + kBZ - 1) / kBZ, nshot), block(kBX, kBZ);
+    long long launches = 0;
+    cudaEventRecord(e0, st);
+    for (int it = 1; it <= NT; it++) {
+        const int cu = (it % 2 == 1) ? 1 : 0;  // odd steps: u2 / q2 current (VM:417-505)
+        if (it <= nwt) {
+            vti_inject_kernel<<<nshot, 32, 0, st>>>(a, cu, w[it]);
+            launches++;
+        }
+        vti_step_kernel<<<grid, block, 0, st>>>(a, cu, it - half);
+        launches++;
+    }
+    cudaEventRecord(e1, st);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(records, recs.p, rec_n * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    float ms = 0.0f;
+    if (err == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) return SFD_ERR_CUDA;
+    if (timing) {
+        std::memset(timing, 0, sizeof(*timing));
+        timing->loop_ms = ms;
+        timing->device_ms = ms;
+        timing->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        timing->point_updates = (double)nx * nz * NT * nshot;
+        timing->launches = launches;
+        timing->h2d_bytes = h2d;
+        timing->d2h_bytes = (long long)(rec_n * sizeof(float));
+        timing->graph = 0;
+        timing->kernel_variant = 70;
+    }
+    return SFD_OK;
+}
+
+}  // extern "C"

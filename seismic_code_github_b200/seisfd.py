@@ -99,6 +99,20 @@ class Timing(ctypes.Structure):
                 ("graph", ctypes.c_int), ("kernel_variant", ctypes.c_int)]
 
 
+class VtiPar(ctypes.Structure):
+    """sfd_vti_par: the VTI modeller's .par fields (VS:342-425) in cells and seconds."""
+    _fields_ = [("nx_v", ctypes.c_int), ("nz_v", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int), ("nx_bound_l", ctypes.c_int),
+                ("nx_bound_r", ctypes.c_int), ("nz_bound_u", ctypes.c_int), ("nz_bound_d", ctypes.c_int),
+                ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int)]
+
+
+class VtiShot(ctypes.Structure):
+    """sfd_vti_shot: the reference's 1-based source column / row, receiver row and aperture."""
+    _fields_ = [("nsx", ctypes.c_int), ("nsz0", ctypes.c_int), ("nrz0", ctypes.c_int), ("xmin", ctypes.c_int),
+                ("xmax", ctypes.c_int)]
+
+
 # Every symbol include/seisfd.h declares, with (restype, argtypes).
 SIGNATURES = {
     "sfd_abi_version": (ctypes.c_int, []),
@@ -144,6 +158,9 @@ SIGNATURES = {
     "sfd_fd_coeffs": (ctypes.c_int, [ctypes.c_int, _F32P]),
     "sfd_pad_model": (ctypes.c_int, [_F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, _F32P]),
+    "sfd_vti_coefficients": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _F32P]),
+    "sfd_vti_forward": (ctypes.c_int, [ctypes.POINTER(VtiPar), _F32P, _F32P, _F32P, ctypes.c_int,
+                                       ctypes.POINTER(VtiShot), ctypes.c_int, _F32P, ctypes.POINTER(Timing)]),
 }
 
 _lib = None
@@ -190,6 +207,39 @@ def wavelet(convention: int, nt: int, dt: float, f0: float, delay: int = 150) ->
     if rc:
         raise SfdError(rc, "sfd_wavelet")
     return out
+
+
+def vti_coefficients(order: int, first: bool) -> np.ndarray:
+    """coefficient_2nd (first False) / coefficient_1st (first True) of the VTI modeller, as it
+    computes them in single precision (VS:1264-1472)."""
+    out = np.zeros((order + 1) // 2 if first else order // 2, np.float32)
+    rc = load().sfd_vti_coefficients(order, 1 if first else 0, _fp(out))
+    if rc:
+        raise SfdError(rc, "sfd_vti_coefficients")
+    return out
+
+
+def vti_forward(vz: np.ndarray, epsilon: np.ndarray, delta: np.ndarray, dx: float, dz: float, dt: float, f0: float,
+                nt: int, bounds, shots, orders=(10, 9, 10), device: int = 0):
+    """VTI pseudo-acoustic modelling of a survey (sfd_vti_forward): model arrays (nx_v, nz_v)
+    x-major; bounds = (nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d) PML cells; shots a list of
+    (nsx, nsz0, nrz0, xmin, xmax) in the reference's 1-based grid numbers, all with the same
+    xmax - xmin.  Returns (records [nshot][xmax - xmin + 1][nt], timing dict)."""
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (vz, epsilon, delta)]
+    nx_v, nz_v = arrs[0].shape
+    for a in arrs[1:]:
+        if a.shape != (nx_v, nz_v):
+            raise ValueError("vz, epsilon and delta must have the same shape")
+    par = VtiPar(nx_v, nz_v, dx, dz, dt, f0, nt, *bounds, *orders)
+    sh = (VtiShot * len(shots))(*[VtiShot(*s) for s in shots])
+    rng = shots[0][4] - shots[0][3] + 1
+    out = np.zeros((len(shots), rng, nt), np.float32)
+    t = Timing()
+    rc = load().sfd_vti_forward(ctypes.byref(par), *[_fp(a) for a in arrs], len(shots), sh, device, _fp(out),
+                                ctypes.byref(t))
+    if rc:
+        raise SfdError(rc, "sfd_vti_forward")
+    return out, {k: getattr(t, k) for k, _ in Timing._fields_}
 
 
 def afd_sponge(nx: int, nz: int, pml: int) -> np.ndarray:

@@ -197,6 +197,29 @@ def config5(nshot: int = 16, nt_scale: float = 1.0):
             "vp_slab": vp_slab, "src": src, "rec": rec, "nt": nts}
 
 
+def vti_card(nshot: int = 64, nt: int = 2000, seed: int = 20261205):
+    """The VTI modeller's shipped .par geometry (de-multiple/convolution_srm/vti_qa_2d_c3_demo1/
+    vti_qa_2d_modelling_new.par): a 300 x 300 model at dx = dz = 5 m, dt = 0.5 ms, 30 Hz, PML 250 m
+    on the left, right and bottom and none on top, offsets -1500 .. 1495 m (600 traces per shot),
+    order 10 / 9 / 10; the card's shots step one cell from sx0 = 0.  The card's model files are
+    not shipped: a seeded synthetic model stands in (8 layers, vz 1500-3500 m/s with a +-3% lateral
+    field, epsilon 0.05-0.25 and delta 0.02-0.12 increasing with depth).  nshot shots spread over
+    the 300 source positions; the card's nt is 10000."""
+    rng = np.random.default_rng(seed)
+    nxv = nzv = 300
+    z = np.arange(nzv)
+    layer = np.minimum((z * 8) // nzv, 7)
+    vz1 = 1500.0 + 2000.0 * layer / 7.0
+    lat = 1.0 + 0.03 * np.sin(2 * np.pi * np.arange(nxv) / nxv * rng.uniform(1.0, 3.0) + rng.uniform(0, 6.28))
+    vz = (vz1[None, :] * lat[:, None]).astype(np.float32)
+    eps = np.tile(0.05 + 0.20 * layer / 7.0, (nxv, 1)).astype(np.float32)
+    de = np.tile(0.02 + 0.10 * layer / 7.0, (nxv, 1)).astype(np.float32)
+    nsx = [1 + int(i * nxv / nshot) for i in range(nshot)]
+    shots = [(s, 1, 1, s - 300, s + 299) for s in nsx]  # nint(offset / dx): -300 .. 299
+    return {"name": "vti_card_300x300", "vz": vz, "eps": eps, "delta": de, "dx": 5.0, "dz": 5.0, "dt": 5e-4,
+            "f0": 30.0, "nt": nt, "bounds": (50, 50, 0, 50), "shots": shots}
+
+
 def small_varden(seed: int = 7) -> AcousticCase:
     """Non-square, variable-density case used to pin the restatement against the reference
     build: 80 (x) x 60 (z) interior, 15-cell sponge, 300 steps, off-centre source."""
