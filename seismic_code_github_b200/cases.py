@@ -150,16 +150,25 @@ def gradient3d(args):
         return e.timing()
 
 
+def vti(args):
+    """The VTI modeller on the shipped .par geometry (workloads.vti_card), nshot shots, nt samples."""
+    c = W.vti_card(nshot=args.nshot, nt=args.nt)
+    _, t = S.vti_forward(c["vz"], c["eps"], c["delta"], c["dx"], c["dz"], c["dt"], c["f0"], c["nt"], c["bounds"],
+                         c["shots"])
+    return t
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["acoustic3d", "viscoac", "gradient", "forward2d", "qgradient", "gradient3d",
-                                     "viscoel", "elastic"])
+                                     "viscoel", "elastic", "vti"])
     ap.add_argument("--n", type=int, default=384, help="3-D padded grid size per axis")
     ap.add_argument("--nshot", type=int, default=2)
     ap.add_argument("--nt", type=int, default=3)
     args = ap.parse_args()
     cases = {"acoustic3d": acoustic3d, "viscoac": viscoac, "gradient": gradient, "forward2d": forward2d,
-             "qgradient": qgradient, "gradient3d": gradient3d, "viscoel": viscoel, "elastic": elastic}
+             "qgradient": qgradient, "gradient3d": gradient3d, "viscoel": viscoel, "elastic": elastic,
+             "vti": vti}
     t = cases[args.case](args)
     print(json.dumps(t))
 

@@ -5,9 +5,12 @@
 // Per time step the reference calls extrapolation_one_step_1 (new u from the current u and q,
 // VS:432-960) and then extrapolation_one_step_2 (new q from the current u and q, VS:965-1258).
 // Neither reads what the other writes -- step 2 takes the current u, not the new one -- so one
-// kernel does both: each thread owns one cell of one shot, reads the current u and q through
-// the 10th-order cross stencils (L1-cached, the cross of 21 + 21 values), updates the split PML
-// fields of its cell in place and writes the new u and q into the slots of the old ones.  The
+// kernel does both.  A CTA stages the current u and q of a 32 x 8 tile with its 5-cell halo in
+// shared memory; each thread owns one cell of one shot, forms the stencil sums that both
+// subroutines share once, updates the split PML fields of its cell in place and writes the new
+// u and q into the slots of the old ones.  All global loads of a thread are issued before the
+// tile barrier, and the registers are bounded for five CTAs per SM (the kernel is bound by the
+// latency of those loads and of the IEEE divisions the reference order requires).  The
 // operation order is the reference's as written, every multiply, add and divide rounded
 // separately (__fmul_rn, __fadd_rn, __fdiv_rn, __fsqrt_rn), so the records equal the FP32
 // restatement in oracle/vti_oracle.cpp bit for bit.  A one-thread-per-shot kernel adds the source
@@ -25,7 +28,13 @@
 
 namespace {
 
-constexpr int kBX = 32, kBZ = 8;
+constexpr int kBX = 32, kBZ = 8;             // threads per CTA (x, z)
+constexpr int kTX = 32, kH = 5;               // cells per CTA tile in x, stencil halo
+constexpr int kSX = kTX + 2 * kH;
+// One cell per thread and registers bounded for five CTAs per SM.  Measured on the .par geometry
+// (64 shots of 348 x 698): 1, 2 and 4 cells per thread 36.9, 35.3 and 28.6 Gpts/s at four CTAs per
+// SM; one cell at five and six CTAs per SM 39.3 and 39.2 Gpts/s (the latter spills).
+constexpr int kCPT = 1, kMinBlocks = 5;
 
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
@@ -41,7 +50,7 @@ struct VtiDev {
     long long xs, zs;              // floats per x strip, per z strip
     int pitch, nx, nz, nxl, nxr, nzu, nzd, range, nt;
     float dx, dz, dt, L;
-    float cE[5], c2[5], c1[5];
+    float cE[5], c1[5];    // coefficient_2nd(10) (fd_coe and fd_coe_pml_2nd alike), coefficient_1st
     const int* src;        // per shot: source cell i, j
     const int* rrow;       // per shot: receiver row and whether it is the row-6 fallback
     float* records;        // [shot][range][nt]
@@ -67,18 +76,18 @@ __device__ __forceinline__ VtiSlab slab(const VtiDev& a, int s) {
 }
 
 // second-derivative sum of VS:511-525: (c1 (f+1 + f-1 - 2 f0) + ... + c5 (...)) / h**2
-__device__ __forceinline__ float d2(const float* f, long long c, long long st, const float* cf, float h) {
-    const float two_f0 = fm(2.0f, __ldg(f + c));
-    float s = fm(cf[0], fs(fa(__ldg(f + c + st), __ldg(f + c - st)), two_f0));
+__device__ __forceinline__ float d2(const float* f, int c, int st, const float* cf, float h) {
+    const float two_f0 = fm(2.0f, f[c]);
+    float s = fm(cf[0], fs(fa(f[c + st], f[c - st]), two_f0));
 #pragma unroll
-    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(fa(__ldg(f + c + m * st), __ldg(f + c - m * st)), two_f0)));
+    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(fa(f[c + m * st], f[c - m * st]), two_f0)));
     return fd(s, fm(h, h));
 }
 // first-derivative sum of VS:567-578: (p1 (f+1 - f-1) + ... + p5 (...)) / h
-__device__ __forceinline__ float d1(const float* f, long long c, long long st, const float* cf, float h) {
-    float s = fm(cf[0], fs(__ldg(f + c + st), __ldg(f + c - st)));
+__device__ __forceinline__ float d1(const float* f, int c, int st, const float* cf, float h) {
+    float s = fm(cf[0], fs(f[c + st], f[c - st]));
 #pragma unroll
-    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(__ldg(f + c + m * st), __ldg(f + c - m * st))));
+    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(f[c + m * st], f[c - m * st])));
     return fd(s, h);
 }
 
@@ -109,35 +118,35 @@ __global__ void vti_inject_kernel(VtiDev a, int cu, float w) {
     p.u(cu)[c] = fa(p.u(cu)[c], w);
 }
 
-__global__ void __launch_bounds__(kBX * kBZ) vti_step_kernel(VtiDev a, int cu, int iit) {
-    const int i = blockIdx.x * kBX + threadIdx.x + 1, j = blockIdx.y * kBZ + threadIdx.y + 1, s = blockIdx.z;
-    if (i > a.nx || j > a.nz) return;
+// one cell (i, j) of shot s: U and Q are the shared-memory tiles of the current u and q, sc the
+// cell's tile index, P the tile's row stride; c indexes the cell in the field layout
+// (v, de, ep: the cell's model; uo, qo: its old u and q, loaded by the caller ahead of time)
+__device__ __forceinline__ void vti_cell(const VtiDev& a, const VtiSlab& p, const float* U, const float* Q, int sc,
+                                         int P, int i, int j, int s, int cu, int iit, float v, float de, float ep,
+                                         float uo, float qo) {
     const int ou = 1 - cu;
-    const VtiSlab p = slab(a, s);
-    const long long c = (long long)(j + 4) * a.pitch + (i + 4), P = a.pitch;
-    const float* U = p.u(cu);
-    const float* Q = p.q(cu);
-    const float v = p.vz()[c], de = p.de()[c], ep = p.ep()[c];
+    const int c = sc;
+    const long long g = (long long)(j + 4) * a.pitch + (i + 4);
     const float dt = a.dt, dx = a.dx, dz = a.dz, L = a.L;
     const int nx = a.nx, nz = a.nz, nxl = a.nxl, nxr = a.nxr, nzu = a.nzu, nzd = a.nzd;
     const bool xin = i > nxl && i < nx - nxr + 1;
     float un, qn;
 
-    // ---- extrapolation_one_step_1 (VS:432-960): new u ----
+    // The sums of the current u and q that both subroutines form: coefficient_2nd(10) is both
+    // fd_coe and fd_coe_pml_2nd, the x sums of u and q appear in step 1 and step 2 (added in the
+    // other order there, which IEEE addition does not distinguish), the z sum of u in every
+    // region of step 1.  Each is formed once.
+    const float sxu = d2(U, c, 1, a.cE, dx), sxq = d2(Q, c, 1, a.cE, dx), szu = d2(U, c, P, a.cE, dz);
+
+    // ---- extrapolation_one_step_1 (VS:432-960): new u; step 2's PML cells share its terms ----
     if (xin && j > nzu && j < nz - nzd + 1) {
-        const float sxu = d2(U, c, 1, a.cE, dx), szu = d2(U, c, P, a.cE, dz), sxq = d2(Q, c, 1, a.cE, dx);
-        un = fa(fs(fm(2.0f, U[c]), p.u(ou)[c]), fm(fm(fm(dt, dt), fm(v, v)), fa(fm(fa(1.0f, fm(2.0f, de)), fa(sxu, sxq)), szu)));
+        un = fa(fs(fm(2.0f, U[c]), uo), fm(fm(fm(dt, dt), fm(v, v)), fa(fm(fa(1.0f, fm(2.0f, de)), fa(sxu, sxq)), szu)));
     } else if (!xin) {
         const bool left = i <= nxl;
         const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
         const float vx = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, ep))));
-        float s1 = d1(U, c, 1, a.c1, dx);
-        const float s1q = d1(Q, c, 1, a.c1, dx);
-        float s2 = d2(U, c, 1, a.c2, dx);
-        const float sz2 = d2(U, c, P, a.c2, dz);
-        const float s2q = d2(Q, c, 1, a.c2, dx);
-        s1 = fa(s1, s1q);
-        s2 = fa(s2, s2q);
+        const float s1 = fa(d1(U, c, 1, a.c1, dx), d1(Q, c, 1, a.c1, dx));
+        const float s2 = fa(sxu, sxq);
         const float axis = fm((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
         const float thick = fm((float)(left ? nxl : nxr), dx);
         const int is = left ? i : i - (nx - nxr) + nxl;
@@ -150,16 +159,18 @@ __global__ void __launch_bounds__(kBX * kBZ) vti_step_kernel(VtiDev a, int cu, i
                  fm(k2, fm(s2, fm(dx, dx))), fm(fm(k2, dd), fm(s1, dx)));
         float* a3 = p.ux(3, ou);
         const float* a3o = p.ux(3, cu);
-        const float n3 = fa(fs(fm(2.0f, a3o[x]), a3[x]), fd(fm(fm(fm(v, v), fm(dt, dt)), fm(sz2, fm(dz, dz))), fm(dz, dz)));
+        const float n3 = fa(fs(fm(2.0f, a3o[x]), a3[x]), fd(fm(fm(fm(v, v), fm(dt, dt)), fm(szu, fm(dz, dz))), fm(dz, dz)));
         a3[x] = n3;
         un = fa(fa(p.ux(0, ou)[x], p.ux(1, ou)[x]), n3);
+        // extrapolation_one_step_2's PML cell (VS:1073-1150): the same s1, s2, d and dd
+        const float kq = fm(fs(fm(vx, vx), fm(vn, vn)), fm(dt, dt));
+        pml_cell(d, dt, dx, p.qx(0, ou), p.qx(0, cu), p.qx(2, ou), p.qx(2, cu), p.qx(1, ou), p.qx(1, cu), x,
+                 fm(kq, fm(s2, fm(dx, dx))), fm(fm(kq, dd), fm(s1, dx)));
+        qn = fa(p.qx(0, ou)[x], p.qx(1, ou)[x]);
     } else {
         const bool top = j <= nzu;
         const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
         const float sz1 = d1(U, c, P, a.c1, dx);  // divided by dx as written (VS:796, 880)
-        const float sx2 = d2(U, c, 1, a.c2, dx);
-        const float sz2 = d2(U, c, P, a.c2, dz);
-        const float sx2q = d2(Q, c, 1, a.c2, dx);
         const float axis = fm((float)(top ? j - (nzu + 1) : j - (nz - nzd)), dz);
         const float thick = fm((float)(top ? nzu : nzd), dz);
         const int js = top ? j : j - (nz - nzd) + nzu;
@@ -169,47 +180,88 @@ __global__ void __launch_bounds__(kBX * kBZ) vti_step_kernel(VtiDev a, int cu, i
         const long long z = (long long)(js - 1) * nx + (i - 1);
         const float k2 = fm(fm(v, v), fm(dt, dt));
         pml_cell(d, dt, dz, p.uz(0, ou), p.uz(0, cu), p.uz(2, ou), p.uz(2, cu), p.uz(1, ou), p.uz(1, cu), z,
-                 fm(k2, fm(sz2, fm(dz, dz))), fm(fm(k2, dd), fm(sz1, dz)));
+                 fm(k2, fm(szu, fm(dz, dz))), fm(fm(k2, dd), fm(sz1, dz)));
         float* a3 = p.uz(3, ou);
         const float* a3o = p.uz(3, cu);
-        const float n3 = fa(fs(fm(2.0f, a3o[z]), a3[z]), fm(fm(fm(vn, vn), fm(dt, dt)), fa(sx2, sx2q)));
+        const float n3 = fa(fs(fm(2.0f, a3o[z]), a3[z]), fm(fm(fm(vn, vn), fm(dt, dt)), fa(sxu, sxq)));
         a3[z] = n3;
         un = fa(fa(p.uz(0, ou)[z], p.uz(1, ou)[z]), n3);
     }
 
-    // ---- extrapolation_one_step_2 (VS:965-1258): new q from the current u ----
-    if (xin) {
-        const float sxu = d2(U, c, 1, a.cE, dx), sxq = d2(Q, c, 1, a.cE, dx);
-        qn = fa(fs(fm(2.0f, Q[c]), p.q(ou)[c]), fm(fm(fm(dt, dt), fm(v, v)), fm(fm(2.0f, fs(ep, de)), fa(sxq, sxu))));
-    } else {
-        const bool left = i <= nxl;
-        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
-        const float vx = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, ep))));
-        float s1 = d1(Q, c, 1, a.c1, dx);
-        const float s1u = d1(U, c, 1, a.c1, dx);
-        float s2 = d2(Q, c, 1, a.c2, dx);
-        const float s2u = d2(U, c, 1, a.c2, dx);
-        s1 = fa(s1, s1u);
-        s2 = fa(s2, s2u);
-        const float axis = fm((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
-        const float thick = fm((float)(left ? nxl : nxr), dx);
-        const int is = left ? i : i - (nx - nxr) + nxl;
-        const float A = fd(fm(3.0f, vx), fm(2.0f, thick));
-        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
-        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
-        const long long x = (long long)(j - 1) * (nxl + nxr) + (is - 1);
-        const float k2 = fm(fs(fm(vx, vx), fm(vn, vn)), fm(dt, dt));
-        pml_cell(d, dt, dx, p.qx(0, ou), p.qx(0, cu), p.qx(2, ou), p.qx(2, cu), p.qx(1, ou), p.qx(1, cu), x,
-                 fm(k2, fm(s2, fm(dx, dx))), fm(fm(k2, dd), fm(s1, dx)));
-        qn = fa(p.qx(0, ou)[x], p.qx(1, ou)[x]);
-    }
-    p.u(ou)[c] = un;
-    p.q(ou)[c] = qn;
+    // ---- extrapolation_one_step_2 (VS:965-1072): new q inside, from the current u ----
+    if (xin)
+        qn = fa(fs(fm(2.0f, Q[c]), qo), fm(fm(fm(dt, dt), fm(v, v)), fm(fm(2.0f, fs(ep, de)), fa(sxq, sxu))));
+    p.u(ou)[g] = un;
+    p.q(ou)[g] = qn;
 
     // ---- recording (VM:446-453, 494-501): new u on the receiver row ----
     const int rr = a.rrow[2 * s], low = a.rrow[2 * s + 1];
     if (j == rr && i > nxl && i <= nxl + a.range && iit <= a.nt && ((!low && iit >= 1) || (low && iit > 1)))
         a.records[((long long)s * a.range + (i - nxl - 1)) * a.nt + (iit - 1)] = un;
+}
+
+// Tiles of 32 x (8 CPT) cells per CTA (32 x 8 threads, CPT cells per thread): the current u and
+// q of the tile and its 5-cell halo are staged in shared memory once, every stencil reads them
+// there.
+template <int CPT, int MINB>
+__global__ void __launch_bounds__(kBX * kBZ, MINB) vti_step_kernel(VtiDev a, int cu, int iit) {
+    constexpr int kTZ = kBZ * CPT, kSZ = kTZ + 2 * kH;
+    __shared__ float sU[kSX * kSZ], sQ[kSX * kSZ];
+    const int s = blockIdx.z, tx = threadIdx.x, ty = threadIdx.y, tid = ty * kBX + tx;
+    const int i0 = blockIdx.x * kTX + 1, j0 = blockIdx.y * kTZ + 1;
+    const VtiSlab p = slab(a, s);
+    const float* U = p.u(cu);
+    const float* Q = p.q(cu);
+    // tile cell (lx, lz) is field cell (i0 - 5 + lx, j0 - 5 + lz), array column i + 4 >= 0 and row
+    // j + 4 >= 0; columns past the pitch and rows past nz + 5 (only reached by the tile's own cells
+    // beyond the grid, which store nothing) read as zero.  All of the thread's global loads -- its
+    // share of the tiles and its cells' model and old u, q -- are issued before the first use.
+    constexpr int NE = kSX * kSZ, IT = (NE + kBX * kBZ - 1) / (kBX * kBZ);
+    float ru[IT], rq[IT];
+#pragma unroll
+    for (int t = 0; t < IT; t++) {
+        const int e = tid + t * kBX * kBZ;
+        const int lz = e / kSX, lx = e - lz * kSX;
+        const int gi = i0 - kH + lx + 4, gj = j0 - kH + lz + 4;
+        ru[t] = 0.0f;
+        rq[t] = 0.0f;
+        if (e < NE && gi < a.pitch && gj < a.nz + 10) {
+            const long long gg = (long long)gj * a.pitch + gi;
+            ru[t] = U[gg];
+            rq[t] = Q[gg];
+        }
+    }
+    const int i = i0 + tx, ou = 1 - cu;
+    float mv[CPT], md[CPT], me[CPT], mu[CPT], mq[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+        const int j = j0 + ty + kBZ * k;
+        mv[k] = md[k] = me[k] = mu[k] = mq[k] = 0.0f;
+        if (i <= a.nx && j <= a.nz) {
+            const long long g = (long long)(j + 4) * a.pitch + (i + 4);
+            mv[k] = p.vz()[g];
+            md[k] = p.de()[g];
+            me[k] = p.ep()[g];
+            mu[k] = p.u(ou)[g];
+            mq[k] = p.q(ou)[g];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < IT; t++) {
+        const int e = tid + t * kBX * kBZ;
+        if (e < NE) {
+            sU[e] = ru[t];
+            sQ[e] = rq[t];
+        }
+    }
+    __syncthreads();
+    if (i > a.nx) return;
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+        const int lz = ty + kBZ * k, j = j0 + lz;
+        if (j > a.nz) break;
+        vti_cell(a, p, sU, sQ, (lz + kH) * kSX + tx + kH, kSX, i, j, s, cu, iit, mv[k], md[k], me[k], mu[k], mq[k]);
+    }
 }
 
 // coefficient_2nd / coefficient_1st (VS:1264-1472): a(i,j) = i^p / p! (p = 2j or 2j-1) inverted
@@ -290,7 +342,7 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
     a.nx = nx; a.nz = nz; a.nxl = nxl; a.nxr = nxr; a.nzu = nzu; a.nzd = nzd; a.range = range; a.nt = c.nt;
     a.dx = c.dx; a.dz = c.dz; a.dt = c.dt;
     a.L = std::log(1.0f / 1.0e-3f);  // log(1/R), R = 1.0E-3 (VS:14)
-    if (coefficients(10, 0, a.cE) || coefficients(c.order_pml_2nd, 0, a.c2) || coefficients(c.order_pml_1st, 1, a.c1))
+    if (coefficients(10, 0, a.cE) || coefficients(c.order_pml_1st, 1, a.c1))
         return SFD_ERR_ARG;
     a.pitch = (nx + 10 + 31) / 32 * 32;
     a.field = (long long)a.pitch * (nz + 10);
@@ -385,7 +437,8 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const dim3 grid((nx + kBX - 1) / kBX, (nz + kBZ - 1) / kBZ, nshot), block(kBX, kBZ);
+    const int tz = kBZ * kCPT;
+    const dim3 grid((nx + kTX - 1) / kTX, (nz + tz - 1) / tz, nshot), block(kBX, kBZ);
     long long launches = 0;
     cudaEventRecord(e0, st);
     for (int it = 1; it <= NT; it++) {
@@ -394,7 +447,7 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
             vti_inject_kernel<<<nshot, 32, 0, st>>>(a, cu, w[it]);
             launches++;
         }
-        vti_step_kernel<<<grid, block, 0, st>>>(a, cu, it - half);
+        vti_step_kernel<kCPT, kMinBlocks><<<grid, block, 0, st>>>(a, cu, it - half);
         launches++;
     }
     cudaEventRecord(e1, st);
