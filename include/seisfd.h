@@ -338,6 +338,9 @@ typedef struct {
     int nt;                /* record length                                                   */
     int nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d;  /* PML cells, nint(thickness / dx) (VM:136-141) */
     int order_explicit, order_pml_1st, order_pml_2nd;
+    int flags;             /* SFD_EXACT: every operation rounded separately in the reference's order
+                              (bit-exact with the restatement); 0: FMA contraction and approximate
+                              divisions (relative L2 <= 1e-5 of it)                            */
 } sfd_vti_par;
 
 typedef struct {

@@ -36,10 +36,14 @@ constexpr int kSX = kTX + 2 * kH;
 // SM; one cell at five and six CTAs per SM 39.3 and 39.2 Gpts/s (the latter spills).
 constexpr int kCPT = 1, kMinBlocks = 5;
 
-__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+// E = true: every operation rounded separately in the reference's order (bit-exact with the
+// restatement); E = false: multiplies and adds may contract into FMAs and divisions are the
+// approximate __fdividef (records within relative L2 1e-5 of the restatement)
+template <bool E> __device__ __forceinline__ float fm(float a, float b) { return E ? __fmul_rn(a, b) : a * b; }
+template <bool E> __device__ __forceinline__ float fa(float a, float b) { return E ? __fadd_rn(a, b) : a + b; }
+template <bool E> __device__ __forceinline__ float fs(float a, float b) { return E ? __fsub_rn(a, b) : a - b; }
+template <bool E> __device__ __forceinline__ float fd(float a, float b) { return E ? __fdiv_rn(a, b) : __fdividef(a, b); }
+template <bool E> __device__ __forceinline__ float fsq(float a) { return E ? __fsqrt_rn(a) : sqrtf(a); }
 
 struct VtiDev {
     // per shot: fields u[2], q[2] (pitch x (nz + 10), cell (i, j) 1-based at (j+4)*pitch + i+4),
@@ -76,38 +80,41 @@ __device__ __forceinline__ VtiSlab slab(const VtiDev& a, int s) {
 }
 
 // second-derivative sum of VS:511-525: (c1 (f+1 + f-1 - 2 f0) + ... + c5 (...)) / h**2
+template <bool E>
 __device__ __forceinline__ float d2(const float* f, int c, int st, const float* cf, float h) {
-    const float two_f0 = fm(2.0f, f[c]);
-    float s = fm(cf[0], fs(fa(f[c + st], f[c - st]), two_f0));
+    const float two_f0 = fm<E>(2.0f, f[c]);
+    float s = fm<E>(cf[0], fs<E>(fa<E>(f[c + st], f[c - st]), two_f0));
 #pragma unroll
-    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(fa(f[c + m * st], f[c - m * st]), two_f0)));
-    return fd(s, fm(h, h));
+    for (int m = 2; m <= 5; m++) s = fa<E>(s, fm<E>(cf[m - 1], fs<E>(fa<E>(f[c + m * st], f[c - m * st]), two_f0)));
+    return fd<E>(s, fm<E>(h, h));
 }
 // first-derivative sum of VS:567-578: (p1 (f+1 - f-1) + ... + p5 (...)) / h
+template <bool E>
 __device__ __forceinline__ float d1(const float* f, int c, int st, const float* cf, float h) {
-    float s = fm(cf[0], fs(f[c + st], f[c - st]));
+    float s = fm<E>(cf[0], fs<E>(f[c + st], f[c - st]));
 #pragma unroll
-    for (int m = 2; m <= 5; m++) s = fa(s, fm(cf[m - 1], fs(f[c + m * st], f[c - m * st])));
-    return fd(s, h);
+    for (int m = 2; m <= 5; m++) s = fa<E>(s, fm<E>(cf[m - 1], fs<E>(f[c + m * st], f[c - m * st])));
+    return fd<E>(s, h);
 }
 
 // the split PML recurrences of one boundary cell (VS:651-663, 840-858): a1 (second-derivative
 // part), t2 (first-derivative part with the damping derivative), a2; k2s2 = speed^2 dt^2 (s2 h^2)
 // and k2dd = speed^2 dt^2 dd (s1 h), both formed by the caller in the reference's order
+template <bool E>
 __device__ __forceinline__ void pml_cell(float d, float dt, float h, float* a1, const float* a1o, float* t2,
                                          const float* t2o, float* a2, const float* a2o, long long x, float k2s2,
                                          float k2dd) {
-    const float h2 = fm(h, h);
-    const float d2dt = fm(fm(2.0f, d), dt);
-    const float P = fs(fa(fm(2.0f, h2), fm(d2dt, h2)), fm(fm(fm(d, d), h2), fm(dt, dt)));
-    const float Den = fa(h2, fm(d2dt, h2));
-    const float n1 = fd(fa(fs(fm(a1o[x], P), fm(h2, a1[x])), k2s2), Den);
-    const float P2 = fs(fa(fm(2.0f, h), fm(d2dt, h)), fm(fm(fm(dt, dt), h), fm(d, d)));
-    const float Den2 = fa(h, fm(d2dt, h));
-    const float nt = fd(fs(fs(fm(t2o[x], P2), fm(h, t2[x])), k2dd), Den2);
+    const float h2 = fm<E>(h, h);
+    const float d2dt = fm<E>(fm<E>(2.0f, d), dt);
+    const float P = fs<E>(fa<E>(fm<E>(2.0f, h2), fm<E>(d2dt, h2)), fm<E>(fm<E>(fm<E>(d, d), h2), fm<E>(dt, dt)));
+    const float Den = fa<E>(h2, fm<E>(d2dt, h2));
+    const float n1 = fd<E>(fa<E>(fs<E>(fm<E>(a1o[x], P), fm<E>(h2, a1[x])), k2s2), Den);
+    const float P2 = fs<E>(fa<E>(fm<E>(2.0f, h), fm<E>(d2dt, h)), fm<E>(fm<E>(fm<E>(dt, dt), h), fm<E>(d, d)));
+    const float Den2 = fa<E>(h, fm<E>(d2dt, h));
+    const float nt = fd<E>(fs<E>(fs<E>(fm<E>(t2o[x], P2), fm<E>(h, t2[x])), k2dd), Den2);
     a1[x] = n1;
     t2[x] = nt;
-    a2[x] = fa(fm(a2o[x], fs(1.0f, fm(d, dt))), fm(nt, dt));
+    a2[x] = fa<E>(fm<E>(a2o[x], fs<E>(1.0f, fm<E>(d, dt))), fm<E>(nt, dt));
 }
 
 __global__ void vti_inject_kernel(VtiDev a, int cu, float w) {
@@ -115,12 +122,13 @@ __global__ void vti_inject_kernel(VtiDev a, int cu, float w) {
     if (threadIdx.x != 0) return;
     const VtiSlab p = slab(a, s);
     const long long c = (long long)(a.src[2 * s + 1] + 4) * a.pitch + (a.src[2 * s] + 4);
-    p.u(cu)[c] = fa(p.u(cu)[c], w);
+    p.u(cu)[c] = __fadd_rn(p.u(cu)[c], w);
 }
 
 // one cell (i, j) of shot s: U and Q are the shared-memory tiles of the current u and q, sc the
 // cell's tile index, P the tile's row stride; c indexes the cell in the field layout
 // (v, de, ep: the cell's model; uo, qo: its old u and q, loaded by the caller ahead of time)
+template <bool E>
 __device__ __forceinline__ void vti_cell(const VtiDev& a, const VtiSlab& p, const float* U, const float* Q, int sc,
                                          int P, int i, int j, int s, int cu, int iit, float v, float de, float ep,
                                          float uo, float qo) {
@@ -136,61 +144,61 @@ __device__ __forceinline__ void vti_cell(const VtiDev& a, const VtiSlab& p, cons
     // fd_coe and fd_coe_pml_2nd, the x sums of u and q appear in step 1 and step 2 (added in the
     // other order there, which IEEE addition does not distinguish), the z sum of u in every
     // region of step 1.  Each is formed once.
-    const float sxu = d2(U, c, 1, a.cE, dx), sxq = d2(Q, c, 1, a.cE, dx), szu = d2(U, c, P, a.cE, dz);
+    const float sxu = d2<E>(U, c, 1, a.cE, dx), sxq = d2<E>(Q, c, 1, a.cE, dx), szu = d2<E>(U, c, P, a.cE, dz);
 
     // ---- extrapolation_one_step_1 (VS:432-960): new u; step 2's PML cells share its terms ----
     if (xin && j > nzu && j < nz - nzd + 1) {
-        un = fa(fs(fm(2.0f, U[c]), uo), fm(fm(fm(dt, dt), fm(v, v)), fa(fm(fa(1.0f, fm(2.0f, de)), fa(sxu, sxq)), szu)));
+        un = fa<E>(fs<E>(fm<E>(2.0f, U[c]), uo), fm<E>(fm<E>(fm<E>(dt, dt), fm<E>(v, v)), fa<E>(fm<E>(fa<E>(1.0f, fm<E>(2.0f, de)), fa<E>(sxu, sxq)), szu)));
     } else if (!xin) {
         const bool left = i <= nxl;
-        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
-        const float vx = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, ep))));
-        const float s1 = fa(d1(U, c, 1, a.c1, dx), d1(Q, c, 1, a.c1, dx));
-        const float s2 = fa(sxu, sxq);
-        const float axis = fm((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
-        const float thick = fm((float)(left ? nxl : nxr), dx);
+        const float vn = fm<E>(v, fsq<E>(fa<E>(1.0f, fm<E>(2.0f, de))));
+        const float vx = fm<E>(v, fsq<E>(fa<E>(1.0f, fm<E>(2.0f, ep))));
+        const float s1 = fa<E>(d1<E>(U, c, 1, a.c1, dx), d1<E>(Q, c, 1, a.c1, dx));
+        const float s2 = fa<E>(sxu, sxq);
+        const float axis = fm<E>((float)(left ? i - (nxl + 1) : i - (nx - nxr)), dx);
+        const float thick = fm<E>((float)(left ? nxl : nxr), dx);
         const int is = left ? i : i - (nx - nxr) + nxl;
-        const float A = fd(fm(3.0f, vx), fm(2.0f, thick));
-        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
-        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
+        const float A = fd<E>(fm<E>(3.0f, vx), fm<E>(2.0f, thick));
+        const float d = fm<E>(fm<E>(A, fm<E>(fd<E>(axis, thick), fd<E>(axis, thick))), L);
+        const float dd = fm<E>(fm<E>(A, fd<E>(fm<E>(2.0f, axis), fm<E>(thick, thick))), L);
         const long long x = (long long)(j - 1) * (nxl + nxr) + (is - 1);
-        const float k2 = fm(fm(vn, vn), fm(dt, dt));
-        pml_cell(d, dt, dx, p.ux(0, ou), p.ux(0, cu), p.ux(2, ou), p.ux(2, cu), p.ux(1, ou), p.ux(1, cu), x,
-                 fm(k2, fm(s2, fm(dx, dx))), fm(fm(k2, dd), fm(s1, dx)));
+        const float k2 = fm<E>(fm<E>(vn, vn), fm<E>(dt, dt));
+        pml_cell<E>(d, dt, dx, p.ux(0, ou), p.ux(0, cu), p.ux(2, ou), p.ux(2, cu), p.ux(1, ou), p.ux(1, cu), x,
+                 fm<E>(k2, fm<E>(s2, fm<E>(dx, dx))), fm<E>(fm<E>(k2, dd), fm<E>(s1, dx)));
         float* a3 = p.ux(3, ou);
         const float* a3o = p.ux(3, cu);
-        const float n3 = fa(fs(fm(2.0f, a3o[x]), a3[x]), fd(fm(fm(fm(v, v), fm(dt, dt)), fm(szu, fm(dz, dz))), fm(dz, dz)));
+        const float n3 = fa<E>(fs<E>(fm<E>(2.0f, a3o[x]), a3[x]), fd<E>(fm<E>(fm<E>(fm<E>(v, v), fm<E>(dt, dt)), fm<E>(szu, fm<E>(dz, dz))), fm<E>(dz, dz)));
         a3[x] = n3;
-        un = fa(fa(p.ux(0, ou)[x], p.ux(1, ou)[x]), n3);
+        un = fa<E>(fa<E>(p.ux(0, ou)[x], p.ux(1, ou)[x]), n3);
         // extrapolation_one_step_2's PML cell (VS:1073-1150): the same s1, s2, d and dd
-        const float kq = fm(fs(fm(vx, vx), fm(vn, vn)), fm(dt, dt));
-        pml_cell(d, dt, dx, p.qx(0, ou), p.qx(0, cu), p.qx(2, ou), p.qx(2, cu), p.qx(1, ou), p.qx(1, cu), x,
-                 fm(kq, fm(s2, fm(dx, dx))), fm(fm(kq, dd), fm(s1, dx)));
-        qn = fa(p.qx(0, ou)[x], p.qx(1, ou)[x]);
+        const float kq = fm<E>(fs<E>(fm<E>(vx, vx), fm<E>(vn, vn)), fm<E>(dt, dt));
+        pml_cell<E>(d, dt, dx, p.qx(0, ou), p.qx(0, cu), p.qx(2, ou), p.qx(2, cu), p.qx(1, ou), p.qx(1, cu), x,
+                 fm<E>(kq, fm<E>(s2, fm<E>(dx, dx))), fm<E>(fm<E>(kq, dd), fm<E>(s1, dx)));
+        qn = fa<E>(p.qx(0, ou)[x], p.qx(1, ou)[x]);
     } else {
         const bool top = j <= nzu;
-        const float vn = fm(v, __fsqrt_rn(fa(1.0f, fm(2.0f, de))));
-        const float sz1 = d1(U, c, P, a.c1, dx);  // divided by dx as written (VS:796, 880)
-        const float axis = fm((float)(top ? j - (nzu + 1) : j - (nz - nzd)), dz);
-        const float thick = fm((float)(top ? nzu : nzd), dz);
+        const float vn = fm<E>(v, fsq<E>(fa<E>(1.0f, fm<E>(2.0f, de))));
+        const float sz1 = d1<E>(U, c, P, a.c1, dx);  // divided by dx as written (VS:796, 880)
+        const float axis = fm<E>((float)(top ? j - (nzu + 1) : j - (nz - nzd)), dz);
+        const float thick = fm<E>((float)(top ? nzu : nzd), dz);
         const int js = top ? j : j - (nz - nzd) + nzu;
-        const float A = fd(fm(3.0f, v), fm(2.0f, thick));
-        const float d = fm(fm(A, fm(fd(axis, thick), fd(axis, thick))), L);
-        const float dd = fm(fm(A, fd(fm(2.0f, axis), fm(thick, thick))), L);
+        const float A = fd<E>(fm<E>(3.0f, v), fm<E>(2.0f, thick));
+        const float d = fm<E>(fm<E>(A, fm<E>(fd<E>(axis, thick), fd<E>(axis, thick))), L);
+        const float dd = fm<E>(fm<E>(A, fd<E>(fm<E>(2.0f, axis), fm<E>(thick, thick))), L);
         const long long z = (long long)(js - 1) * nx + (i - 1);
-        const float k2 = fm(fm(v, v), fm(dt, dt));
-        pml_cell(d, dt, dz, p.uz(0, ou), p.uz(0, cu), p.uz(2, ou), p.uz(2, cu), p.uz(1, ou), p.uz(1, cu), z,
-                 fm(k2, fm(szu, fm(dz, dz))), fm(fm(k2, dd), fm(sz1, dz)));
+        const float k2 = fm<E>(fm<E>(v, v), fm<E>(dt, dt));
+        pml_cell<E>(d, dt, dz, p.uz(0, ou), p.uz(0, cu), p.uz(2, ou), p.uz(2, cu), p.uz(1, ou), p.uz(1, cu), z,
+                 fm<E>(k2, fm<E>(szu, fm<E>(dz, dz))), fm<E>(fm<E>(k2, dd), fm<E>(sz1, dz)));
         float* a3 = p.uz(3, ou);
         const float* a3o = p.uz(3, cu);
-        const float n3 = fa(fs(fm(2.0f, a3o[z]), a3[z]), fm(fm(fm(vn, vn), fm(dt, dt)), fa(sxu, sxq)));
+        const float n3 = fa<E>(fs<E>(fm<E>(2.0f, a3o[z]), a3[z]), fm<E>(fm<E>(fm<E>(vn, vn), fm<E>(dt, dt)), fa<E>(sxu, sxq)));
         a3[z] = n3;
-        un = fa(fa(p.uz(0, ou)[z], p.uz(1, ou)[z]), n3);
+        un = fa<E>(fa<E>(p.uz(0, ou)[z], p.uz(1, ou)[z]), n3);
     }
 
     // ---- extrapolation_one_step_2 (VS:965-1072): new q inside, from the current u ----
     if (xin)
-        qn = fa(fs(fm(2.0f, Q[c]), qo), fm(fm(fm(dt, dt), fm(v, v)), fm(fm(2.0f, fs(ep, de)), fa(sxq, sxu))));
+        qn = fa<E>(fs<E>(fm<E>(2.0f, Q[c]), qo), fm<E>(fm<E>(fm<E>(dt, dt), fm<E>(v, v)), fm<E>(fm<E>(2.0f, fs<E>(ep, de)), fa<E>(sxq, sxu))));
     p.u(ou)[g] = un;
     p.q(ou)[g] = qn;
 
@@ -203,7 +211,7 @@ __device__ __forceinline__ void vti_cell(const VtiDev& a, const VtiSlab& p, cons
 // Tiles of 32 x (8 CPT) cells per CTA (32 x 8 threads, CPT cells per thread): the current u and
 // q of the tile and its 5-cell halo are staged in shared memory once, every stencil reads them
 // there.
-template <int CPT, int MINB>
+template <int CPT, int MINB, bool E>
 __global__ void __launch_bounds__(kBX * kBZ, MINB) vti_step_kernel(VtiDev a, int cu, int iit) {
     constexpr int kTZ = kBZ * CPT, kSZ = kTZ + 2 * kH;
     __shared__ float sU[kSX * kSZ], sQ[kSX * kSZ];
@@ -260,7 +268,7 @@ __global__ void __launch_bounds__(kBX * kBZ, MINB) vti_step_kernel(VtiDev a, int
     for (int k = 0; k < CPT; k++) {
         const int lz = ty + kBZ * k, j = j0 + lz;
         if (j > a.nz) break;
-        vti_cell(a, p, sU, sQ, (lz + kH) * kSX + tx + kH, kSX, i, j, s, cu, iit, mv[k], md[k], me[k], mu[k], mq[k]);
+        vti_cell<E>(a, p, sU, sQ, (lz + kH) * kSX + tx + kH, kSX, i, j, s, cu, iit, mv[k], md[k], me[k], mu[k], mq[k]);
     }
 }
 
@@ -437,6 +445,7 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    const bool exact = (c.flags & SFD_EXACT) != 0;
     const int tz = kBZ * kCPT;
     const dim3 grid((nx + kTX - 1) / kTX, (nz + tz - 1) / tz, nshot), block(kBX, kBZ);
     long long launches = 0;
@@ -447,7 +456,8 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
             vti_inject_kernel<<<nshot, 32, 0, st>>>(a, cu, w[it]);
             launches++;
         }
-        vti_step_kernel<kCPT, kMinBlocks><<<grid, block, 0, st>>>(a, cu, it - half);
+        if (exact) vti_step_kernel<kCPT, kMinBlocks, true><<<grid, block, 0, st>>>(a, cu, it - half);
+        else vti_step_kernel<kCPT, kMinBlocks, false><<<grid, block, 0, st>>>(a, cu, it - half);
         launches++;
     }
     cudaEventRecord(e1, st);
@@ -471,7 +481,7 @@ int sfd_vti_forward(const sfd_vti_par* par, const float* vz, const float* epsilo
         timing->h2d_bytes = h2d;
         timing->d2h_bytes = (long long)(rec_n * sizeof(float));
         timing->graph = 0;
-        timing->kernel_variant = 70;
+        timing->kernel_variant = exact ? 71 : 70;
     }
     return SFD_OK;
 }

@@ -104,7 +104,8 @@ class VtiPar(ctypes.Structure):
     _fields_ = [("nx_v", ctypes.c_int), ("nz_v", ctypes.c_int), ("dx", ctypes.c_float), ("dz", ctypes.c_float),
                 ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("nt", ctypes.c_int), ("nx_bound_l", ctypes.c_int),
                 ("nx_bound_r", ctypes.c_int), ("nz_bound_u", ctypes.c_int), ("nz_bound_d", ctypes.c_int),
-                ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int)]
+                ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int),
+                ("flags", ctypes.c_int)]
 
 
 class VtiShot(ctypes.Structure):
@@ -220,17 +221,19 @@ def vti_coefficients(order: int, first: bool) -> np.ndarray:
 
 
 def vti_forward(vz: np.ndarray, epsilon: np.ndarray, delta: np.ndarray, dx: float, dz: float, dt: float, f0: float,
-                nt: int, bounds, shots, orders=(10, 9, 10), device: int = 0):
+                nt: int, bounds, shots, orders=(10, 9, 10), device: int = 0, exact: bool = False):
     """VTI pseudo-acoustic modelling of a survey (sfd_vti_forward): model arrays (nx_v, nz_v)
     x-major; bounds = (nx_bound_l, nx_bound_r, nz_bound_u, nz_bound_d) PML cells; shots a list of
     (nsx, nsz0, nrz0, xmin, xmax) in the reference's 1-based grid numbers, all with the same
-    xmax - xmin.  Returns (records [nshot][xmax - xmin + 1][nt], timing dict)."""
+    xmax - xmin.  exact: the reference's operation order, bit-exact with the restatement
+    (SFD_EXACT); otherwise FMA contraction and approximate divisions (relative L2 <= 1e-5).
+    Returns (records [nshot][xmax - xmin + 1][nt], timing dict)."""
     arrs = [np.ascontiguousarray(a, np.float32) for a in (vz, epsilon, delta)]
     nx_v, nz_v = arrs[0].shape
     for a in arrs[1:]:
         if a.shape != (nx_v, nz_v):
             raise ValueError("vz, epsilon and delta must have the same shape")
-    par = VtiPar(nx_v, nz_v, dx, dz, dt, f0, nt, *bounds, *orders)
+    par = VtiPar(nx_v, nz_v, dx, dz, dt, f0, nt, *bounds, *orders, EXACT if exact else 0)
     sh = (VtiShot * len(shots))(*[VtiShot(*s) for s in shots])
     rng = shots[0][4] - shots[0][3] + 1
     out = np.zeros((len(shots), rng, nt), np.float32)

@@ -1,5 +1,7 @@
 """GPU parity of the VTI pseudo-acoustic modeller (sfd_vti_forward, csrc/vti2d.cu) with the FP32
-restatement (oracle/vti_oracle.cpp): the records must be equal bit for bit.  The cases cover
+restatement (oracle/vti_oracle.cpp): with SFD_EXACT the records must be equal bit for bit, in
+the default mode (FMA contraction, approximate divisions) within relative L2 1e-5 of the FP32
+and the FP64 restatement.  The cases cover
 the reference's own layout (no top PML, receivers on row 6 because nrz0 + nz_bound_u < 6,
 VM:446-453), a top PML with the receivers below it, apertures clamped at both model edges
 (VS:298-300), and a batch of shots against the per-shot restatement."""
@@ -7,6 +9,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as ol
+from conftest import rel_l2
 from seismic_code_github_b200 import seisfd as S
 
 pytestmark = pytest.mark.gpu
@@ -36,14 +39,14 @@ def test_single_shot_bitexact(name):
     bounds, shot = CASES[name]
     vz, eps, de = model()
     nt = 600
-    rec, t = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, [shot])
+    rec, t = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, [shot], exact=True)
     ref = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *shot)
     diff = np.abs(rec[0] - ref).max()
     print(f"{name}: max |GPU - restatement| {diff:.3e}, peak {np.abs(ref).max():.3e}, {t['launches']} launches, "
           f"{t['loop_ms']:.2f} ms")
     assert np.abs(ref).max() > 0
     assert np.array_equal(rec[0].view(np.uint32), ref.view(np.uint32))
-    assert t["kernel_variant"] == 70
+    assert t["kernel_variant"] == 71
 
 
 def test_batched_shots_equal_per_shot_restatement():
@@ -51,13 +54,27 @@ def test_batched_shots_equal_per_shot_restatement():
     bounds = (20, 20, 0, 20)
     nt = 500
     shots = [(nsx, 1, 1, nsx - 60, nsx + 59) for nsx in (40, 90, 150)]
-    rec, t = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, shots)
+    rec, t = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, shots, exact=True)
     for k, sh in enumerate(shots):
         ref = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *sh)
         assert np.array_equal(rec[k].view(np.uint32), ref.view(np.uint32)), k
     # one launch per step for all shots, plus the source injections
     nwt = int(round(2 * 0.07 / 5e-4)) + 1
     assert t["launches"] == nt + (nwt - 1) // 2 + nwt
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fast_mode_within_tolerance(name):
+    bounds, shot = CASES[name]
+    vz, eps, de = model()
+    nt = 600
+    rec, t = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, [shot])
+    ref = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *shot)
+    r64 = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *shot, fp64=True)
+    e32, e64 = rel_l2(rec[0], ref), rel_l2(rec[0], r64)
+    print(f"{name}: fast mode relL2 vs FP32 restatement {e32:.2e}, vs FP64 {e64:.2e}")
+    assert t["kernel_variant"] == 70
+    assert e32 <= 1e-5 and e64 <= 1e-5
 
 
 def test_invalid_arguments():
