@@ -302,6 +302,23 @@ typedef struct {
     int rgau;
 } sfd_isopar;
 int sfd_isopar_read(const char* path, sfd_isopar* out);
+/* VTI modeller parameter card (VS:342-425, de-multiple/convolution_srm/vti_qa_2d_c3_demo1):
+ * pairs of a label line and a value line, in this order. */
+typedef struct {
+    char vz[256], epsilon[256], delta[256];                /* model files (nz_v x nx_v Fortran arrays) */
+    char shot1[256], shot2[256];                           /* per-shot SU prefix / merged SU prefix */
+    int nshot;
+    float offset_min, offset_max;                          /* m                                   */
+    float sx0, sz0, rz0;                                   /* m                                   */
+    float dsx;                                             /* m                                   */
+    int nx_v, nz_v;
+    float dx_v, dz_v;
+    int nt;
+    float dt, f0;
+    float bound_x_l, bound_x_r, bound_z_u, bound_z_d;      /* PML thickness (m)                  */
+    int order_explicit, order_pml_1st, order_pml_2nd;
+} sfd_vtipar;
+int sfd_vtipar_read(const char* path, sfd_vtipar* out);
 /* Raw little-endian float32 files: models (x-major, z fastest: QS:238-284, tools/get_vel_model.cpp:
  * 50-58), AFD's record / snapshot outputs (AFD:343-393).  append = 1 opens for appending. */
 int sfd_read_floats(const char* path, long long n, float* out);
@@ -315,6 +332,8 @@ int sfd_su_write(const char* path, const float* traces, int ntr, int nt, int sho
 /* The same with header options: SFD_SU_CDP sets cdp as QS:1535 does; yang_version's writer
  * (YPUB:1533-1604) leaves it 0. */
 #define SFD_SU_CDP 0x1
+/* SFD_SU_NO_OFFSET leaves offset 0, as the VTI modeller's writer does (VS:163-217) */
+#define SFD_SU_NO_OFFSET 0x2
 int sfd_su_write_ex(const char* path, const float* traces, int ntr, int nt, int shot_no, int isx, int ixmin, float dx,
                     float dt, int flags);
 /* Concatenate per-shot SU files in order (QS:1550-1624); delete_inputs = 1 removes them as the

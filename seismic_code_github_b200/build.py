@@ -30,7 +30,8 @@ LIB_SOURCES = ["api.cu", "acoustic2d.cu", "acoustic2d_fma.cu", "adjoint2d.cu", "
                "helpers.cpp", "noalloc.cu", "acoustic3d.cu", "snapshots.cu",
                "fileio.cpp"]
 OPTIONAL_SOURCES = []
-PROGRAMS = {"afd_fd": "cli_afd.cpp", "q_forward": "cli_qforward.cpp", "iso_forward": "cli_isoforward.cpp"}
+PROGRAMS = {"afd_fd": "cli_afd.cpp", "q_forward": "cli_qforward.cpp", "iso_forward": "cli_isoforward.cpp",
+            "vti_forward": "cli_vtiforward.cpp"}
 
 
 def _sources():

@@ -130,6 +130,67 @@ int sfd_qpar_read(const char* path, sfd_qpar* p) {
     return SFD_OK;
 }
 
+int sfd_vtipar_read(const char* path, sfd_vtipar* p) {
+    if (!path || !p) return SFD_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SFD_ERR_IO;
+    std::memset(p, 0, sizeof(*p));
+    std::string label, line;
+    // VS:383-392: five file names, then the numeric cards (VS:393-421), each after one label line
+    int rc = SFD_OK;
+    char* names[5] = {p->vz, p->epsilon, p->delta, p->shot1, p->shot2};
+    for (int i = 0; i < 5 && rc == SFD_OK; i++) {
+        if (!read_line(f, &label) || !read_line(f, &line)) rc = SFD_ERR_IO;
+        else std::snprintf(names[i], sizeof(p->vz), "%s", strip(line).c_str());
+    }
+    struct Card {
+        int n;
+        double* d[3];
+    };
+    double nshot, omin, omax, sx0, sz0, rz0, dsx, nx, nz, dx, dz, nt, dt, f0, bxl, bxr, bzu, bzd, oe, o1, o2;
+    const Card cards[] = {{1, {&nshot}}, {2, {&omin, &omax}}, {3, {&sx0, &sz0, &rz0}}, {1, {&dsx}},
+                          {2, {&nx, &nz}}, {2, {&dx, &dz}},   {1, {&nt}},             {1, {&dt}},
+                          {1, {&f0}},    {2, {&bxl, &bxr}},   {2, {&bzu, &bzd}},      {1, {&oe}},
+                          {1, {&o1}},    {1, {&o2}}};
+    for (const Card& c : cards) {
+        if (rc != SFD_OK) break;
+        if (!read_line(f, &label) || !read_line(f, &line)) {
+            rc = SFD_ERR_IO;
+            break;
+        }
+        const std::vector<double> v = numbers(line);
+        if ((int)v.size() < c.n) {
+            rc = SFD_ERR_ARG;
+            break;
+        }
+        for (int i = 0; i < c.n; i++) *c.d[i] = v[i];
+    }
+    std::fclose(f);
+    if (rc != SFD_OK) return rc;
+    p->nshot = (int)nshot;
+    p->offset_min = (float)omin;
+    p->offset_max = (float)omax;
+    p->sx0 = (float)sx0;
+    p->sz0 = (float)sz0;
+    p->rz0 = (float)rz0;
+    p->dsx = (float)dsx;
+    p->nx_v = (int)nx;
+    p->nz_v = (int)nz;
+    p->dx_v = (float)dx;
+    p->dz_v = (float)dz;
+    p->nt = (int)nt;
+    p->dt = (float)dt;
+    p->f0 = (float)f0;
+    p->bound_x_l = (float)bxl;
+    p->bound_x_r = (float)bxr;
+    p->bound_z_u = (float)bzu;
+    p->bound_z_d = (float)bzd;
+    p->order_explicit = (int)oe;
+    p->order_pml_1st = (int)o1;
+    p->order_pml_2nd = (int)o2;
+    return SFD_OK;
+}
+
 int sfd_isopar_read(const char* path, sfd_isopar* p) {
     if (!path || !p) return SFD_ERR_ARG;
     FILE* f = std::fopen(path, "rb");
@@ -237,7 +298,7 @@ int sfd_su_write_ex(const char* path, const float* traces, int ntr, int nt, int 
     for (int i = 1; i <= ntr && rc == SFD_OK; i++) {
         const int gx = (int)((float)(ixmin - 1 + i - 1) * dx);
         put32(h, 80, gx);                                            // gx
-        put32(h, 36, gx - sx);                                       // offset
+        if (!(flags & SFD_SU_NO_OFFSET)) put32(h, 36, gx - sx);      // offset
         if (flags & SFD_SU_CDP) put32(h, 20, (int)std::lround((float)(gx + sx) / dx) + 1);  // cdp
         if (std::fwrite(h, 1, 240, f) != 240 ||
             std::fwrite(traces + (size_t)(i - 1) * nt, sizeof(float), (size_t)nt, f) != (size_t)nt)

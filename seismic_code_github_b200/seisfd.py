@@ -74,6 +74,7 @@ def read_isopar(path: str) -> IsoPar:
 
 
 SU_CDP = 0x1
+SU_NO_OFFSET = 0x2  # leave offset 0, as the VTI modeller's writer does (VS:163-217)
 
 
 def su_write(path: str, traces: np.ndarray, shot_no: int, isx: int, ixmin: int, dx: float, dt: float,
@@ -106,6 +107,18 @@ class VtiPar(ctypes.Structure):
                 ("nx_bound_r", ctypes.c_int), ("nz_bound_u", ctypes.c_int), ("nz_bound_d", ctypes.c_int),
                 ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int),
                 ("flags", ctypes.c_int)]
+
+
+class VtiCardFields(ctypes.Structure):
+    """sfd_vtipar: the VTI modeller's parameter card (VS:342-425) as sfd_vtipar_read fills it."""
+    _fields_ = [("vz", ctypes.c_char * 256), ("epsilon", ctypes.c_char * 256), ("delta", ctypes.c_char * 256),
+                ("shot1", ctypes.c_char * 256), ("shot2", ctypes.c_char * 256), ("nshot", ctypes.c_int),
+                ("offset_min", ctypes.c_float), ("offset_max", ctypes.c_float), ("sx0", ctypes.c_float),
+                ("sz0", ctypes.c_float), ("rz0", ctypes.c_float), ("dsx", ctypes.c_float), ("nx_v", ctypes.c_int),
+                ("nz_v", ctypes.c_int), ("dx_v", ctypes.c_float), ("dz_v", ctypes.c_float), ("nt", ctypes.c_int),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("bound_x_l", ctypes.c_float),
+                ("bound_x_r", ctypes.c_float), ("bound_z_u", ctypes.c_float), ("bound_z_d", ctypes.c_float),
+                ("order_explicit", ctypes.c_int), ("order_pml_1st", ctypes.c_int), ("order_pml_2nd", ctypes.c_int)]
 
 
 class VtiShot(ctypes.Structure):
@@ -159,6 +172,7 @@ SIGNATURES = {
     "sfd_fd_coeffs": (ctypes.c_int, [ctypes.c_int, _F32P]),
     "sfd_pad_model": (ctypes.c_int, [_F32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, _F32P]),
+    "sfd_vtipar_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p]),
     "sfd_vti_coefficients": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _F32P]),
     "sfd_vti_forward": (ctypes.c_int, [ctypes.POINTER(VtiPar), _F32P, _F32P, _F32P, ctypes.c_int,
                                        ctypes.POINTER(VtiShot), ctypes.c_int, _F32P, ctypes.POINTER(Timing)]),

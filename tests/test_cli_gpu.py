@@ -228,3 +228,39 @@ def test_iso_forward_program_against_restatement(tmp_path, mode, hilly):
     _, _, fin = ol.iso_forward(vp, vs, rho, p.dx, p.dz, p.dt, p.f0, last - idecay, np_, np_, isx - ixmine + np_ + 1,
                                refs[-1][5], ixmine=ixmine, ixmaxe=ixmine + nxe - 1, want_final=True, **kw)
     assert bits_equal(snap, fin[np_:np_ + nxe, top:top + nz])
+
+
+def test_vti_forward_program_against_restatement(tmp_path):
+    """vti_forward on a card of three shots whose apertures reach past the model's left edge: the
+    merged SU file holds the FP32 restatement's records bit for bit, computed with epsilon and
+    delta zero as read_data leaves them (VS:147-148), with VS:184-214's headers (fldr, trid, sx,
+    gx, ns, dt; no offset, no cdp)."""
+    from test_fileio import VTICARD, expected_header
+    nx, nz, nt = 200, 80, 300
+    rng = np.random.default_rng(21)
+    z = np.arange(nz)
+    vz = np.tile(np.where(z < 40, 1900.0, 2600.0), (nx, 1)).astype(np.float32)
+    vz += rng.uniform(-40, 40, vz.shape).astype(np.float32)
+    vz.tofile(tmp_path / "vz.bin")
+    (0.2 * rng.random((nx, nz))).astype(np.float32).tofile(tmp_path / "eps.bin")
+    (0.1 * rng.random((nx, nz))).astype(np.float32).tofile(tmp_path / "delta.bin")
+    (tmp_path / "vti.par").write_text(VTICARD.format(d=str(tmp_path), nx=nx, nz=nz, nt=nt))
+    run([os.path.join(BIN, "vti_forward"), str(tmp_path / "vti.par")], cwd=tmp_path)
+    assert not (tmp_path / "vti_tmp1.su").exists()
+    raw = open(tmp_path / "vti_all.su", "rb").read()
+    zero = np.zeros_like(vz)
+    rec_bytes = 240 + 4 * nt
+    off = 0
+    for i in range(1, 4):
+        nsx = 21 + (i - 1) * 10  # nint(100/5) + 1 + nint((i-1) 50/5)
+        xmin, xmax = nsx - 60, nsx + 59
+        ref = ol.vti_forward(vz, zero, zero, 5.0, 5.0, 0.0005, 30.0, nt, (20, 20, 0, 20), nsx, 1, 1, xmin, xmax)
+        for tr in range(1, xmax - xmin + 2):
+            rec = raw[off:off + rec_bytes]
+            off += rec_bytes
+            want = bytearray(expected_header(i, nsx, xmin, 5.0, 0.0005, nt, tr))
+            want[20:24] = b"\0\0\0\0"
+            want[36:40] = b"\0\0\0\0"
+            assert rec[:240] == bytes(want), (i, tr)
+            assert np.array_equal(np.frombuffer(rec[240:], np.uint32), ref[tr - 1].view(np.uint32)), (i, tr)
+    assert off == len(raw)

@@ -1,8 +1,9 @@
 """CPU checks of the file contract helpers (seismic_code_github_b200/csrc/fileio.cpp): the
-Q_forward parameter card reader (QS:121-234), the yang_version card reader (YPUB:48-145), the SU
-shot writer (QS:1476-1546, and YPUB:1533-1604 without the cdp word), the merge (QS:1550-1624)
-and the raw float32 files.  The expected SU headers are built here from the
+Q_forward parameter card reader (QS:121-234), the yang_version card reader (YPUB:48-145), the VTI
+modeller's card reader (VS:342-425), the SU shot writer (QS:1476-1546, YPUB:1533-1604 without the
+cdp word, VS:163-217 without cdp and offset), the merge (QS:1550-1624) and the raw float32 files.  The expected SU headers are built here from the
 Fortran statements of QS:1502-1533 with numpy float32 arithmetic."""
+import ctypes
 import os
 import struct
 
@@ -239,6 +240,78 @@ def test_su_without_cdp(tmp_path):
         assert rec[:240] == bytes(want), i
 
 
+# A VTI modeller card in the layout of VS:383-421 (label line, value line), values of this test.
+VTICARD = """!*velocity filename*!
+{d}/vz.bin
+!*epsilon filename*!
+{d}/eps.bin
+!*delta filename*!
+{d}/delta.bin
+!*NO.1 shot record filename(tmp)*!
+{d}/vti_tmp
+!*NO.2 shot record filename(all)*!
+{d}/vti_all
+!*nshot(samples)*!
+3
+!*offset_min,offset_max*!
+-300  295.0
+!*sx0,sz0,rz0(m)*!
+100.0 0.0 0.0
+!*dsx(m)*!
+50.0
+!*nx_v,nz_v(samples)*!
+{nx} {nz}
+!*dx_v,dz_v(m)*!
+5.0 5.0
+!*nt(samples)*!
+{nt}
+!*dt(s)*!
+0.0005
+!*f0(Hz)*!
+30.0
+!*pml_thick x left and right direction(m)*!
+100.0 100.0
+!*pml_thick z up and down direction(m)*
+0.0 100.0
+!*fd_order_explicit*!
+10
+!*order_pml_1st*!
+9
+!*order_pml_2nd*!
+10
+"""
+
+
+def test_vti_card_reader(tmp_path):
+    (tmp_path / "vti.par").write_text(VTICARD.format(d="/data", nx=300, nz=200, nt=10000))
+    p = S.VtiCardFields()
+    assert S.load().sfd_vtipar_read(str(tmp_path / "vti.par").encode(), ctypes.byref(p)) == 0
+    assert p.vz.decode() == "/data/vz.bin" and p.delta.decode() == "/data/delta.bin"
+    assert p.shot1.decode() == "/data/vti_tmp" and p.shot2.decode() == "/data/vti_all"
+    assert (p.nshot, p.nx_v, p.nz_v, p.nt) == (3, 300, 200, 10000)
+    assert (p.offset_min, p.offset_max, p.sx0, p.dsx) == (-300.0, 295.0, 100.0, 50.0)
+    assert np.float32(p.dt) == np.float32(0.0005) and p.f0 == 30.0
+    assert (p.bound_x_l, p.bound_x_r, p.bound_z_u, p.bound_z_d) == (100.0, 100.0, 0.0, 100.0)
+    assert (p.order_explicit, p.order_pml_1st, p.order_pml_2nd) == (10, 9, 10)
+    (tmp_path / "short.par").write_text("\n".join(VTICARD.splitlines()[:20]))
+    assert S.load().sfd_vtipar_read(str(tmp_path / "short.par").encode(), ctypes.byref(p)) != 0
+
+
+def test_su_without_offset(tmp_path):
+    """The VTI modeller's writer (VS:184-214) sets fldr, trid, sx, gx, ns and dt only."""
+    nt, ntr = 17, 4
+    tr = np.random.default_rng(2).standard_normal((ntr, nt)).astype(np.float32)
+    path = str(tmp_path / "shot2.su")
+    S.su_write(path, tr, 2, 61, -239, 5.0, 0.0005, flags=S.SU_NO_OFFSET)
+    raw = open(path, "rb").read()
+    for i in range(1, ntr + 1):
+        rec = raw[(i - 1) * (240 + 4 * nt):i * (240 + 4 * nt)]
+        want = bytearray(expected_header(2, 61, -239, 5.0, 0.0005, nt, i))
+        want[20:24] = b"\0\0\0\0"
+        want[36:40] = b"\0\0\0\0"
+        assert rec[:240] == bytes(want), i
+
+
 def test_programs_are_built():
-    for name in ("afd_fd", "q_forward", "iso_forward"):
+    for name in ("afd_fd", "q_forward", "iso_forward", "vti_forward"):
         assert os.access(os.path.join(ROOT, "seismic_code_github_b200", "bin", name), os.X_OK)
