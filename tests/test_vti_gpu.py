@@ -77,6 +77,20 @@ def test_fast_mode_within_tolerance(name):
     assert e32 <= 1e-5 and e64 <= 1e-5
 
 
+def test_fast_mode_long_record():
+    """The default mode over 3000 samples (the error of approximate divisions and FMA contraction
+    accumulates with the record length): still within relative L2 1e-5 of the FP64 restatement."""
+    bounds, shot = CASES["reference_layout"]
+    vz, eps, de = model()
+    nt = 3000
+    rec, _ = S.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, [shot])
+    r64 = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *shot, fp64=True)
+    r32 = ol.vti_forward(vz, eps, de, 5.0, 5.0, 5e-4, 30.0, nt, bounds, *shot)
+    e64, e32 = rel_l2(rec[0], r64), rel_l2(r32, r64)
+    print(f"nt {nt}: fast mode relL2 vs FP64 {e64:.2e} (FP32 restatement vs FP64 {e32:.2e})")
+    assert e64 <= 1e-5
+
+
 def test_invalid_arguments():
     vz, eps, de = model(60, 40)
     with pytest.raises(S.SfdError) as e:  # shots of one call share the grid
