@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "sfd_internal.h"
 
@@ -654,6 +655,13 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // Programmatic dependent launch (the step kernels are launched with programmatic stream
+    // serialisation): the next step's CTAs may be scheduled once every CTA of this grid has
+    // started, so they fill the SMs that this step's last wave leaves idle.  Every thread waits
+    // here until the previous grid in the stream has completed and its writes are visible; all
+    // reads of wavefields, imaging sums and records follow this point.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
     if (NST == 1 && tid == 0 && a.l2_ahead > 0 && (int)blockIdx.x + a.l2_ahead < total)
         prefetch(blockIdx.x + a.l2_ahead);
@@ -707,6 +715,17 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
     }
 }
 
+// Programmatic dependent launch of consecutive step kernels (SFD_PDL=0 in the environment
+// turns it off; the kernels' griddepcontrol.wait is then a no-op)
+bool pdl_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* env = std::getenv("SFD_PDL");
+        on = (env && std::atoi(env) == 0) ? 0 : 1;
+    }
+    return on == 1;
+}
+
 int sm_count() {
     static int n = 0;
     if (n == 0) {
@@ -730,8 +749,17 @@ cudaError_t launch_t(const Acou2DArgs& a, int active, cudaStream_t st) {
     const int total = a.L.ntx * a.L.ntz * active;
     // one stage: one tile per CTA, two CTAs per SM; two stages: one persistent CTA per SM
     const int grid = NST == 1 ? total : (total < sm_count() ? total : sm_count());
-    k<<<grid, kThreads, smem, st>>>(a, active);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, a, active);
 }
 
 template <int R, bool ADJ>
