@@ -124,9 +124,10 @@ def cpu_reference_sample(case, steps_per_proc: int):
     import ref_runner
     procs = os.cpu_count() or 1
     pts = case.Nx * case.Nz * steps_per_proc
+    # the wavelet comes from a numpy restatement of tools/ricker.cpp:44: nothing of this
+    # repository's native library is loaded on the reference path
+    w = ref_runner.ric_wavelet(steps_per_proc, case.dt, case.f0, 150)
     if ref_runner.available():
-        from seismic_code_github_b200 import seisfd as S
-        w = S.wavelet(S.WAVELET_RIC, steps_per_proc, case.dt, case.f0, 150)
         cfgs = [ref_runner.AfdRefConfig(NX=case.NX, NZ=case.NZ, PML=case.PML, Nt=steps_per_proc, dx=case.dx,
                                         dz=case.dz, dt=case.dt, vp=case.vp, den=case.den, wavelet=w,
                                         sx=case.src_x[i % case.nshot], sz=case.src_z[i % case.nshot],
@@ -137,8 +138,6 @@ def cpu_reference_sample(case, steps_per_proc: int):
                           f"oracle/_ref/afd_ref) on the {case.Nx}x{case.Nz} padded grid, {steps_per_proc} steps each",
                 "wall_s": r["wall_s"]}
     import oracle_lib as ol
-    from seismic_code_github_b200 import seisfd as S
-    w = S.wavelet(S.WAVELET_RIC, steps_per_proc, case.dt, case.f0, 150)
     rx, rz = case.receivers()
     t0 = time.perf_counter()
     ol.afd_forward(case.Nx, case.Nz, case.PML, steps_per_proc, case.dx, case.dz, case.dt, case.vp, case.den, w,
@@ -183,9 +182,25 @@ def run_reference_arm(args, world, rank):
             "config": config_dict(case, args),
             "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
-            "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "repo_libs_mapped": repo_libs_mapped()}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def repo_libs_mapped():
+    """Shared objects of this repository mapped into this process (the reference arm must show
+    none: it runs the reference's own build and numpy only)."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and os.path.realpath(path).startswith(os.path.realpath(ROOT) + os.sep):
+                    found.add(os.path.relpath(os.path.realpath(path), os.path.realpath(ROOT)))
+    except OSError:
+        return None
+    return sorted(found)
 
 
 def measure_gradient(args, dev):

@@ -27,7 +27,7 @@ Declared patch (each anchor must match exactly once, otherwise the build fails):
                default keeps the original vertical line P1[nx_location][i]
 Arithmetic, loop order and update semantics of the time loop (AFD:237-380) are untouched.
 
-Usage: python oracle/ref_build.py [--reference /root/reference]
+Usage: python oracle/ref_build.py [--reference DIR]   (default: $SFD_REFERENCE, else /root/reference)
 """
 import argparse
 import os
@@ -137,7 +137,7 @@ def build(reference: str) -> None:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("SFD_REFERENCE", "/root/reference"))
     a = ap.parse_args()
     build(a.reference)
 

@@ -21,6 +21,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+def ric_wavelet(nt: int, dt: float, f0: float, delay: int = 150) -> np.ndarray:
+    """The Ricker trace of tools/ricker.cpp:44 (pi = 3.1415926, integer frequency, double
+    arithmetic, delay in samples), rounded to float32: the wavelet fed to the reference build."""
+    pi = 3.1415926
+    j = np.arange(nt, dtype=np.float64)
+    a = pi * float(int(f0)) * (j - delay) * np.float64(np.float32(dt))
+    return ((1 - 2 * a * a) * np.exp(-a * a)).astype(np.float32)
+
+
 def ref_binary(name: str = "afd_ref") -> str:
     return os.path.join(REF_DIR, name)
 

@@ -261,12 +261,8 @@ cudaError_t launch_t(const Acou2DArgs& a, int active, cudaStream_t st) {
     // the reference-order kernel; the FMA path lives in acoustic2d_fma.cu
     const size_t smem = sizeof(float) * Tile<R>::SMEM_FLOATS;
     auto k = acoustic2d_step_kernel<R, EXACT, VARDEN>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static bool attr[kMaxDevices] = {};
+    if (cudaError_t e = smem_attr_once((const void*)k, (int)smem, attr)) return e;
     dim3 grid(a.L.ntx * a.L.ntz, active);
     k<<<grid, kThreads, smem, st>>>(a);
     return cudaGetLastError();

@@ -740,12 +740,8 @@ template <int R, int NST, bool VARDEN, bool ADJ>
 cudaError_t launch_t(const Acou2DArgs& a, int active, cudaStream_t st) {
     const size_t smem = sizeof(float) * TP<R, NST>::SMEM_FLOATS;
     auto k = acoustic2d_step_fma_kernel<R, NST, VARDEN, ADJ>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static bool attr[kMaxDevices] = {};
+    if (cudaError_t e = smem_attr_once((const void*)k, (int)smem, attr)) return e;
     const int total = a.L.ntx * a.L.ntz * active;
     // one stage: one tile per CTA, two CTAs per SM; two stages: one persistent CTA per SM
     const int grid = NST == 1 ? total : (total < sm_count() ? total : sm_count());

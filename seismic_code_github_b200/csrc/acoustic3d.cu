@@ -607,12 +607,8 @@ template <int R, bool VARDEN, bool ADJ>
 cudaError_t launch_t(const Acou3DArgs& a, int active, cudaStream_t st) {
     const size_t smem = sizeof(float) * K3<R>::SMEM_FLOATS;
     auto k = acoustic3d_step_kernel<R, VARDEN, ADJ>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static bool attr[kMaxDevices] = {};
+    if (cudaError_t e = smem_attr_once((const void*)k, (int)smem, attr)) return e;
     const dim3 grid(a.L.nty * a.L.ntz, active);
     k<<<grid, kThreads, smem, st>>>(a);
     return cudaGetLastError();

@@ -440,14 +440,9 @@ __global__ void __launch_bounds__(32) iso_smooth_kernel(const __grid_constant__ 
 cudaError_t elastic2d_launch_step(const IArgs& a, int active, int nx_max, cudaStream_t st, int* launches) {
     dim3 grid(a.L.ntx * a.L.ntz, active);
     const size_t smem = sizeof(float) * 3 * SMEM;
-    static bool attr = false;
-    if (!attr) {
-        for (auto k : {iso_velocity_kernel<false>, iso_velocity_kernel<true>}) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        attr = true;
-    }
+    static bool attr0[kMaxDevices] = {}, attr1[kMaxDevices] = {};
+    if (cudaError_t e = smem_attr_once((const void*)iso_velocity_kernel<false>, (int)smem, attr0)) return e;
+    if (cudaError_t e = smem_attr_once((const void*)iso_velocity_kernel<true>, (int)smem, attr1)) return e;
     *launches = 2;
     if (a.fs) {
         iso_velocity_kernel<true><<<grid, kThreads, smem, st>>>(a);

@@ -59,6 +59,9 @@ extern "C" int sfd_forward_noalloc(const sfd_grid* g, const float* vp_dev, const
                                    const int* rec_z, float* records_dev, void* stream) {
     if (!g || !vp_dev || !wavelet_dev || nt < 1 || nrec < 0 || (nrec > 0 && (!rec_x || !rec_z || !records_dev)))
         return SFD_ERR_ARG;
+    // an error left pending by earlier work of the caller's thread is not this call's: drop it so
+    // that the launch checks below report only this call's launches
+    (void)cudaGetLastError();
     if (g->scheme != SFD_ACOUSTIC_2D || g->ny > 1) return SFD_ERR_UNSUPPORTED;
     float cf[8];
     if (sfd_fd_coeffs(g->order, cf) != SFD_OK) return SFD_ERR_ARG;

@@ -12,6 +12,21 @@
 namespace sfd {
 
 constexpr int kMaxRadius = 8;
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per device: the attribute belongs to the
+// device, so a kernel first launched on a second GPU of the process needs it set there as well.
+// `done` is the calling launcher's static table (one flag per device ordinal).
+constexpr int kMaxDevices = 64;
+inline cudaError_t smem_attr_once(const void* fn, int bytes, bool* done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const bool tracked = dev >= 0 && dev < kMaxDevices;
+    if (tracked && done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && tracked) done[dev] = true;
+    return e;
+}
 // Both 2-D acoustic step kernels work on the same 64 x 64 tiles, so they share the field
 // layout and the per-tile receiver tables.
 constexpr int kTileX = 64;

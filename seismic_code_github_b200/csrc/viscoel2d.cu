@@ -267,12 +267,8 @@ __global__ void __launch_bounds__(kThreads) e_stress_kernel(const __grid_constan
 cudaError_t viscoel2d_launch_step(const EArgs& a, int active, cudaStream_t st) {
     dim3 grid(a.L.ntx * a.L.ntz, active);
     const size_t smem = sizeof(float) * 3 * SMEM;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(e_velocity_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static bool attr[kMaxDevices] = {};
+    if (cudaError_t e = smem_attr_once((const void*)e_velocity_kernel, (int)smem, attr)) return e;
     e_velocity_kernel<<<grid, kThreads, smem, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

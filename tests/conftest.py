@@ -6,6 +6,8 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# the reference checkout (only CPU tests that read its shipped cards use it; they skip without it)
+REFERENCE = os.environ.get("SFD_REFERENCE", "/root/reference")
 for p in (ROOT, os.path.join(ROOT, "oracle")):
     if p not in sys.path:
         sys.path.insert(0, p)

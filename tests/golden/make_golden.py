@@ -16,7 +16,7 @@ reference tree and the builds of oracle/ref_build.py; the GPU tests only read th
         every-10-steps Pall.dat switched on: the outputs of the afd_fd program are pinned to it.
   manifest.json      sizes and sha256 of the above.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py [--reference DIR]   (default: $SFD_REFERENCE, else /root/reference)
 """
 import argparse
 import hashlib
@@ -55,7 +55,7 @@ def ric_wavelet(nt, dt, f0, delay=150):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("SFD_REFERENCE", "/root/reference"))
     args = ap.parse_args()
     ref = args.reference
     if not ref_runner.available():

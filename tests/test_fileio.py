@@ -10,7 +10,7 @@ import struct
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import REFERENCE, ROOT
 from seismic_code_github_b200 import seisfd as S
 
 CARD = """!*P-wave velocity filename*!
@@ -74,7 +74,7 @@ def test_parameter_card(tmp_path, eol):
 
 def test_reference_parameter_card():
     """The card shipped with the reference (forward/Q_forward/isoq_2d_modelling_simple.par)."""
-    path = "/root/reference/forward/Q_forward/isoq_2d_modelling_simple.par"
+    path = os.path.join(REFERENCE, "forward/Q_forward/isoq_2d_modelling_simple.par")
     if not os.path.exists(path):
         pytest.skip("reference tree not present")
     q = S.read_qpar(path)
@@ -216,7 +216,7 @@ def test_yang_parameter_card(tmp_path):
 
 def test_reference_yang_parameter_card():
     """The card shipped with the reference (forward/yang_version_2016_2_2/iso_2d_modelling_sin_test.par)."""
-    path = "/root/reference/forward/yang_version_2016_2_2/iso_2d_modelling_sin_test.par"
+    path = os.path.join(REFERENCE, "forward/yang_version_2016_2_2/iso_2d_modelling_sin_test.par")
     if not os.path.exists(path):
         pytest.skip("reference tree not present")
     q = S.read_isopar(path)
