@@ -211,6 +211,13 @@ int sfd_gradient_per_shot(sfd_ctx* ctx, const float* obs, float* misfit, float* 
  * wavelet-to-records map, used by the dot-product test. */
 int sfd_get_wavelet_gradient(sfd_ctx* ctx, int shot, float* out);
 
+/* Test hook of the step kernels' bounded waits (no counterpart in the reference, which has no
+ * device waits): in the forwards and gradients that follow, CTA `cta` of the 2-D acoustic FMA
+ * step `step` issues none of its TMA box loads and gives up waiting for them after limit_s
+ * seconds (0 < limit_s <= 10; every other wait keeps its limit of about one second).  That call
+ * returns SFD_ERR_TIMEOUT and leaves the context usable.  cta < 0 removes the hook. */
+int sfd_test_wait_timeout(sfd_ctx* ctx, int cta, int step, double limit_s);
+
 /* Checkpoint interval of sfd_gradient in steps (0 = ceil(sqrt(nt))).  The forward state of
  * every shot is kept every `steps` steps; each segment is recomputed once during the
  * backward pass, so memory is O(nt/steps + steps) wavefields per shot. */

@@ -272,7 +272,7 @@ template <int R>
 cudaError_t launch_r(const Acou2DPlan& plan, const Acou2DArgs& a, int active, bool exact, bool varden,
                      cudaStream_t st) {
     if (exact) return varden ? launch_t<R, true, true>(a, active, st) : launch_t<R, true, false>(a, active, st);
-    return acoustic2d_fma_launch(R, a, active, varden, plan.stages, st);
+    return acoustic2d_fwd_launch(plan, R, a, active, varden, st);
 }
 
 }  // namespace
@@ -288,6 +288,7 @@ bool acoustic2d_plan(int radius, Acou2DPlan* plan) {
         plan->smem_bytes = sizeof(float) * Tile<RR>::SMEM_FLOATS;     \
         plan->gz = acoustic2d_fma_gz(RR);                             \
         plan->stages = 1;                                             \
+        plan->seg = 0;                                                \
         return true;
         SFD_PLAN(1) SFD_PLAN(2) SFD_PLAN(4) SFD_PLAN(5) SFD_PLAN(8)
 #undef SFD_PLAN

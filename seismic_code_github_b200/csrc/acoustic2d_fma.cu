@@ -623,10 +623,13 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
         z0 = (tile - tx_i * a.L.ntz) * T::TZ;
         return x0 < a.shots[shot].nx;
     };
+    // the test hook: this CTA issues no loads and waits test_wait_ns instead of about one second
+    const bool probed = (int)blockIdx.x == a.test_cta && a.step == a.test_step;
+    const unsigned long long wait_ns = probed ? a.test_wait_ns : 1000000000ull;
     // thread 0: start the three box loads of tile t into stage stg
     auto issue = [&](int t, int stg) {
         int shot, tile, x0, z0;
-        if (!locate(t, shot, tile, x0, z0)) return;
+        if (probed || !locate(t, shot, tile, x0, z0)) return;
         float* st = smem + stg * T::STAGE;
         uint64_t* bar = bars + stg;
         // order this thread's view of earlier generic-proxy writes to the stage before the
@@ -690,7 +693,7 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
             bool ok = mbar_try_wait(bars + b, pa);
             if (!ok) {
                 const uint64_t t0 = global_ns();
-                while (!(ok = mbar_try_wait(bars + b, pa)) && global_ns() - t0 < 1000000000ull) {
+                while (!(ok = mbar_try_wait(bars + b, pa)) && global_ns() - t0 < wait_ns) {
                 }
             }
             return ok;
@@ -713,17 +716,6 @@ acoustic2d_step_fma_kernel(const __grid_constant__ Acou2DArgs a, int active) {
         else tile_body<R, NST, VARDEN, false, ADJ>(a, smem, st, sd, shot, tile, x0, z0);
         __syncthreads();  // stage, interleave buffer and tables are free again
     }
-}
-
-// Programmatic dependent launch of consecutive step kernels (SFD_PDL=0 in the environment
-// turns it off; the kernels' griddepcontrol.wait is then a no-op)
-bool pdl_enabled() {
-    static int on = -1;
-    if (on < 0) {
-        const char* env = std::getenv("SFD_PDL");
-        on = (env && std::atoi(env) == 0) ? 0 : 1;
-    }
-    return on == 1;
 }
 
 int sm_count() {
@@ -774,6 +766,23 @@ void boxes_t(int bp[2], int bvx[2], int bvz[2]) {
 }
 
 }  // namespace
+
+// Programmatic dependent launch of consecutive step kernels (SFD_PDL=0 in the environment
+// turns it off; the kernels' griddepcontrol.wait is then a no-op)
+bool pdl_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* env = std::getenv("SFD_PDL");
+        on = (env && std::atoi(env) == 0) ? 0 : 1;
+    }
+    return on == 1;
+}
+
+cudaError_t acoustic2d_fwd_launch(const Acou2DPlan& plan, int radius, const Acou2DArgs& a, int active, bool varden,
+                                  cudaStream_t st) {
+    if (plan.seg > 0) return acoustic2d_march_launch(radius, a, active, varden, plan.seg, st, pdl_enabled());
+    return acoustic2d_fma_launch(radius, a, active, varden, plan.stages, st);
+}
 
 cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, bool varden, int stages,
                                  cudaStream_t st, bool adj) {

@@ -68,6 +68,8 @@ struct sfd_ctx {
     int* d_tri = nullptr;      // per-tile receiver indices
     int* d_torder = nullptr;   // FMA kernel's forward tile order: interior tiles, then edge tiles
     int tile_major = 1;        // forward steps of the FMA kernel: tile-major over d_torder
+    int test_cta = -1, test_step = 0;      // sfd_test_wait_timeout
+    unsigned long long test_wait_ns = 0;
     int l2_ahead = 0;          // FMA kernel, one tile per CTA: L2 prefetch distance in CTAs
     float* d_rec_tn = nullptr; // [nt][nrec] per shot
     float* d_rec_nt = nullptr; // [nrec][nt] per shot (output layout)
@@ -76,6 +78,7 @@ struct sfd_ctx {
     int* d_flag = nullptr;     // NaN watchdog
     int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
     CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
+    CUtensorMap mtmaps[6];     // the same buffers with the x-marching kernel's boxes
 
     // 3-D scheme: dense [x][y][pitch] slabs, 8 fields (P, Vx, Vy, Vz, two buffers each)
     Layout3D L3{};
@@ -355,7 +358,13 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.tm_p = c->tmaps[i];
     a.tm_vx = c->tmaps[2 + i];
     a.tm_vz = c->tmaps[4 + i];
+    a.tm_mp = c->mtmaps[i];
+    a.tm_mvx = c->mtmaps[2 + i];
+    a.tm_mvz = c->mtmaps[4 + i];
     a.err_flag = c->d_err;
+    a.test_cta = c->test_cta;
+    a.test_step = c->test_step;
+    a.test_wait_ns = c->test_wait_ns;
     a.step = step;
     for (const auto& sn : c->snaps)
         if (sn.count > 0 && sn.field == SFD_FIELD_P) a.src_pre = c->d_src_pre;
@@ -708,24 +717,44 @@ int finish_nan(sfd_ctx* ctx) {
     return SFD_OK;
 }
 
-// Tuner for the FMA step kernel's schedule (one tile per CTA with two CTAs per SM, or
-// persistent CTAs with double-buffered TMA): a few steps of each on the real shot set, the
-// faster one is kept.  SFD_FMA_STAGES=1|2 in the environment forces a schedule.
+// Tuner for the forward step of the default (FMA) scheme.  Candidates: the tile kernel with one
+// tile per CTA (two CTAs per SM), the persistent tile kernel with double-buffered TMA, and the
+// x-marching kernel with segments of 128, 256 or 512 columns (segments longer than the shots are
+// skipped).  Each runs a few steps on the real shot set, twice; the fastest is kept.  All
+// candidates give bit-identical results.  SFD_FMA_STAGES=1|2 forces a tile schedule,
+// SFD_MARCH_SEG=<columns> forces the x-marching kernel with that segment length.
 int tune_schedule(sfd_ctx* ctx) {
     if ((ctx->g.flags & SFD_EXACT) || ctx->g.scheme != SFD_ACOUSTIC_2D) return SFD_OK;
     if (const char* env = std::getenv("SFD_FMA_STAGES")) {
         const int s = std::atoi(env);
         if (s == 1 || s == 2) {
             ctx->plan.stages = s;
+            ctx->plan.seg = 0;
             return SFD_OK;
         }
     }
+    if (const char* env = std::getenv("SFD_MARCH_SEG")) {
+        const int s = std::atoi(env);
+        if (s >= 16 && s % 16 == 0) {
+            ctx->plan.stages = 1;
+            ctx->plan.seg = s;
+            return SFD_OK;
+        }
+    }
+    struct Cand {
+        int stages, seg;
+    };
+    std::vector<Cand> cands = {{1, 0}, {2, 0}};
+    const int width = ctx->L.ntx * ctx->L.tx;
+    for (int seg : {128, 256, 512})
+        if (seg < width || seg == 128) cands.push_back({1, seg});
     const int act = active_shots(ctx, 0);
     const int steps = std::min(ctx->nt_max, 10);
-    float best[3] = {1e30f, 1e30f, 1e30f};
-    for (int round = 0; round < 2; round++)  // two rounds, best of each schedule
-        for (int s = 1; s <= 2; s++) {
-            ctx->plan.stages = s;
+    std::vector<float> best(cands.size(), 1e30f);
+    for (int round = 0; round < 2; round++)  // two rounds, best of each candidate
+        for (size_t ci = 0; ci < cands.size(); ci++) {
+            ctx->plan.stages = cands[ci].stages;
+            ctx->plan.seg = cands[ci].seg;
             int rc = prologue(ctx);
             if (rc) return rc;
             for (int k = 0; k < steps; k++) {
@@ -736,9 +765,13 @@ int tune_schedule(sfd_ctx* ctx) {
             CK(cudaStreamSynchronize(ctx->stream));
             float ms = 0.0f;
             if (steps > 2) CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-            best[s] = std::min(best[s], ms);
+            best[ci] = std::min(best[ci], ms);
         }
-    ctx->plan.stages = best[2] < best[1] ? 2 : 1;
+    size_t pick = 0;
+    for (size_t ci = 1; ci < cands.size(); ci++)
+        if (best[ci] < best[pick]) pick = ci;
+    ctx->plan.stages = cands[pick].stages;
+    ctx->plan.seg = cands[pick].seg;
     return SFD_OK;
 }
 
@@ -747,7 +780,8 @@ int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_VISCOAC_2D) return 40;
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
-    return (ctx->g.flags & SFD_EXACT) ? 1 : 10 + ctx->plan.stages;
+    if (ctx->g.flags & SFD_EXACT) return 1;
+    return ctx->plan.seg > 0 ? 13 : 10 + ctx->plan.stages;
 }
 
 int run_forward(sfd_ctx* ctx, float* out_dev) {
@@ -917,7 +951,7 @@ int grad_fwd_step(sfd_ctx* ctx, const GradRange& r, int k, int act, float* div_o
     Acou2DArgs a = make_args(ctx, k);
     a.slot_to_shot = r.slots;
     a.div_out = div_out;
-    CK(acoustic2d_fma_launch(ctx->radius, a, act, ctx->varden, ctx->plan.stages, ctx->stream));
+    CK(acoustic2d_fwd_launch(ctx->plan, ctx->radius, a, act, ctx->varden, ctx->stream));
     return SFD_OK;
 }
 
@@ -2218,8 +2252,12 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         acoustic2d_fma_boxes(ctx->radius, bp, bvx, bvz);
         const int* boxes[3] = {bp, bvx, bvz};
         const long long fs = (long long)nshot * L.shot_stride;
+        int mp[2], mvx[2], mvz[2];
+        acoustic2d_march_boxes(mp, mvx, mvz);
+        const int* mboxes[3] = {mp, mvx, mvz};
         for (int b = 0; b < 6; b++) {
-            const int rc2 = encode_field_map(ctx, &ctx->tmaps[b], ctx->d_state + b * fs, L, nshot, boxes[b / 2]);
+            int rc2 = encode_field_map(ctx, &ctx->tmaps[b], ctx->d_state + b * fs, L, nshot, boxes[b / 2]);
+            if (!rc2) rc2 = encode_field_map(ctx, &ctx->mtmaps[b], ctx->d_state + b * fs, L, nshot, mboxes[b / 2]);
             if (rc2) return rc2;
         }
     }
@@ -2457,6 +2495,16 @@ int sfd_set_memory_limit(sfd_ctx* ctx, long long bytes) {
 int sfd_set_checkpoint_interval(sfd_ctx* ctx, int steps) {
     if (!ctx || steps < 0) return SFD_ERR_ARG;
     ctx->ckpt_interval = steps;
+    return SFD_OK;
+}
+
+int sfd_test_wait_timeout(sfd_ctx* ctx, int cta, int step, double limit_s) {
+    if (!ctx || (cta >= 0 && (step < 0 || !(limit_s > 0.0) || limit_s > 10.0))) return SFD_ERR_ARG;
+    ctx->test_cta = cta < 0 ? -1 : cta;
+    ctx->test_step = step;
+    ctx->test_wait_ns = cta < 0 ? 0ull : (unsigned long long)(limit_s * 1e9);
+    ctx->graph_valid = false;  // the captured loop holds the step arguments
+    ctx->grad_valid = false;
     return SFD_OK;
 }
 

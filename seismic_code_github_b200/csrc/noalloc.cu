@@ -161,6 +161,7 @@ extern "C" int sfd_forward_noalloc(const sfd_grid* g, const float* vp_dev, const
 
     // step arguments: the model and wavelet are read in place from the caller's buffers
     Acou2DArgs a{};
+    a.test_cta = -1;  // no test hook
     const long long fs = L.shot_stride;
     a.L = L;
     a.nz = nz;

@@ -230,7 +230,13 @@ void viscoac2d_stamp(int nx, int nz, int sx, int sz, int* box, std::vector<float
 struct Acou2DArgs {
     // TMA descriptors of this step's input fields (3-D: z, column, shot), used by the FMA kernel
     CUtensorMap tm_p, tm_vx, tm_vz;
+    // the same fields with the boxes of the x-marching kernel (acoustic2d_march.cu)
+    CUtensorMap tm_mp, tm_mvx, tm_mvz;
     int* err_flag;          // set to 1 by a CTA whose bounded wait ran out (SFD_ERR_TIMEOUT)
+    // test hook of the bounded waits (sfd_test_wait_timeout): CTA test_cta of step test_step
+    // issues no box loads and gives up its waits after test_wait_ns; test_cta < 0: off
+    int test_cta, test_step;
+    unsigned long long test_wait_ns;
     const float* p_in;  float* p_out;
     const float* vx_in; float* vx_out;
     const float* vz_in; float* vz_out;
@@ -302,7 +308,8 @@ struct Acou2DPlan {
     int tx, tz, threads;
     size_t smem_bytes;
     int gz;      // z ghost margin the step kernels need (multiple of 4)
-    int stages;  // FMA kernel schedule (1 or 2), chosen by the context's tuner
+    int stages;  // FMA tile kernel schedule (1 or 2)
+    int seg;     // > 0: forward steps run the x-marching kernel with segments of `seg` columns
 };
 // Model arrays on the device carry this many replicated rows above z = 0 and below z = nz - 1
 // so that vectorised halo reads stay inside the allocation and see finite values.
@@ -315,6 +322,18 @@ cudaError_t acoustic2d_launch_step(const Acou2DPlan& plan, const Acou2DArgs& a, 
 cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, bool varden, int stages,
                                  cudaStream_t st, bool adj = false);
 int acoustic2d_fma_gz(int radius);
+// Forward step of the FMA scheme on the x-marching kernel (bit-identical to the tile kernel):
+// one CTA per (shot, 64-wide z strip, segment of seg_cols columns), seg_cols a multiple of 16.
+cudaError_t acoustic2d_march_launch(int radius, const Acou2DArgs& a, int active, bool varden, int seg_cols,
+                                   cudaStream_t st, bool pdl);
+// TMA box extents (z, x) of the x-marching kernel's P, Vx and Vz loads.
+void acoustic2d_march_boxes(int box_p[2], int box_vx[2], int box_vz[2]);
+// Forward step of the default (FMA) scheme with the plan's kernel: x-marching when plan.seg > 0,
+// else the tile kernel with plan.stages.
+cudaError_t acoustic2d_fwd_launch(const Acou2DPlan& plan, int radius, const Acou2DArgs& a, int active, bool varden,
+                                  cudaStream_t st);
+// Programmatic dependent launch of consecutive step kernels (SFD_PDL=0 turns it off).
+bool pdl_enabled();
 // TMA box extents (z, x) the FMA kernel loads for P, Vx and Vz at this radius.
 void acoustic2d_fma_boxes(int radius, int box_p[2], int box_vx[2], int box_vz[2]);
 cudaError_t acoustic2d_launch_inject0(const Acou2DArgs& a, int nshot, bool exact, cudaStream_t st);

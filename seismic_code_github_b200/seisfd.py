@@ -146,6 +146,7 @@ SIGNATURES = {
     "sfd_gradient_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sfd_test_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "sfd_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "sfd_set_gauss_radius": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_set_free_surface": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -422,6 +423,11 @@ class Engine:
         out = np.empty(self._shots[shot].nt, np.float32)
         self._check(self._lib.sfd_get_wavelet_gradient(self._h, shot, _fp(out)), "sfd_get_wavelet_gradient")
         return out
+
+    def test_wait_timeout(self, cta: int, step: int, limit_s: float = 1e-4):
+        """Test hook (sfd_test_wait_timeout): CTA `cta` of step `step` issues no tile loads and
+        gives up its bounded wait after limit_s seconds; cta < 0 removes the hook."""
+        self._check(self._lib.sfd_test_wait_timeout(self._h, cta, step, limit_s), "sfd_test_wait_timeout")
 
     def set_checkpoint_interval(self, steps: int):
         self._check(self._lib.sfd_set_checkpoint_interval(self._h, steps), "sfd_set_checkpoint_interval")
