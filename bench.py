@@ -264,9 +264,10 @@ def measure_gradient(args, dev):
 
 def measure_gradient_sharded(args, dev, world, rank):
     """Config 4 on N GPUs: every rank takes the gradient of its round-robin share of the shots
-    (forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90:124-141) and one all-reduce (NCCL)
-    sums the per-rank gradients and misfits.  Time: device time of the local gradient plus the
-    all-reduce, max over ranks."""
+    (forward/Q_forward/Q_multishot_fd_main_fsbc_zy_rotated.f90:124-141) into device memory
+    (sfd_gradient_device) and one all-reduce (NCCL, in place on the device) sums the per-rank
+    gradients and misfits; no host copy of the gradient.  Time: device time of the local gradient
+    plus the all-reduce, max over ranks."""
     import torch
     import torch.distributed as dist
     from seismic_code_github_b200 import seisfd as S
@@ -281,24 +282,24 @@ def measure_gradient_sharded(args, dev, world, rank):
                   device=dev) as e:
         e.set_model(vp_true, case.den)
         e.set_shots(shots)
-        obs = e.forward().copy()
+        obs = torch.from_numpy(e.forward().copy()).to(f"cuda:{dev}")
         e.set_model(case.vp, case.den)
         e.set_checkpoint_interval(case.extra["checkpoint_interval"])
-        mis, g, _ = e.gradient(obs)  # warm-up
-        SH.allreduce_gradient(mis, g, device=f"cuda:{dev}")
+        shape = (case.Nx, case.Nz)
+        SH.sharded_gradient_device(e, obs, shape)  # warm-up
         dist.barrier()
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        mis, g, _ = e.gradient(obs)
-        mis_all, g_all, _ = SH.allreduce_gradient(mis, g, device=f"cuda:{dev}")
+        mis_t, g_t, _ = SH.sharded_gradient_device(e, obs, shape)
         t1.record()
         torch.cuda.synchronize()
+        mis_all, g_all = float(mis_t.item()), g_t.cpu().numpy()
     ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=f"cuda:{dev}")
     dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     return {"workload": f"config 4 gradient, {len(case.src_x)} shots sharded round-robin over {world} GPUs, "
-                        f"one all-reduce of the {g.size * 4 / 1e6:.1f} MB gradient",
+                        f"one in-place NCCL all-reduce of the {g_all.size * 4 / 1e6:.1f} MB gradient on the device",
             "shots_per_s": len(case.src_x) / (ms.item() / 1e3), "ms": ms.item(), "misfit": float(mis_all),
             "grad_norm": float(np.linalg.norm(g_all))}
 
@@ -777,6 +778,171 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+# ----------------------------------------------------------------------------------------------
+# Small runs of one scheme for profiler captures (python bench.py --case NAME ...): a seeded
+# synthetic model with the benchmark geometries, one warm-up call and one timed call of the batched
+# path; prints the engine's timing record.  Sizes come from --case-n / --case-nshot / --case-nt so
+# that a capture stays small.
+# ----------------------------------------------------------------------------------------------
+
+def case_acoustic3d(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    n, pml, d, dt = args.case_n, min(50, args.case_n // 8), 10.0, 1e-3
+    z = np.arange(n)
+    vp = np.empty((n, n, n), np.float32)
+    vp[:] = (1500.0 + 2500.0 * z / n)[None, None, :]
+    w = S.wavelet(S.WAVELET_RIC, args.case_nt, dt, 15.0, 40)
+    r = np.arange(pml, n - pml, dtype=np.int32)
+    shots = [S.ShotSpec(n // 2, pml + 5, r, np.full_like(r, pml + 2), w, sy=n // 2, rec_y=r)
+             for _ in range(args.case_nshot)]
+    with S.Engine(S.ACOUSTIC_3D, n, n, d, d, dt, pml, order=8, ny=n, dy=d) as e:
+        e.set_model(vp)
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def case_viscoac(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.case_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, args.case_nt, c["dt"], c["f0"]))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.VISCOAC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model(c["vp"], c["rho"], c["q"])
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def case_viscoel(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.case_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, args.case_nt, c["dt"], c["f0"]))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.VISCOEL_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"], c["q"],
+                            (0.7 * c["q"]).astype(np.float32))
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def case_elastic(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.case_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_ISO, args.case_nt, c["dt"], c["f0"], delay=args.case_nt // 2))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.ELASTIC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model_elastic(c["vp"], (c["vp"] / 1.8).astype(np.float32), c["rho"])
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def case_forward2d(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    case = W.config2(nshot=args.case_nshot, nt=args.case_nt)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    shots = [S.ShotSpec(sx, sz, rx, rz, w) for sx, sz in zip(case.src_x, case.src_z)]
+    with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16) as e:
+        e.set_model(case.vp, case.den)
+        e.set_shots(shots)
+        e.forward_device(0)
+        e.forward_device(0)
+        return e.timing()
+
+
+def case_gradient(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    case, vp_true = W.config4(nshot=args.case_nshot, nt=args.case_nt)
+    w = S.wavelet(S.WAVELET_RIC, case.nt, case.dt, case.f0, 150)
+    rx, rz = case.receivers()
+    shots = [S.ShotSpec(sx, sz, rx, rz, w) for sx, sz in zip(case.src_x, case.src_z)]
+    with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16) as e:
+        e.set_model(vp_true, case.den)
+        e.set_shots(shots)
+        obs = e.forward()
+        e.set_model(case.vp, case.den)
+        e.set_checkpoint_interval(case.extra["checkpoint_interval"])
+        e.gradient(obs)
+        e.gradient(obs)
+        return e.timing()
+
+
+def case_qgradient(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.config3(nshot=args.case_nshot)
+    Nx, Nz = c["vp"].shape
+    rx = np.arange(c["PML"], Nx - c["PML"], dtype=np.int32)
+    rz = np.full_like(rx, c["rec_z"])
+    shots = [S.ShotSpec(sx, sz, rx, rz, S.wavelet(S.WAVELET_Q, args.case_nt, c["dt"], c["f0"]))
+             for sx, sz in zip(c["src_x"], c["src_z"])]
+    with S.Engine(S.VISCOAC_2D, Nx, Nz, c["dx"], c["dz"], c["dt"], c["PML"], order=10, f0=c["f0"]) as e:
+        e.set_model(c["vp"], c["rho"], (c["q"] * 0.8).astype(np.float32))
+        e.set_shots(shots)
+        obs = e.forward()
+        e.set_model(c["vp"], c["rho"], c["q"])
+        e.gradient(obs, want_invq=True)
+        e.gradient(obs, want_invq=True)
+        return e.timing()
+
+
+def case_gradient3d(args):
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    n, pml, d, dt = args.case_n, min(50, args.case_n // 8), 10.0, 1e-3
+    z = np.arange(n)
+    vp = np.empty((n, n, n), np.float32)
+    vp[:] = (1500.0 + 2500.0 * z / n)[None, None, :]
+    w = S.wavelet(S.WAVELET_RIC, args.case_nt, dt, 15.0, 40)
+    r = np.arange(pml, n - pml, dtype=np.int32)
+    shots = [S.ShotSpec(n // 2, pml + 5, r, np.full_like(r, pml + 2), w, sy=n // 2, rec_y=r)
+             for _ in range(args.case_nshot)]
+    with S.Engine(S.ACOUSTIC_3D, n, n, d, d, dt, pml, order=8, ny=n, dy=d) as e:
+        e.set_model((vp * 1.02).astype(np.float32))
+        e.set_shots(shots)
+        obs = e.forward()
+        e.set_model(vp)
+        e.gradient(obs)
+        e.gradient(obs)
+        return e.timing()
+
+
+def case_vti(args):
+    """The VTI modeller on the shipped .par geometry (workloads.vti_card), nshot shots, nt samples."""
+    from seismic_code_github_b200 import seisfd as S
+    from seismic_code_github_b200 import workloads as W
+    c = W.vti_card(nshot=args.case_nshot, nt=args.case_nt)
+    _, t = S.vti_forward(c["vz"], c["eps"], c["delta"], c["dx"], c["dz"], c["dt"], c["f0"], c["nt"], c["bounds"],
+                         c["shots"])
+    return t
+
+CASES = {"acoustic3d": case_acoustic3d, "viscoac": case_viscoac, "gradient": case_gradient, "forward2d": case_forward2d,
+         "qgradient": case_qgradient, "gradient3d": case_gradient3d, "viscoel": case_viscoel, "elastic": case_elastic,
+         "vti": case_vti}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -813,7 +979,15 @@ def main():
     ap.add_argument("--qg-plain-shots", type=int, default=0, help="plain per-shot gradient shots (0 = all)")
     ap.add_argument("--d3g-nshot", type=int, default=4, help="3-D gradient shots (0 = skip)")
     ap.add_argument("--d3g-nt-scale", type=float, default=0.05)
+    ap.add_argument("--case", choices=sorted(CASES), help="run one small case for a profiler capture and print "
+                    "its timing record (no benchmark line)")
+    ap.add_argument("--case-n", type=int, default=384, help="--case: 3-D padded grid size per axis")
+    ap.add_argument("--case-nshot", type=int, default=2)
+    ap.add_argument("--case-nt", type=int, default=3)
     args = ap.parse_args()
+    if args.case:
+        print(json.dumps(CASES[args.case](args)))
+        return 0
     world, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)

@@ -202,6 +202,13 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out);
  * counterpart (the reference has no adjoint). */
 int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);
 
+/* sfd_gradient with every buffer in the caller's device memory (zero-copy for torch and for a
+ * device-side all-reduce of per-rank gradients): obs_dev (sfd_forward layout), misfit_dev (one
+ * float), grad_vp_dev and grad_invq_dev (padded model grid; either may be NULL).  The results
+ * equal sfd_gradient's bit for bit.  Pointers must be on the context's device. */
+int sfd_gradient_device(sfd_ctx* ctx, const float* obs_dev, float* misfit_dev, float* grad_vp_dev,
+                        float* grad_invq_dev);
+
 /* Same gradient with the plain per-shot schedule: shots one after another, one kernel launch
  * per time step, no graph -- the baseline the batched gradient is measured against. */
 int sfd_gradient_per_shot(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq);

@@ -156,6 +156,7 @@ struct sfd_ctx {
     double* d_misfit = nullptr;
     double* d_grad = nullptr;   // gradient on the model grid (double)
     double* d_grad2 = nullptr;  // viscoacoustic: d misfit / d (1/Q) on the model grid
+    GradSrc* d_gsrc = nullptr;  // per shot: source cell and -dt DEN there (device-output gradient)
     int* d_apx0 = nullptr;      // viscoacoustic: each shot's aperture start in the model
     // 3-D gradient (shot groups of g3_G slabs, checkpoint levels g3_C1 / g3_C2)
     int state_slabs = 0;        // shot slabs per field held by d_state (3-D)
@@ -277,7 +278,7 @@ void free_shot_buffers(sfd_ctx* c) {
     c->graph_valid = false;
     dfree(c->d_ckpt); dfree(c->d_div); dfree(c->d_adj); dfree(c->d_gseg); dfree(c->d_gacc);
     dfree(c->d_obs_nt); dfree(c->d_obs_tn); dfree(c->d_res); dfree(c->d_lam); dfree(c->d_misfit);
-    dfree(c->d_grad); dfree(c->d_grad2); dfree(c->d_apx0);
+    dfree(c->d_grad); dfree(c->d_grad2); dfree(c->d_apx0); dfree(c->d_gsrc);
     dfree(c->g3_adj); dfree(c->g3_div); dfree(c->g3_ck1); dfree(c->g3_ck2); dfree(c->g3_gseg); dfree(c->g3_gacc);
     c->g3_G = c->g3_C1 = c->g3_C2 = c->g3_n1 = c->g3_n2 = 0;
     c->state_slabs = 0;
@@ -306,7 +307,7 @@ sfd_ctx::~sfd_ctx() {
 namespace {
 int alloc_state_3d(sfd_ctx* ctx, int nslab);
 int full_state_3d(sfd_ctx* ctx);
-int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched);
+int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched, bool dev);
 }  // namespace
 
 namespace {
@@ -1148,14 +1149,45 @@ int enqueue_gradient(sfd_ctx* ctx, bool batched, long long* launches) {
     return SFD_OK;
 }
 
-int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq, bool batched) {
+// Outputs to the caller's device memory: misfit (one float), grad_vp and grad_invq (model grid
+// floats), converted from the double sums on the device, with the source term of d misfit / d vp
+// added there in the host path's order (the results equal sfd_gradient's bit for bit).
+int finish_gradient_device(sfd_ctx* ctx, float* misfit, float* grad_vp, float* grad_invq, bool source_term) {
+    const bool is3d = ctx->g.scheme == SFD_ACOUSTIC_3D;
+    const long long nm = (long long)ctx->g.nx * (is3d ? ctx->g.ny : 1) * ctx->g.nz;
+    if (grad_vp && source_term) {
+        std::vector<GradSrc> src(ctx->nshot);
+        for (int s = 0; s < ctx->nshot; s++) {
+            const ShotDev& sd = ctx->h_shots[s];
+            const size_t mi = is3d ? ((size_t)sd.sx * ctx->g.ny + sd.sy) * ctx->g.nz + sd.sz
+                                   : (size_t)(sd.x0 + sd.sx) * ctx->g.nz + sd.sz;
+            const double den = ctx->varden ? ctx->h_den[mi] : ctx->den_c;
+            src[s].mi = (long long)mi;
+            src[s].scale = -(double)ctx->g.dt * den;
+        }
+        if (!ctx->d_gsrc) CK(cudaMalloc(&ctx->d_gsrc, sizeof(GradSrc) * ctx->nshot));
+        CK(cudaMemcpyAsync(ctx->d_gsrc, src.data(), sizeof(GradSrc) * src.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(launch_grad_source(ctx->d_grad, ctx->d_gsrc, ctx->d_shots, ctx->nshot, ctx->d_lam, ctx->nt_max, ctx->d_wav,
+                              ctx->stream));
+    }
+    if (grad_vp) CK(launch_to_float(ctx->d_grad, grad_vp, nm, ctx->stream));
+    if (grad_invq) CK(launch_to_float(ctx->d_grad2, grad_invq, nm, ctx->stream));
+    if (misfit) CK(launch_to_float(ctx->d_misfit, misfit, 1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->timing.h2d_bytes = 0;
+    ctx->timing.d2h_bytes = 0;
+    return SFD_OK;
+}
+
+int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq, bool batched,
+                 bool dev = false) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (!obs) return set_err(ctx, SFD_ERR_ARG, "observed records are required");
     const bool visco = ctx->g.scheme == SFD_VISCOAC_2D;
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) {
         if (grad_invq) return set_err(ctx, SFD_ERR_ARG, "grad_invq applies to the viscoacoustic scheme only");
-        return run_gradient_3d(ctx, obs, misfit, grad_vp, batched);
+        return run_gradient_3d(ctx, obs, misfit, grad_vp, batched, dev);
     }
     if (ctx->g.scheme != SFD_ACOUSTIC_2D && !visco)
         return set_err(ctx, SFD_ERR_UNSUPPORTED, "scheme %d has no gradient", ctx->g.scheme);
@@ -1163,7 +1195,8 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     auto t0 = std::chrono::steady_clock::now();
     if ((rc = grad_alloc(ctx))) return rc;
     if (!ctx->graph_valid && (rc = tune_schedule(ctx))) return rc;
-    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total,
+                       dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     long long launches = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (batched) {
@@ -1206,6 +1239,12 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     const int kkeep = ctx->grad_keep * ctx->grad_C;
     for (const auto& s : ctx->h_shots) pts += (double)s.nx * ctx->g.nz * (2.0 * s.nt + std::min(s.nt, kkeep));
     ctx->timing.point_updates = pts;
+    if (dev) {
+        ctx->have_grad = true;
+        rc = finish_gradient_device(ctx, misfit, grad_vp, grad_invq, !visco);
+        ctx->timing.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
     double mis = 0;
     CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
     if (misfit) *misfit = (float)mis;
@@ -1786,13 +1825,14 @@ int g3_group(sfd_ctx* ctx, const int* slots, const std::vector<int>& h_slots, lo
     return SFD_OK;
 }
 
-int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched) {
+int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, bool batched, bool dev) {
     int rc;
     auto t0 = std::chrono::steady_clock::now();
     Plan3 p;
     if ((rc = plan3_choose(ctx, batched ? ctx->nshot : 1, &p))) return rc;
     if ((rc = g3_alloc(ctx, p))) return rc;
-    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_obs_nt, obs, sizeof(float) * ctx->rec_total,
+                       dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     long long launches = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
@@ -1826,6 +1866,10 @@ int run_gradient_3d(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_v
     double pts = 0;
     for (const auto& sd : ctx->h_shots) pts += (double)sd.nx * ctx->g.ny * ctx->g.nz * sd.nt;
     ctx->timing.point_updates = (p.C2 < p.C1 ? 4.0 : 3.0) * pts;  // forward, recomputation(s), adjoint
+    if (dev) {
+        ctx->have_grad = true;
+        return finish_gradient_device(ctx, misfit, grad_vp, nullptr, true);
+    }
     double mis = 0;
     CK(cudaMemcpy(&mis, ctx->d_misfit, sizeof(double), cudaMemcpyDeviceToHost));
     if (misfit) *misfit = (float)mis;
@@ -2510,6 +2554,11 @@ int sfd_test_wait_timeout(sfd_ctx* ctx, int cta, int step, double limit_s) {
 
 int sfd_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq) {
     return run_gradient(ctx, obs, misfit, grad_vp, grad_invq, true);
+}
+
+int sfd_gradient_device(sfd_ctx* ctx, const float* obs_dev, float* misfit_dev, float* grad_vp_dev,
+                        float* grad_invq_dev) {
+    return run_gradient(ctx, obs_dev, misfit_dev, grad_vp_dev, grad_invq_dev, true, true);
 }
 
 int sfd_gradient_per_shot(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, float* grad_invq) {

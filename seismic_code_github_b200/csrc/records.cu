@@ -37,7 +37,42 @@ __global__ void nan_scan_kernel(const float* __restrict__ v, long long n, int* f
         }
 }
 
+// d misfit / d vp at the source cells: the source term P[src] -= (dt DEN Vp) w[k] gives
+// -dt DEN sum_k lambda_k w[k].  One thread, shots and samples in order, double precision with
+// explicitly rounded operations: the same sums, in the same order, as the host path of
+// sfd_gradient, so both give the same bits.
+__global__ void grad_source_kernel(double* grad, const GradSrc* src, const ShotDev* shots, int nshot, const float* lam,
+                                   int nt_max, const float* wav) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int s = 0; s < nshot; s++) {
+        const ShotDev sd = shots[s];
+        double sw = 0.0;
+        for (int j = 0; j < sd.nt; j++)
+            sw = __dadd_rn(sw, __dmul_rn((double)lam[(long long)s * nt_max + j], (double)wav[sd.wav_off + j]));
+        grad[src[s].mi] = __dadd_rn(grad[src[s].mi], __dmul_rn(src[s].scale, sw));
+    }
+}
+
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = __double2float_rn(in[i]);
+}
+
 }  // namespace
+
+cudaError_t launch_grad_source(double* grad, const GradSrc* src, const ShotDev* shots, int nshot, const float* lam,
+                               int nt_max, const float* wav, cudaStream_t st) {
+    if (nshot <= 0) return cudaSuccess;
+    grad_source_kernel<<<1, 32, 0, st>>>(grad, src, shots, nshot, lam, nt_max, wav);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_float(const double* in, float* out, long long n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    to_float_kernel<<<blocks, 256, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const ShotDev* shots, int nshot,
                                      int nrec_max, int nt_max, cudaStream_t st) {

@@ -340,6 +340,16 @@ cudaError_t acoustic2d_launch_inject0(const Acou2DArgs& a, int nshot, bool exact
 cudaError_t launch_records_transpose(const float* rec_tn, float* rec_nt, const ShotDev* shots, int nshot,
                                      int nrec_max, int nt_max, cudaStream_t st);
 cudaError_t launch_nan_scan(const float* rec, long long n, int* flag, cudaStream_t st);
+// source cell of one shot for the gradient's source term: model index and -(dt) * DEN there
+struct GradSrc {
+    long long mi;
+    double scale;
+};
+// grad[mi_s] += scale_s * sum_k lam[s][k] w_s[k] for every shot, in shot and sample order
+cudaError_t launch_grad_source(double* grad, const GradSrc* src, const ShotDev* shots, int nshot, const float* lam,
+                               int nt_max, const float* wav, cudaStream_t st);
+// out[i] = (float) in[i]
+cudaError_t launch_to_float(const double* in, float* out, long long n, cudaStream_t st);
 
 // ---- wavefield snapshots (snapshots.cu) ----
 struct SnapArgs {

@@ -144,6 +144,8 @@ SIGNATURES = {
     "sfd_get_wavefield": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _F32P]),
     "sfd_gradient": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
     "sfd_gradient_per_shot": (ctypes.c_int, [ctypes.c_void_p, _F32P, _F32P, _F32P, _F32P]),
+    "sfd_gradient_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
     "sfd_get_wavelet_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F32P]),
     "sfd_set_checkpoint_interval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sfd_test_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
@@ -418,6 +420,13 @@ class Engine:
         self._check(fn(self._h, _fp(obs), _fp(mis), _fp(g), _fp(gq)), "sfd_gradient")
         shape = (self.grid.nx, self.grid.nz) if self.grid.ny == 1 else (self.grid.nx, self.grid.ny, self.grid.nz)
         return float(mis[0]), g.reshape(shape), (None if gq is None else gq.reshape(shape))
+
+    def gradient_device(self, obs_dev: int, misfit_dev: int, grad_vp_dev: int, grad_invq_dev: Optional[int] = None):
+        """sfd_gradient_device: every argument is a device address on this engine's device (for
+        torch tensors, tensor.data_ptr()): obs in the record layout of forward(), misfit one
+        float32, grad_vp / grad_invq the model grid in float32."""
+        self._check(self._lib.sfd_gradient_device(self._h, obs_dev, misfit_dev, grad_vp_dev, grad_invq_dev),
+                    "sfd_gradient_device")
 
     def wavelet_gradient(self, shot: int) -> np.ndarray:
         out = np.empty(self._shots[shot].nt, np.float32)

@@ -83,6 +83,32 @@ def _rank(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+def rank_payload(rank):
+    """A rank's partial misfit and gradient for the tensor all-reduce test (seeded per rank)."""
+    rng = np.random.default_rng(100 + rank)
+    return float(rng.random()), rng.standard_normal((44, 36)).astype(np.float32)
+
+
+def _rank_tensors(rank, world, port, out_dir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        J, g = rank_payload(rank)
+        mis = torch.tensor([J], dtype=torch.float32)
+        gv = torch.from_numpy(g.copy())
+        gq = torch.from_numpy(2.0 * g)
+        out = SH.allreduce_gradient_tensors(mis, gv, gq)
+        assert out[1] is gv  # reduced in place
+        np.save(os.path.join(out_dir, f"t{rank}.npy"), np.stack([gv.numpy(), gq.numpy()]))
+        np.save(os.path.join(out_dir, f"m{rank}.npy"), mis.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
 def free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -99,3 +125,17 @@ def test_gradient_allreduce_two_gloo_ranks(tmp_path):
         Jr = float(np.load(tmp_path / f"J{r}.npy")[0])
         assert abs(Jr - J) <= 1e-12 * J
         assert rel_l2(gr, g) <= 1e-6
+
+
+def test_tensor_allreduce_two_gloo_ranks(tmp_path):
+    """The in-place tensor form used on GPUs (sharding.allreduce_gradient_tensors, which NCCL runs
+    on device tensors) with CPU tensors over gloo: every rank ends with the sums."""
+    world = 2
+    mp.spawn(_rank_tensors, args=(world, free_port(), str(tmp_path)), nprocs=world, join=True)
+    parts = [rank_payload(r) for r in range(world)]
+    J = sum(p[0] for p in parts)
+    g = sum(p[1].astype(np.float64) for p in parts)
+    for r in range(world):
+        t = np.load(tmp_path / f"t{r}.npy")
+        assert rel_l2(t[0], g) <= 1e-6 and rel_l2(t[1], 2.0 * g) <= 1e-6
+        assert abs(float(np.load(tmp_path / f"m{r}.npy")[0]) - J) <= 1e-6 * J
