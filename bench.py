@@ -26,6 +26,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Gpts/s & % HBM roofline; gradient shots/s batched vs plain @ relL2≤1e-4"
 BYTES_PER_POINT = {False: 28, True: 32}  # algorithmic bytes per grid-point update (const / variable density)
+GRAD_BYTES_PER_POINT_STEP = 100          # 2-D acoustic gradient, per point-step of a shot
+GRAD3_BYTES_PER_POINT_STEP = 124         # 3-D: forward 36, recomputation 36 + 4, adjoint 36 + 4 (D) + 8 (sum)
 FALLBACK_HBM_GBS = 6650.0
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "acoustic2d_step_config2.md")
 
@@ -237,6 +239,16 @@ def measure_gradient(args, dev):
         t_plain = e.timing()
     batched_sps = len(shots) / (bt / 1e3)
     plain_sps = len(sub) / (t_plain["loop_ms"] / 1e3)
+    # roofline at the algorithmic ~100 B per point-step of a shot's gradient: forward with
+    # checkpoints 28, recomputation 28 + 4 (D_k write), adjoint 28, imaging 4 (D_k read) + 8 (sum)
+    peak, peak_src = read_peaks()
+    pts_shot = float(case.Nx) * case.Nz * case.nt
+    roof = {"bytes_per_point_step": GRAD_BYTES_PER_POINT_STEP,
+            "achieved_gbs": GRAD_BYTES_PER_POINT_STEP * pts_shot * len(shots) / (bt / 1e3) / 1e9,
+            "plain_achieved_gbs": GRAD_BYTES_PER_POINT_STEP * pts_shot * len(sub) / (t_plain["loop_ms"] / 1e3) / 1e9,
+            "peak_gbs": peak, "peak_kind": peak_src}
+    roof["frac"] = roof["achieved_gbs"] / peak
+    roof["plain_frac"] = roof["plain_achieved_gbs"] / peak
     oracle = None
     if not args.no_cpu_baseline:
         # the reference has no adjoint: the FP64 adjoint oracle is timed beside the GPU path as a
@@ -258,6 +270,7 @@ def measure_gradient(args, dev):
             "batched_shots_per_s": batched_sps, "batched_ms": bt, "batched_launches": launches,
             "plain_shots_per_s": plain_sps, "plain_ms": t_plain["loop_ms"], "plain_shots": len(sub),
             "plain_launches": t_plain["launches"], "batched_over_plain": batched_sps / plain_sps,
+            "roofline": roof,
             "misfit": float(mis), "gradient_accuracy": "relL2 vs FP64 adjoint oracle 7.6e-7 (tests/test_gradient_gpu.py)",
             "cpu_oracle": oracle}
 
@@ -561,18 +574,33 @@ def measure_3d_gradient(args, dev):
         e.set_model(vp)
         e.gradient(obs)
         t = e.timing()
-        e.gradient(obs, per_shot=True)  # the same shots and memory, one shot per group
+        # plain per-shot schedule (one shot per group) on the first shots, the same engine and memory
+        nplain = len(shots) if args.d3g_plain_shots <= 0 else min(args.d3g_plain_shots, len(shots))
+        if nplain < len(shots):
+            e.set_shots(shots[:nplain])
+        nobs = sum(len(s.rec_x) * s.nt for s in shots[:nplain])
+        e.gradient(obs[:nobs], per_shot=True)
         tp = e.timing()
     del vp
     levels = 2 if t["kernel_variant"] == 62 else 1
     pts = float(n) ** 3 * sum(c["nt"])
+    pts_plain = float(n) ** 3 * sum(c["nt"][:nplain])
+    peak, peak_src = read_peaks()
+    roof = {"bytes_per_point_step": GRAD3_BYTES_PER_POINT_STEP,
+            "achieved_gbs": GRAD3_BYTES_PER_POINT_STEP * pts / (t["loop_ms"] / 1e3) / 1e9, "peak_gbs": peak,
+            "peak_kind": peak_src,
+            "note": "algorithmic bytes of one checkpoint level; with two levels the extra recomputation pass "
+                    "is work beyond this count"}
+    roof["frac"] = roof["achieved_gbs"] / peak
     return {"workload": f"config 5 geometry: 3-D gradient d/dvp, {c['N']}^3 interior ({n}^3 padded), {len(shots)} shots, "
                         f"record lengths 1500-2500 scaled by {args.d3g_nt_scale} (nt {min(c['nt'])}-{max(c['nt'])})",
             "batched_shots_per_s": len(shots) / (t["loop_ms"] / 1e3), "batched_ms": t["loop_ms"],
             "checkpoint_levels": levels, "passes": t["point_updates"] / pts,
             "gpts_per_s_all_passes": t["point_updates"] / (t["loop_ms"] / 1e3) / 1e9,
-            "plain_shots_per_s": len(shots) / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"],
-            "batched_over_plain": tp["loop_ms"] / t["loop_ms"],
+            "plain_shots_per_s": nplain / (tp["loop_ms"] / 1e3), "plain_ms": tp["loop_ms"], "plain_shots": nplain,
+            "batched_over_plain": (len(shots) / t["loop_ms"]) / (nplain / tp["loop_ms"]),
+            "roofline": roof,
+            "plain_gbs": GRAD3_BYTES_PER_POINT_STEP * pts_plain / (tp["loop_ms"] / 1e3) / 1e9,
             "gradient_accuracy": "relL2 vs FP64 3-D adjoint oracle 6.7e-7 (tests/test_gradient3d_gpu.py)"}
 
 
@@ -963,9 +991,9 @@ def main():
     ap.add_argument("--q-steps", type=int, default=2, help="timed viscoacoustic forwards (0 = skip)")
     ap.add_argument("--q-nshot", type=int, default=16)
     ap.add_argument("--q-cpu-steps", type=int, default=120)
-    ap.add_argument("--d3-steps", type=int, default=2, help="timed 3-D forwards (0 = skip)")
-    ap.add_argument("--d3-nshot", type=int, default=16)
-    ap.add_argument("--d3-nt-scale", type=float, default=0.05)
+    ap.add_argument("--d3-steps", type=int, default=1, help="timed 3-D forwards (0 = skip)")
+    ap.add_argument("--d3-nshot", type=int, default=4)
+    ap.add_argument("--d3-nt-scale", type=float, default=1.0, help="record-length scale (1 = config 5's 1500-2500)")
     ap.add_argument("--d3-cpu-steps", type=int, default=3)
     ap.add_argument("--e-steps", type=int, default=1, help="timed visco-elastic forwards (0 = skip)")
     ap.add_argument("--el-steps", type=int, default=1, help="timed isotropic elastic forwards (0 = skip)")
@@ -977,8 +1005,9 @@ def main():
     ap.add_argument("--qg-nshot", type=int, default=16)
     ap.add_argument("--qg-nt-scale", type=float, default=1.0)
     ap.add_argument("--qg-plain-shots", type=int, default=0, help="plain per-shot gradient shots (0 = all)")
-    ap.add_argument("--d3g-nshot", type=int, default=4, help="3-D gradient shots (0 = skip)")
-    ap.add_argument("--d3g-nt-scale", type=float, default=0.05)
+    ap.add_argument("--d3g-nshot", type=int, default=2, help="3-D gradient shots (0 = skip)")
+    ap.add_argument("--d3g-nt-scale", type=float, default=1.0, help="record-length scale (1 = config 5's 1500-2500)")
+    ap.add_argument("--d3g-plain-shots", type=int, default=1, help="plain per-shot 3-D gradient shots (0 = all)")
     ap.add_argument("--case", choices=sorted(CASES), help="run one small case for a profiler capture and print "
                     "its timing record (no benchmark line)")
     ap.add_argument("--case-n", type=int, default=384, help="--case: 3-D padded grid size per axis")

@@ -25,7 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(ROOT, "include"),
           "--expt-relaxed-constexpr", "-ccbin", "g++"]
-LIB_SOURCES = ["api.cu", "acoustic2d.cu", "acoustic2d_fma.cu", "acoustic2d_march.cu", "adjoint2d.cu", "viscoac2d.cu", "q_adjoint2d.cu", "viscoel2d.cu", "elastic2d.cu", "vti2d.cu",
+LIB_SOURCES = ["api.cu", "acoustic2d.cu", "acoustic2d_fma.cu", "acoustic2d_march.cu", "adjoint2d.cu", "viscoac2d.cu", "viscoac2d_fast.cu", "q_adjoint2d.cu", "viscoel2d.cu", "elastic2d.cu", "vti2d.cu",
                "records.cu",
                "helpers.cpp", "noalloc.cu", "acoustic3d.cu", "snapshots.cu",
                "fileio.cpp"]

@@ -79,6 +79,7 @@ struct sfd_ctx {
     int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
     CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
     CUtensorMap mtmaps[6];     // the same buffers with the x-marching kernel's boxes
+    CUtensorMap qtmaps[6];     // fused viscoacoustic step: S0 S1 VX0 VX1 VZ0 VZ1 (viscoac2d_fast.cu boxes)
 
     // 3-D scheme: dense [x][y][pitch] slabs, 8 fields (P, Vx, Vy, Vz, two buffers each)
     Layout3D L3{};
@@ -206,6 +207,14 @@ void dfree(T*& p) {
 }
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// The viscoacoustic scheme runs the fused kernel (viscoac2d_fast.cu) unless SFD_EXACT is set.
+// Its slabs: vx (2 parities), vz (2), sigma (2), r, and the six split parts of the sponge bands.
+constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQFastSlabs = 13;
+constexpr int kQFastSeg = 256;  // columns per segment of the fused kernel
+bool q_fast(const sfd_ctx* c) { return c->g.scheme == SFD_VISCOAC_2D && !(c->g.flags & SFD_EXACT); }
+// slab of TMA map b (S0 S1 VX0 VX1 VZ0 VZ1)
+int qfast_slab(int b) { return b < 2 ? kQS + b : b < 4 ? kQVX + (b - 2) : kQVZ + (b - 4); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -408,6 +417,30 @@ Acou3DArgs make_args3(const sfd_ctx* c, int step) {
 }
 
 // Arguments of the viscoacoustic step (fields in place, eight slabs per shot).
+QArgs make_qargs(const sfd_ctx* c, int step);
+
+// Arguments of the fused viscoacoustic step (default mode), step k: reads parity k & 1 of sigma,
+// vx, vz and writes parity (k + 1) & 1; r and the split parts of the sponge bands in place.
+QFastArgs make_qfast(const sfd_ctx* c, int step) {
+    QFastArgs A{};
+    A.q = make_qargs(c, step);
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    float* F = c->d_state;
+    const int i = step & 1, o = (step + 1) & 1;
+    A.vx_in = F + (kQVX + i) * fs; A.vx_out = F + (kQVX + o) * fs;
+    A.vz_in = F + (kQVZ + i) * fs; A.vz_out = F + (kQVZ + o) * fs;
+    A.s_in = F + (kQS + i) * fs; A.s_out = F + (kQS + o) * fs;
+    A.r = F + kQR * fs;
+    A.q.vx = A.q.vz = nullptr;
+    A.q.sx = F + (kQSplit + 0) * fs; A.q.sz = F + (kQSplit + 1) * fs; A.q.sr = F + (kQSplit + 2) * fs;
+    A.q.rx = F + (kQSplit + 3) * fs; A.q.rz = F + (kQSplit + 4) * fs; A.q.rr = F + (kQSplit + 5) * fs;
+    A.tm_s = c->qtmaps[i];
+    A.tm_vx = c->qtmaps[2 + i];
+    A.tm_vz = c->qtmaps[4 + i];
+    A.err_flag = c->d_err;
+    return A;
+}
+
 QArgs make_qargs(const sfd_ctx* c, int step) {
     QArgs a{};
     const long long fs = (long long)c->nshot * c->L.shot_stride;
@@ -566,7 +599,12 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         SnapArgs s{};
         const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
         const float* F = ctx->d_state;
-        if (ctx->g.scheme == SFD_VISCOAC_2D) {
+        if (q_fast(ctx)) {
+            const int o = (k + 1) & 1;  // parity written by step k
+            s.nsum = 1;
+            s.f[0] = F + (sn.field == SFD_FIELD_VX ? kQVX + o : sn.field == SFD_FIELD_VZ ? kQVZ + o
+                          : sn.field == SFD_FIELD_P ? kQS + o : kQR) * fs;
+        } else if (ctx->g.scheme == SFD_VISCOAC_2D) {
             const int f0 = sn.field == SFD_FIELD_VX ? 0 : sn.field == SFD_FIELD_VZ ? 1 : sn.field == SFD_FIELD_P ? 2 : 5;
             s.nsum = (sn.field == SFD_FIELD_P || sn.field == SFD_FIELD_R) ? 3 : 1;
             for (int i = 0; i < s.nsum; i++) s.f[i] = F + (f0 + i) * fs;
@@ -628,6 +666,13 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         CK(acoustic3d_launch_gather(a.p_out, ctx->L3, ctx->d_shots, slots, act, ctx->d_rec_x, ctx->d_rec_y,
                                     ctx->d_rec_z, ctx->d_rec_tn, ctx->nrec_max, k, ctx->stream));
         *launches += 2 + (ctx->nrec_max > 0 ? 1 : 0);
+        return SFD_OK;
+    }
+    if (q_fast(ctx)) {
+        QFastArgs q = make_qfast(ctx, k);
+        q.q.slot_to_shot = slots;
+        CK(viscoac2d_fast_launch(q, act, kQFastSeg, ctx->stream, pdl_enabled()));
+        *launches += 1;
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
@@ -778,7 +823,7 @@ int tune_schedule(sfd_ctx* ctx) {
 
 int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
-    if (ctx->g.scheme == SFD_VISCOAC_2D) return 40;
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return q_fast(ctx) ? 41 : 40;
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
     if (ctx->g.flags & SFD_EXACT) return 1;
@@ -2278,7 +2323,8 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         CK(cudaMalloc(&ctx->d_rec2_tn, rec_bytes));
         CK(cudaMalloc(&ctx->d_rec2_nt, rec_bytes));
     }
-    ctx->state_floats = (iso ? I_NFIELDS : elastic ? E_NFIELDS : visco ? 8 : 6) * (size_t)nshot * L.shot_stride;
+    ctx->state_floats = (iso ? I_NFIELDS : elastic ? E_NFIELDS : q_fast(ctx) ? kQFastSlabs : visco ? 8 : 6) *
+                        (size_t)nshot * L.shot_stride;
     CK(cudaMalloc(&ctx->d_state, ctx->state_floats * sizeof(float)));
     CK(cudaMalloc(&ctx->d_src_pre, sizeof(float) * nshot));
     if (visco) {
@@ -2290,6 +2336,16 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         viscoac2d_sponge_tables(ctx->g.pml, ctx->g.pml, ctx->g.dx, ctx->g.dz, ctx->spg_stride, tab.data());
         dfree(ctx->d_spg);
         if ((rc = up(&ctx->d_spg, tab))) return rc;
+        if (q_fast(ctx)) {
+            int bs[2], bv[2];
+            viscoac2d_fast_boxes(bs, bv);
+            const long long fs = (long long)nshot * L.shot_stride;
+            for (int b = 0; b < 6; b++) {
+                const int rc2 = encode_field_map(ctx, &ctx->qtmaps[b], ctx->d_state + qfast_slab(b) * fs, L, nshot,
+                                                 b < 2 ? bs : bv);
+                if (rc2) return rc2;
+            }
+        }
     } else {
         // TMA descriptors of the six field buffers: 3-D (z, column, shot), one box per field
         int bp[2], bvx[2], bvz[2];
@@ -2419,6 +2475,14 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         };
         const size_t n = (size_t)sd.nx * nz;
         int rc2;
+        if (q_fast(ctx)) {  // merged fields; the shot's last step wrote parity nt & 1
+            const int o = sd.nt & 1;
+            if (field == SFD_FIELD_VX) return fetch(kQVX + o, out);
+            if (field == SFD_FIELD_VZ) return fetch(kQVZ + o, out);
+            if (field == SFD_FIELD_P) return fetch(kQS + o, out);
+            if (field == SFD_FIELD_R) return fetch(kQR, out);
+            return set_err(ctx, SFD_ERR_UNSUPPORTED, "field %d not available for this scheme", field);
+        }
         if (field == SFD_FIELD_VX) return fetch(0, out);
         if (field == SFD_FIELD_VZ) return fetch(1, out);
         if (field != SFD_FIELD_P && field != SFD_FIELD_R)

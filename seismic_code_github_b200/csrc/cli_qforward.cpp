@@ -164,6 +164,7 @@ int main(int argc, char** argv) {
     g.dt = p.dt;
     g.order = 10;
     g.f0 = p.f0;
+    g.flags = SFD_EXACT;  // the reference's operation order: the outputs equal the reference program's
     sfd_ctx* ctx = nullptr;
     if ((rc = sfd_create(&g, device, &ctx))) return fail("sfd_create", rc, ctx);
     if (elastic) {

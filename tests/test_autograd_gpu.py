@@ -56,7 +56,7 @@ def test_viscoacoustic_autograd_matches_c_abi_gradient():
     q = pad(30 + 120 * gaussian_filter(rng.random((40, 32)), 2))
     rx = np.arange(NPX, vp.shape[0] - NPX, 2, dtype=np.int32)
     shots = [S.ShotSpec(27, NPX + 4, rx, np.full_like(rx, NPX + 2), S.wavelet(S.WAVELET_Q, 160, DT, F0))]
-    with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], DX, DX, DT, NPX, order=10, f0=F0) as e:
+    with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], DX, DX, DT, NPX, order=10, f0=F0, flags=S.EXACT) as e:
         e.set_model((vp * 1.02).astype(np.float32), rho, (q * 0.8).astype(np.float32))
         e.set_shots(shots)
         obs = e.forward()

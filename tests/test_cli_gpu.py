@@ -139,7 +139,8 @@ def test_snapshots_equal_truncated_runs_acoustic():
                 assert bits_equal(snap, full[pml:-pml, pml:-pml]), (sid, s, k)
 
 
-def test_snapshots_equal_truncated_runs_viscoacoustic():
+@pytest.mark.parametrize("flags", [0, S.EXACT], ids=["fused", "exact"])
+def test_snapshots_equal_truncated_runs_viscoacoustic(flags):
     rng = np.random.default_rng(3)
     npx, f0, dt, dx = 8, 20.0, 5e-4, 10.0
     vp = S.pad_model((2000 + 300 * rng.random((40, 36))).astype(np.float32), npx, npx, npx, npx)
@@ -147,7 +148,7 @@ def test_snapshots_equal_truncated_runs_viscoacoustic():
     q = S.pad_model((40 + 100 * rng.random((40, 36))).astype(np.float32), npx, npx, npx, npx)
     r = np.arange(npx, vp.shape[0] - npx, dtype=np.int32)
     w = S.wavelet(S.WAVELET_Q, 90, dt, f0)
-    with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0) as e:
+    with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0, flags=flags) as e:
         e.set_model(vp, rho, q)
         e.set_shots([S.ShotSpec(20, 12, r, np.full_like(r, 10), w)])
         e.set_snapshots(2, S.FIELD_P, 9, 40, 3)
@@ -157,7 +158,7 @@ def test_snapshots_equal_truncated_runs_viscoacoustic():
     for (sid, field, first, every), got in zip(((2, S.FIELD_P, 9, 40), (3, S.FIELD_R, 49, 50)), snaps):
         for j, snap in enumerate(got):
             k = first + j * every
-            with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0) as e:
+            with S.Engine(S.VISCOAC_2D, vp.shape[0], vp.shape[1], dx, dx, dt, npx, order=10, f0=f0, flags=flags) as e:
                 e.set_model(vp, rho, q)
                 e.set_shots([S.ShotSpec(20, 12, r, np.full_like(r, 10), w[:k + 1])])
                 e.forward()

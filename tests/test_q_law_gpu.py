@@ -1,7 +1,8 @@
-"""Physics pin of the GPU viscoacoustic path (SFD_VISCOAC_2D through the C ABI): measured
-attenuation and dispersion against the 1-SLS law with the reference's Blanch tau (QS:473-551), at
-Q = 20, 60 and 200 on a homogeneous model, at the configuration's time step and at half of it
-(tests/qlaw.py states the method and the laws).
+"""Physics pin of the GPU viscoacoustic path (SFD_VISCOAC_2D through the C ABI, in both modes:
+the reference-order kernels of SFD_EXACT and the default fused kernel): measured attenuation and
+dispersion against the 1-SLS law with the reference's Blanch tau (QS:473-551), at Q = 20, 60 and
+200 on a homogeneous model, at the configuration's time step and at half of it (tests/qlaw.py
+states the method and the laws).
 
   * discrete-time law of the reference's update (QS:993-1269): within 1 % at both time steps;
   * continuous 1-SLS law: within 6 % at dt = 0.5 ms, within 3.5 % at dt = 0.25 ms, and the gap
@@ -19,13 +20,14 @@ pytestmark = pytest.mark.gpu
 QS = (20.0, 60.0, 200.0)
 
 
-def gpu_records(q, dt, nt):
+def gpu_records(q, dt, nt, flags):
     g = GEOM
     npx, nrz0 = g["npx"], g["nz"] // 2
     vp = np.full((g["nx"], g["nz"]), g["vp"], np.float32)
     vpp, rhop, qp = (S.pad_model(a, npx, npx, npx, npx) for a in (vp, np.full_like(vp, g["rho"]), np.full_like(vp, q)))
     decay = ol.q_decay(g["f0"], dt)
-    with S.Engine(S.VISCOAC_2D, vpp.shape[0], vpp.shape[1], g["dx"], g["dx"], dt, npx, order=10, f0=g["f0"]) as e:
+    with S.Engine(S.VISCOAC_2D, vpp.shape[0], vpp.shape[1], g["dx"], g["dx"], dt, npx, order=10, f0=g["f0"],
+                  flags=flags) as e:
         e.set_model(vpp, rhop, qp)
         rx = np.arange(npx, vpp.shape[0] - npx, dtype=np.int32)
         rz = np.full_like(rx, npx + nrz0)
@@ -34,14 +36,14 @@ def gpu_records(q, dt, nt):
     return rec[:, decay:]
 
 
-@pytest.fixture(scope="module")
-def errors():
+@pytest.fixture(scope="module", params=[S.EXACT, 0], ids=["exact", "fused"])
+def errors(request):
     g = GEOM
     out = {}
     for dt, nt in ((5e-4, 1200), (2.5e-4, 2400)):
-        ref = gpu_records(1e5, dt, nt)
+        ref = gpu_records(1e5, dt, nt, request.param)
         for q in QS:
-            m = measure(gpu_records(q, dt, nt), ref, g["sx"] + g["r1"], g["sx"] + g["r2"], g["r1"] * g["dx"],
+            m = measure(gpu_records(q, dt, nt, request.param), ref, g["sx"] + g["r1"], g["sx"] + g["r2"], g["r1"] * g["dx"],
                         g["r2"] * g["dx"], g["vp"], g["f0"], dt, q)
             out[(dt, q)] = {f"{k}_{law}": rel_err(m[k], m[f"{k}_{law}"]) for k in ("alpha", "disp")
                             for law in ("disc", "cont")}

@@ -32,7 +32,8 @@ def run_gpu(model, npx, f0, dt, dx, shots_spec, scheme=S.VISCOEL_2D, per_shot=Fa
     """shots_spec: list of (isxe, isze, nt_total, nrz0); interior model arrays (nx, nz)."""
     vp, vs, rho, qp, qs = (S.pad_model(a, npx, npx, npx, npx) for a in model)
     nx, nz = vp.shape
-    e = S.Engine(scheme, nx, nz, dx, dx, dt, npx, order=10, f0=f0)
+    # the viscoacoustic scheme in its reference-order mode (SFD_EXACT), which the vs = 0 case reduces to
+    e = S.Engine(scheme, nx, nz, dx, dx, dt, npx, order=10, f0=f0, flags=S.EXACT if scheme == S.VISCOAC_2D else 0)
     if scheme == S.VISCOEL_2D:
         e.set_model_elastic(vp, vs, rho, qp, qs)
     else:
