@@ -116,3 +116,22 @@ def test_tile_numbering_gives_identical_bits(monkeypatch):
         out[m] = (rec, J, g)
     assert bits_equal(out[0][0], out[1][0])
     assert out[0][1] == out[1][1] and bits_equal(out[0][2], out[1][2])
+
+
+def test_second_device_in_the_same_process():
+    """The step kernels' shared-memory size attribute is set per device: a forward on device 0 and
+    then on device 1 of the same process both run (needs two visible GPUs)."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU visible")
+    case = W.small_varden()
+    w = S.wavelet(S.WAVELET_RIC, 80, case.dt, case.f0, 40)
+    rx, rz = case.receivers()
+    recs = []
+    for dev in (0, 1):
+        with S.Engine(S.ACOUSTIC_2D, case.Nx, case.Nz, case.dx, case.dz, case.dt, case.PML, order=16,
+                      device=dev) as e:
+            e.set_model(case.vp, case.den)
+            e.set_shots([S.ShotSpec(case.src_x[0], case.src_z[0], rx, rz, w)])
+            recs.append(e.forward().copy())
+    assert bits_equal(recs[0], recs[1])
