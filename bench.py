@@ -778,6 +778,9 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e_val, "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "launches_per_step": launches_per_call,
+        "kernel": {11: "FMA tile kernel, one tile per CTA", 12: "FMA tile kernel, persistent",
+                   13: "FMA x-marching kernel", 1: "reference-order kernel (SFD_EXACT)"}.get(t["kernel_variant"],
+                                                                                            str(t["kernel_variant"])),
         "clocks": clocks,
     }
     if plain is not None:

@@ -14,7 +14,9 @@
 //     an aligned register pair;
 //   * tiles whose working set is inside the sponge-free, fully updated interior skip the
 //     sponge and mask multiplies (a CTA-uniform branch).
-// Two CTAs share an SM, so one CTA's loads overlap the other's arithmetic.
+// Two CTAs share an SM, so one CTA's loads overlap the other's arithmetic.  The divergence
+// sx + sz is formed with scalar round-to-nearest adds (never fused with the products before
+// them), as in the x-marching kernel (acoustic2d_march.cu), so that the two give the same bits.
 //
 // The same kernel runs the adjoint step (ADJ = true; the recurrence is stated in adjoint2d.cu):
 // the P, Vx, Vz slots then hold the adjoint state nu = M K a Q (halo 2R), X and Z; phase A forms
@@ -428,10 +430,10 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
                 const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(a.dt));
                 const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
                 const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
-                const float2 bl = __fadd2_rn(__fadd2_rn(lo(sxo), dl),
-                                             make_float2(__fdividef(po.x, kl.x), __fdividef(po.y, kl.y)));
-                const float2 bh = __fadd2_rn(__fadd2_rn(hi(sxo), dh),
-                                             make_float2(__fdividef(po.z, kh.x), __fdividef(po.w, kh.y)));
+                const float2 bl = make_float2(__fadd_rn(__fadd_rn(sxo.x, dl.x), __fdividef(po.x, kl.x)),
+                                              __fadd_rn(__fadd_rn(sxo.y, dl.y), __fdividef(po.y, kl.y)));
+                const float2 bh = make_float2(__fadd_rn(__fadd_rn(sxo.z, dh.x), __fdividef(po.z, kh.x)),
+                                              __fadd_rn(__fadd_rn(sxo.w, dh.y), __fdividef(po.w, kh.y)));
                 float4 fa4 = make_float4(1.f, 1.f, 1.f, 1.f), fm4 = fa4;  // sponge a and mask M of the own cells
                 if (EDGE) {
                     const float ax = sAx[row + R], mx = sMx[row + R];
@@ -484,7 +486,8 @@ __device__ __forceinline__ void tile_body(const Acou2DArgs& a, float* smem, floa
             const float2 kh = mul2(mul2(mul2(hi(dn4), hi(vp4)), hi(vp4)), bc(-a.dt));
             const float2 dl = make_float2(cmp2(sz[0], h), cmp2(sz[1], h));
             const float2 dh = make_float2(cmp2(sz[2], h), cmp2(sz[3], h));
-            const float2 divl = __fadd2_rn(lo(sxo), dl), divh = __fadd2_rn(hi(sxo), dh);
+            const float2 divl = make_float2(__fadd_rn(sxo.x, dl.x), __fadd_rn(sxo.y, dl.y));
+            const float2 divh = make_float2(__fadd_rn(sxo.z, dh.x), __fadd_rn(sxo.w, dh.y));
             float2 pl = fma2(kl, divl, lo(po));
             float2 ph = fma2(kh, divh, hi(po));
             if (a.div_out != nullptr && gx < nx && gz < nz) {  // recomputation for the adjoint

@@ -16,7 +16,14 @@
 // phase C1 (rdx S-x Vx into a scratch block of shared memory), phase C2 (rdz S-z Vz, the P
 // update, sponge, source injection and all global stores), then the receivers.  Stencil sums
 // use paired FP32 instructions (FFMA2) over neighbouring z; in the z-stencils every other tap's
-// operand pair straddles an 8-byte boundary and is assembled from the aligned window.
+// operand pair straddles an 8-byte boundary and is assembled from the aligned window.  The
+// divergence sx + sz is formed with scalar round-to-nearest adds, which the compiler never fuses
+// with the products before them (a paired multiply feeding a paired add was fused into one FFMA2,
+// which rounds once where the tile kernel rounds twice).
+// With ADJ the same kernel runs the adjoint step, as the tile kernel's adjoint mode does: the P,
+// Vx and Vz slots hold nu, X and Z, phase A stages B M (X + rdx S+x nu), phase B B M (Z + rdz S+z nu),
+// phase C2 forms the new nu and the imaging sum g += nu_old D_k, and the receivers' residuals of
+// the previous step are added at the end of the chunk.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -64,6 +71,7 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ unsigned sptr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
@@ -107,7 +115,7 @@ struct MarchGeo {
     int nstrip;   // z strips per shot
 };
 
-template <int R, bool VARDEN, bool EDGE>
+template <int R, bool VARDEN, bool EDGE, bool ADJ>
 __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int set, const ShotDev& sd, int shot,
                                            int strip, int xs, int xe, int xb, bool first) {
     float* sP = smem + set * ML::SET + ML::P;
@@ -127,10 +135,6 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
         return (long long)min(max(sd.x0 + x, 0), a.nx_model - 1) * a.mpitch + z;
     };
 
-    float C[R];
-#pragma unroll
-    for (int m = 0; m < R; m++) C[m] = a.coef[m];
-
     // ---- phase A: Vx(t) on columns xb+R .. xb+R+16 (AFD:255-269); thread = z pair x 4 columns ----
     {
         const int zo = 2 * lane;
@@ -146,24 +150,36 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
 #pragma unroll
         for (int o = 0; o < 4; o++) {
             const int x = xb + R + r0 + o;
-            float2 s = mul2(bc(C[0]), sub2(w[o + R], w[o + R - 1]));
+            float2 s = mul2(a.coef2[0], sub2(w[o + R], w[o + R - 1]));
 #pragma unroll
-            for (int m = 1; m < R; m++) s = fma2(bc(C[m]), sub2(w[o + R + m], w[o + R - 1 - m]), s);
+            for (int m = 1; m < R; m++) s = fma2(a.coef2[m], sub2(w[o + R + m], w[o + R - 1 - m]), s);
             float* vrow = sVx + (2 * R + r0 + o) * TZ + zo;
             float2 v = ld2(vrow);
-            float2 b = bc(-a.bx_f);
+            float2 b = bc(-a.bx_f), d = bc(a.den_c);
             if (VARDEN) {
-                const float2 d = __ldg(reinterpret_cast<const float2*>(a.den + midx(x, z0 + zo)));
+                d = __ldg(reinterpret_cast<const float2*>(a.den + midx(x, z0 + zo)));
                 b = make_float2(-a.dtdx / d.x, -a.dtdx / d.y);
             }
-            if (EDGE) {
-                float ax, mx;
-                col_tables<R>(a, x, nx, ax, mx);
-                const float2 sa = ax >= 0.0f ? bc(ax) : az;
-                v = mul2(v, sa);
-                v = mul2(fma2(b, s, v), mul2(bc(mx), mz));
+            float ax = -1.0f, mx = 1.0f;
+            if (EDGE) col_tables<R>(a, x, nx, ax, mx);
+            const float2 sa = EDGE ? (ax >= 0.0f ? bc(ax) : az) : bc(1.0f);
+            float2 out = v;  // the value stored in the Vx (adjoint: X) field
+            if (ADJ) {
+                // staged X'' = B M (X + rdx S+x nu), B = dt / (dx den) (applied in phase C1 for
+                // constant density); stored X = a M X' = a (den dx / dt) X'' (a alone for constant
+                // density, where X'' = M X')
+                v = fma2(bc(a.rdx_f), s, v);
+                if (EDGE) v = mul2(v, mul2(bc(mx), mz));
+                if (VARDEN) v = mul2(v, make_float2(-b.x, -b.y));
+                out = VARDEN ? mul2(v, make_float2(sa.x * d.x * a.adj_xs, sa.y * d.y * a.adj_xs)) : mul2(v, sa);
             } else {
-                v = fma2(b, s, v);
+                if (EDGE) {
+                    v = mul2(v, sa);
+                    v = mul2(fma2(b, s, v), mul2(bc(mx), mz));
+                } else {
+                    v = fma2(b, s, v);
+                }
+                out = v;
             }
             st2(vrow, v);
             // the next chunk's buffer holds Vx(t) from column xb + 16 - R on
@@ -171,8 +187,8 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
             const int gz = z0 + zo;
             if (x >= xs && x < xe && x < nx && gz < nz) {
                 float* dst = a.vx_out + cell(x, gz);
-                if (gz + 1 < nz) st2(dst, v);
-                else dst[0] = v.x;
+                if (gz + 1 < nz) st2(dst, out);
+                else dst[0] = out.x;
             }
         }
     }
@@ -197,9 +213,9 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
         float* vrow = sVz + r * ZW + c0;
 #pragma unroll
         for (int j = 0; j < KZB; j += 2) {
-            float2 s = mul2(bc(C[0]), sub2(pr(9 + j), pr(8 + j)));
+            float2 s = mul2(a.coef2[0], sub2(pr(9 + j), pr(8 + j)));
 #pragma unroll
-            for (int m = 1; m < R; m++) s = fma2(bc(C[m]), sub2(pr(9 + j + m), pr(8 + j - m)), s);
+            for (int m = 1; m < R; m++) s = fma2(a.coef2[m], sub2(pr(9 + j + m), pr(8 + j - m)), s);
             float2 v = ld2(vrow + j);
             float2 nb = bc(-a.bz_f);
             if (VARDEN) {
@@ -207,7 +223,11 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
                 const long long mi = midx(x, gz);
                 nb = make_float2(-(a.dtdz / __ldg(a.den + mi)), -(a.dtdz / __ldg(a.den + mi + 1)));
             }
-            if (EDGE) {
+            if (ADJ) {  // staged Z'' = B M (Z + rdz S+z nu)
+                const float2 mz = EDGE ? make_float2(sMz[c0 + j], sMz[c0 + j + 1]) : bc(1.0f);
+                const float2 cb = VARDEN ? make_float2(-nb.x, -nb.y) : bc(1.0f);
+                v = make_float2(fmaf(a.rdz_f, s.x, v.x) * (mx * mz.x) * cb.x, fmaf(a.rdz_f, s.y, v.y) * (mx * mz.y) * cb.y);
+            } else if (EDGE) {
                 const float2 az = make_float2(sAz[c0 + j], sAz[c0 + j + 1]);
                 const float2 mz = make_float2(sMz[c0 + j], sMz[c0 + j + 1]);
                 v.x *= (ax >= 0.0f ? ax : az.x);
@@ -230,10 +250,10 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
         for (int j = 0; j < 2 * R + 3; j++) w[j] = ld2(sVx + (r0 + j) * TZ + zo);
 #pragma unroll
         for (int o = 0; o < 4; o++) {
-            float2 s = mul2(bc(C[0]), sub2(w[o + R], w[o + R - 1]));
+            float2 s = mul2(a.coef2[0], sub2(w[o + R], w[o + R - 1]));
 #pragma unroll
-            for (int m = 1; m < R; m++) s = fma2(bc(C[m]), sub2(w[o + R + m], w[o + R - m - 1]), s);
-            st2(sX + (r0 + o) * PW + zo, mul2(s, bc(a.rdx_f)));
+            for (int m = 1; m < R; m++) s = fma2(a.coef2[m], sub2(w[o + R + m], w[o + R - m - 1]), s);
+            st2(sX + (r0 + o) * PW + zo, mul2(s, bc(ADJ ? a.adj_cx : a.rdx_f)));
         }
     }
     __syncthreads();
@@ -269,18 +289,97 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int j = 2 * q;
-            float2 s = mul2(bc(C[0]), sub2(pr(8 + j), pr(7 + j)));
+            float2 s = mul2(a.coef2[0], sub2(pr(8 + j), pr(7 + j)));
 #pragma unroll
-            for (int m = 1; m < R; m++) s = fma2(bc(C[m]), sub2(pr(8 + j + m), pr(7 + j - m)), s);
-            sz[q] = mul2(s, bc(a.rdz_f));
+            for (int m = 1; m < R; m++) s = fma2(a.coef2[m], sub2(pr(8 + j + m), pr(7 + j - m)), s);
+            sz[q] = s;  // scaled by rdz (adjoint: adj_cz) where it is added to the x part
         }
         float* pc = sP + r * PW + HZ + zo;
         const float* xc = sX + r * PW + zo;
         float pn[8], divv[8];
         float ax = -1.0f, mx = 1.0f;
         if (EDGE) col_tables<R>(a, x, nx, ax, mx);
+        if (ADJ) {
+            // the adjoint recurrence (stated in adjoint2d.cu): bracket = nu_old / K + S-x(B M X') +
+            // S-z(B M Z'), nu_new = M a K bracket, g += nu_old D_k; stored Z = a M Z'
+            const bool own = x < nx && gz < nz;
+            const long long c = cell(x, gz);
+            float4 dk[2], gk[2];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
+            for (int h = 0; h < 2; h++) {
+                dk[h] = gk[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (own && gz + 7 < nz) {
+                    dk[h] = __ldg(reinterpret_cast<const float4*>(a.adj_div + c + 4 * h));
+                    gk[h] = ld4(a.adj_g + c + 4 * h);
+                }
+            }
+            float nn[8], zo8[8], po8[8], br8[8];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float4 po = ld4(pc + 4 * h);
+                const float4 sx4 = ld4(xc + 4 * h);
+                const float4 vp = vp4[h], dn = dn4[h];
+                const float2 kl = mul2(mul2(mul2(make_float2(dn.x, dn.y), make_float2(vp.x, vp.y)),
+                                            make_float2(vp.x, vp.y)), bc(a.dt));
+                const float2 kh = mul2(mul2(mul2(make_float2(dn.z, dn.w), make_float2(vp.z, vp.w)),
+                                            make_float2(vp.z, vp.w)), bc(a.dt));
+                const float cz = a.adj_cz;
+                const float2 bl = make_float2(
+                    __fadd_rn(__fadd_rn(sx4.x, __fmul_rn(sz[2 * h].x, cz)), __fdividef(po.x, kl.x)),
+                    __fadd_rn(__fadd_rn(sx4.y, __fmul_rn(sz[2 * h].y, cz)), __fdividef(po.y, kl.y)));
+                const float2 bh = make_float2(
+                    __fadd_rn(__fadd_rn(sx4.z, __fmul_rn(sz[2 * h + 1].x, cz)), __fdividef(po.z, kh.x)),
+                    __fadd_rn(__fadd_rn(sx4.w, __fmul_rn(sz[2 * h + 1].y, cz)), __fdividef(po.w, kh.y)));
+                float4 fa4 = make_float4(1.f, 1.f, 1.f, 1.f), fm4 = fa4;  // sponge a and mask M of the cells
+                if (EDGE) {
+                    const float4 az = ld4(sAz + VH + zo + 4 * h), mz = ld4(sMz + VH + zo + 4 * h);
+                    fa4 = ax >= 0.0f ? make_float4(ax, ax, ax, ax) : az;
+                    fm4 = make_float4(mx * mz.x, mx * mz.y, mx * mz.z, mx * mz.w);
+                }
+                const float2 nl = mul2(mul2(bl, kl), mul2(make_float2(fa4.x, fa4.y), make_float2(fm4.x, fm4.y)));
+                const float2 nh = mul2(mul2(bh, kh), mul2(make_float2(fa4.z, fa4.w), make_float2(fm4.z, fm4.w)));
+                float4 zf = fa4;
+                if (VARDEN)
+                    zf = make_float4(fa4.x * dn.x * a.adj_zs, fa4.y * dn.y * a.adj_zs, fa4.z * dn.z * a.adj_zs,
+                                     fa4.w * dn.w * a.adj_zs);
+                const float4 zs = ld4(sVz + r * ZW + VH + zo + 4 * h);
+                const float fzf[4] = {zf.x, zf.y, zf.z, zf.w}, fzs[4] = {zs.x, zs.y, zs.z, zs.w};
+                const float fn[4] = {nl.x, nl.y, nh.x, nh.y}, fb[4] = {bl.x, bl.y, bh.x, bh.y};
+                const float fp[4] = {po.x, po.y, po.z, po.w};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    nn[4 * h + q] = fn[q];
+                    zo8[4 * h + q] = fzs[q] * fzf[q];
+                    po8[4 * h + q] = fp[q];
+                    br8[4 * h + q] = fb[q];
+                }
+            }
+            if (own) {
+                if (x == sd.sx && sd.sz >= gz && sd.sz < gz + 8)
+                    for (int q = 0; q < 8; q++)
+                        if (sd.sz == gz + q) a.adj_lam[(long long)shot * a.nt_max + step] = br8[q];
+                if (gz + 7 < nz) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const float4 d4 = dk[h], g4 = gk[h];
+                        st4(a.adj_g + c + 4 * h, make_float4(fmaf(po8[4 * h], d4.x, g4.x), fmaf(po8[4 * h + 1], d4.y, g4.y),
+                                                           fmaf(po8[4 * h + 2], d4.z, g4.z),
+                                                           fmaf(po8[4 * h + 3], d4.w, g4.w)));
+                        st4(a.p_out + c + 4 * h, make_float4(nn[4 * h], nn[4 * h + 1], nn[4 * h + 2], nn[4 * h + 3]));
+                        st4(a.vz_out + c + 4 * h,
+                            make_float4(zo8[4 * h], zo8[4 * h + 1], zo8[4 * h + 2], zo8[4 * h + 3]));
+                    }
+                } else {
+                    for (int q = 0; q < 8 && gz + q < nz; q++) {
+                        a.adj_g[c + q] = fmaf(po8[q], __ldg(a.adj_div + c + q), a.adj_g[c + q]);
+                        a.p_out[c + q] = nn[q];
+                        a.vz_out[c + q] = zo8[q];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2 && !ADJ; h++) {
             const float4 po = ld4(pc + 4 * h);
             const float4 sx4 = ld4(xc + 4 * h);
             const float4 vp = vp4[h], dn = dn4[h];
@@ -289,8 +388,11 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
                                    bc(-a.dt));
             const float2 kh = mul2(mul2(mul2(make_float2(dn.z, dn.w), make_float2(vp.z, vp.w)), make_float2(vp.z, vp.w)),
                                    bc(-a.dt));
-            const float2 divl = __fadd2_rn(make_float2(sx4.x, sx4.y), sz[2 * h]);
-            const float2 divh = __fadd2_rn(make_float2(sx4.z, sx4.w), sz[2 * h + 1]);
+            const float cz = a.rdz_f;
+            const float2 divl = make_float2(__fadd_rn(sx4.x, __fmul_rn(sz[2 * h].x, cz)),
+                                            __fadd_rn(sx4.y, __fmul_rn(sz[2 * h].y, cz)));
+            const float2 divh = make_float2(__fadd_rn(sx4.z, __fmul_rn(sz[2 * h + 1].x, cz)),
+                                            __fadd_rn(sx4.w, __fmul_rn(sz[2 * h + 1].y, cz)));
             float2 pl = fma2(kl, divl, make_float2(po.x, po.y));
             float2 ph = fma2(kh, divh, make_float2(po.z, po.w));
             if (EDGE) {
@@ -303,7 +405,7 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
             divv[4 * h] = divl.x; divv[4 * h + 1] = divl.y; divv[4 * h + 2] = divh.x; divv[4 * h + 3] = divh.y;
             st4(pc + 4 * h, make_float4(pl.x, pl.y, ph.x, ph.y));  // receivers read the recorded value here
         }
-        if (x < nx && gz < nz) {
+        if (!ADJ && x < nx && gz < nz) {
             if (x == sd.sx && sd.sz >= gz && sd.sz < gz + 8 && step + 1 < sd.nt) {
                 const float inj = sd.inj_scale * __ldg(a.wavelets + sd.wav_off + step + 1);
 #pragma unroll
@@ -336,9 +438,33 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
             }
         }
     }
-    // ---- receivers (AFD:376-377) of this chunk ----
     const int* trp = a.tile_rec_ptr + sd.tile_rec_base + (xb / kTileX) * a.L.ntz + strip;
     const int rb = __ldg(trp), re = __ldg(trp + 1);
+    // ---- adjoint: residual of step k-1 at the receivers of this chunk (AFD:376-377 transposed),
+    // nu += M a K res; several receivers may share a cell, so the adds are atomic ----
+    if (ADJ) {
+        if (step >= 1 && re > rb) {
+            __syncthreads();  // nu_new of the chunk is stored
+            for (int j = rb + tid; j < re; j += kThreads) {
+                const int ridx = a.tile_rec_idx[j];
+                const int rx = a.rec_x[sd.rec_list + ridx];
+                if (rx < xb || rx >= xb + CH) continue;
+                const int rz = a.rec_z[sd.rec_list + ridx];
+                if (rx < R || rx >= nx - R || rz < R || rz >= nz - R) continue;  // M = 0
+                const long long mi = (long long)min(sd.x0 + rx, a.nx_model - 1) * a.mpitch + rz;
+                const float vpv = __ldg(a.vp + mi), dnv = VARDEN ? __ldg(a.den + mi) : a.den_c;
+                float sa = 1.0f;
+                if (rx < a.pml) sa = a.sponge[a.pml - 1 - rx];
+                else if (rx >= nx - a.pml) sa = a.sponge[rx - (nx - a.pml)];
+                else if (rz < a.pml) sa = a.sponge[a.pml - 1 - rz];
+                else if (rz >= nz - a.pml) sa = a.sponge[rz - (nz - a.pml)];
+                const float v = a.adj_res[sd.rec_base + (long long)(step - 1) * sd.nrec + ridx];
+                atomicAdd(a.p_out + cell(rx, rz), dnv * vpv * vpv * a.dt * sa * v);
+            }
+        }
+        return;
+    }
+    // ---- receivers (AFD:376-377) of this chunk ----
     if (re > rb) {
         __syncthreads();
         for (int j = rb + tid; j < re; j += kThreads) {
@@ -351,7 +477,7 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
     }
 }
 
-template <int R, bool VARDEN>
+template <int R, bool VARDEN, bool ADJ>
 __global__ void __launch_bounds__(kThreads, 4)
 acoustic2d_march_kernel(const __grid_constant__ Acou2DArgs a, int active, MarchGeo geo) {
     static_assert(2 * R <= CH && R <= 8, "one chunk carries the 2R columns of Vx the next one needs");
@@ -446,15 +572,15 @@ acoustic2d_march_kernel(const __grid_constant__ Acou2DArgs a, int active, MarchG
         if (tid == 0 && i < nch) issue(i + 1);
         const int xb = xs + (i - 1) * CH;
         const bool xedge = !(xb >= E && xb + CH + R <= nx - E);
-        if (zedge || xedge) chunk_body<R, VARDEN, true>(a, smem, set, sd, shot, strip, xs, xe, xb, i == 0);
-        else chunk_body<R, VARDEN, false>(a, smem, set, sd, shot, strip, xs, xe, xb, i == 0);
+        if (zedge || xedge) chunk_body<R, VARDEN, true, ADJ>(a, smem, set, sd, shot, strip, xs, xe, xb, i == 0);
+        else chunk_body<R, VARDEN, false, ADJ>(a, smem, set, sd, shot, strip, xs, xe, xb, i == 0);
     }
 }
 
-template <int R, bool VARDEN>
+template <int R, bool VARDEN, bool ADJ>
 cudaError_t launch_t(const Acou2DArgs& a, int active, int seg, cudaStream_t st, bool pdl) {
     const size_t smem = sizeof(float) * ML::FLOATS;
-    auto k = acoustic2d_march_kernel<R, VARDEN>;
+    auto k = acoustic2d_march_kernel<R, VARDEN, ADJ>;
     static bool attr[kMaxDevices] = {};
     if (cudaError_t e = smem_attr_once((const void*)k, (int)smem, attr)) return e;
     MarchGeo geo;
@@ -475,22 +601,24 @@ cudaError_t launch_t(const Acou2DArgs& a, int active, int seg, cudaStream_t st, 
 }
 
 template <int R>
-cudaError_t launch_r(const Acou2DArgs& a, int active, bool varden, int seg, cudaStream_t st, bool pdl) {
-    return varden ? launch_t<R, true>(a, active, seg, st, pdl) : launch_t<R, false>(a, active, seg, st, pdl);
+cudaError_t launch_r(const Acou2DArgs& a, int active, bool varden, int seg, cudaStream_t st, bool pdl, bool adj) {
+    if (adj)
+        return varden ? launch_t<R, true, true>(a, active, seg, st, pdl) : launch_t<R, false, true>(a, active, seg, st, pdl);
+    return varden ? launch_t<R, true, false>(a, active, seg, st, pdl) : launch_t<R, false, false>(a, active, seg, st, pdl);
 }
 
 }  // namespace
 
 cudaError_t acoustic2d_march_launch(int radius, const Acou2DArgs& a, int active, bool varden, int seg_cols,
-                                   cudaStream_t st, bool pdl) {
+                                   cudaStream_t st, bool pdl, bool adj) {
     if (seg_cols < CH || seg_cols % CH != 0) return cudaErrorInvalidValue;
     if (a.L.tz != TZ || a.L.tx % CH != 0) return cudaErrorInvalidValue;
     switch (radius) {
-    case 1: return launch_r<1>(a, active, varden, seg_cols, st, pdl);
-    case 2: return launch_r<2>(a, active, varden, seg_cols, st, pdl);
-    case 4: return launch_r<4>(a, active, varden, seg_cols, st, pdl);
-    case 5: return launch_r<5>(a, active, varden, seg_cols, st, pdl);
-    case 8: return launch_r<8>(a, active, varden, seg_cols, st, pdl);
+    case 1: return launch_r<1>(a, active, varden, seg_cols, st, pdl, adj);
+    case 2: return launch_r<2>(a, active, varden, seg_cols, st, pdl, adj);
+    case 4: return launch_r<4>(a, active, varden, seg_cols, st, pdl, adj);
+    case 5: return launch_r<5>(a, active, varden, seg_cols, st, pdl, adj);
+    case 8: return launch_r<8>(a, active, varden, seg_cols, st, pdl, adj);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -69,6 +69,7 @@ struct sfd_ctx {
     int* d_torder = nullptr;   // FMA kernel's forward tile order: interior tiles, then edge tiles
     int tile_major = 1;        // forward steps of the FMA kernel: tile-major over d_torder
     int test_cta = -1, test_step = 0;      // sfd_test_wait_timeout
+    bool q_one_kernel = false;             // viscoacoustic default mode: the one-kernel step (SFD_Q_FUSED=1)
     unsigned long long test_wait_ns = 0;
     int l2_ahead = 0;          // FMA kernel, one tile per CTA: L2 prefetch distance in CTAs
     float* d_rec_tn = nullptr; // [nt][nrec] per shot
@@ -148,6 +149,7 @@ struct sfd_ctx {
     float* d_div = nullptr;     // D_k slots: [C] of the segment being recomputed, then the kept tail
     float* d_adj = nullptr;     // adjoint state: nu0 nu1 x0 x1 z0 z1 (viscoacoustic: 8 adjoints + Qx Qz)
     CUtensorMap adj_tmaps[6];   // TMA descriptors of the acoustic adjoint buffers
+    CUtensorMap adj_mtmaps[6];  // the same buffers with the x-marching kernel's boxes
     float* d_gseg = nullptr;    // per-segment imaging sum (float)
     double* d_gacc = nullptr;   // imaging sum over all segments (double)
     float* d_obs_nt = nullptr;  // observed records as given ([nrec][nt] per shot)
@@ -213,6 +215,10 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQFastSlabs = 13;
 constexpr int kQFastSeg = 256;  // columns per segment of the fused kernel
 bool q_fast(const sfd_ctx* c) { return c->g.scheme == SFD_VISCOAC_2D && !(c->g.flags & SFD_EXACT); }
+// The default mode runs the merged-state pair of kernels (viscoac2d.cu: sigma and r kept summed,
+// all fields in place); SFD_Q_FUSED=1 in the environment selects the one-kernel x-marching step
+// (viscoac2d_fast.cu, sigma, vx, vz ping-pong) instead.
+bool q_fused(const sfd_ctx* c) { return q_fast(c) && c->q_one_kernel; }
 // slab of TMA map b (S0 S1 VX0 VX1 VZ0 VZ1)
 int qfast_slab(int b) { return b < 2 ? kQS + b : b < 4 ? kQVX + (b - 2) : kQVZ + (b - 4); }
 
@@ -351,7 +357,10 @@ Acou2DArgs make_args(const sfd_ctx* c, int step) {
     a.bz_f = (float)a.bz_d;
     a.rdx_f = 1.0f / c->g.dx;
     a.rdz_f = 1.0f / c->g.dz;
-    for (int m = 0; m < c->radius; m++) a.coef[m] = c->coef[m];
+    for (int m = 0; m < c->radius; m++) {
+        a.coef[m] = c->coef[m];
+        a.coef2[m] = make_float2(c->coef[m], c->coef[m]);
+    }
     for (int q = 0; q < c->g.pml && q < 256; q++)
         a.sponge[q] = -0.38 * q * q / (1.0 * c->g.pml * c->g.pml) + 1;
     a.shots = c->d_shots;
@@ -418,6 +427,7 @@ Acou3DArgs make_args3(const sfd_ctx* c, int step) {
 
 // Arguments of the viscoacoustic step (fields in place, eight slabs per shot).
 QArgs make_qargs(const sfd_ctx* c, int step);
+QArgs make_qmerged(const sfd_ctx* c, int step);
 
 // Arguments of the fused viscoacoustic step (default mode), step k: reads parity k & 1 of sigma,
 // vx, vz and writes parity (k + 1) & 1; r and the split parts of the sponge bands in place.
@@ -439,6 +449,21 @@ QFastArgs make_qfast(const sfd_ctx* c, int step) {
     A.tm_vz = c->qtmaps[4 + i];
     A.err_flag = c->d_err;
     return A;
+}
+
+// Arguments of the default (merged-state) viscoacoustic step: vx, vz, sigma and r in place in
+// the first slab of their pairs, the split parts of the sponge bands in the last six slabs.
+QArgs make_qmerged(const sfd_ctx* c, int step) {
+    QArgs a = make_qargs(c, step);
+    const long long fs = (long long)c->nshot * c->L.shot_stride;
+    float* F = c->d_state;
+    a.vx = F + kQVX * fs;
+    a.vz = F + kQVZ * fs;
+    a.sig = F + kQS * fs;
+    a.rsum = F + kQR * fs;
+    a.sx = F + (kQSplit + 0) * fs; a.sz = F + (kQSplit + 1) * fs; a.sr = F + (kQSplit + 2) * fs;
+    a.rx = F + (kQSplit + 3) * fs; a.rz = F + (kQSplit + 4) * fs; a.rr = F + (kQSplit + 5) * fs;
+    return a;
 }
 
 QArgs make_qargs(const sfd_ctx* c, int step) {
@@ -600,7 +625,7 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
         const float* F = ctx->d_state;
         if (q_fast(ctx)) {
-            const int o = (k + 1) & 1;  // parity written by step k
+            const int o = q_fused(ctx) ? (k + 1) & 1 : 0;  // parity written by step k (merged: in place)
             s.nsum = 1;
             s.f[0] = F + (sn.field == SFD_FIELD_VX ? kQVX + o : sn.field == SFD_FIELD_VZ ? kQVZ + o
                           : sn.field == SFD_FIELD_P ? kQS + o : kQR) * fs;
@@ -668,7 +693,7 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         *launches += 2 + (ctx->nrec_max > 0 ? 1 : 0);
         return SFD_OK;
     }
-    if (q_fast(ctx)) {
+    if (q_fused(ctx)) {
         QFastArgs q = make_qfast(ctx, k);
         q.q.slot_to_shot = slots;
         CK(viscoac2d_fast_launch(q, act, kQFastSeg, ctx->stream, pdl_enabled()));
@@ -676,7 +701,7 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
-        QArgs q = make_qargs(ctx, k);
+        QArgs q = q_fast(ctx) ? make_qmerged(ctx, k) : make_qargs(ctx, k);
         q.slot_to_shot = slots;
         CK(viscoac2d_launch_step(q, act, ctx->stream));
         *launches += 2;
@@ -823,7 +848,7 @@ int tune_schedule(sfd_ctx* ctx) {
 
 int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
-    if (ctx->g.scheme == SFD_VISCOAC_2D) return q_fast(ctx) ? 41 : 40;
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return q_fused(ctx) ? 41 : q_fast(ctx) ? 42 : 40;
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
     if (ctx->g.flags & SFD_EXACT) return 1;
@@ -930,9 +955,15 @@ int grad_alloc(sfd_ctx* ctx) {
             int bp[2], bvx[2], bvz[2];
             acoustic2d_fma_boxes(ctx->radius, bp, bvx, bvz);
             const int* boxes[3] = {bp, bvx, bvz};
+            int mp[2], mvx[2], mvz[2];
+            acoustic2d_march_boxes(mp, mvx, mvz);
+            const int* mboxes[3] = {mp, mvx, mvz};
             for (int b = 0; b < 6; b++) {
-                const int rc = encode_field_map(ctx, &ctx->adj_tmaps[b], ctx->d_adj + b * fs, ctx->L, ctx->nshot,
-                                                boxes[b / 2]);
+                int rc = encode_field_map(ctx, &ctx->adj_tmaps[b], ctx->d_adj + b * fs, ctx->L, ctx->nshot,
+                                          boxes[b / 2]);
+                if (!rc)
+                    rc = encode_field_map(ctx, &ctx->adj_mtmaps[b], ctx->d_adj + b * fs, ctx->L, ctx->nshot,
+                                          mboxes[b / 2]);
                 if (rc) return rc;
             }
         }
@@ -1050,6 +1081,9 @@ Acou2DArgs make_adj_args(const sfd_ctx* ctx, const GradRange& r, int k, const fl
     a.tm_p = ctx->adj_tmaps[i];
     a.tm_vx = ctx->adj_tmaps[2 + i];
     a.tm_vz = ctx->adj_tmaps[4 + i];
+    a.tm_mp = ctx->adj_mtmaps[i];
+    a.tm_mvx = ctx->adj_mtmaps[2 + i];
+    a.tm_mvz = ctx->adj_mtmaps[4 + i];
     a.slot_to_shot = r.slots;
     a.tile_major = 0;
     a.tile_order = nullptr;
@@ -1070,8 +1104,12 @@ Acou2DArgs make_adj_args(const sfd_ctx* ctx, const GradRange& r, int k, const fl
 
 int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
     if (ctx->g.scheme == SFD_VISCOAC_2D) return grad_adj_step_q(ctx, r, k, act, div);
-    CK(acoustic2d_fma_launch(ctx->radius, make_adj_args(ctx, r, k, div), act, ctx->varden, ctx->plan.stages,
-                             ctx->stream, true));
+    if (ctx->plan.seg > 0)
+        CK(acoustic2d_march_launch(ctx->radius, make_adj_args(ctx, r, k, div), act, ctx->varden, ctx->plan.seg,
+                                   ctx->stream, pdl_enabled(), true));
+    else
+        CK(acoustic2d_fma_launch(ctx->radius, make_adj_args(ctx, r, k, div), act, ctx->varden, ctx->plan.stages,
+                                 ctx->stream, true));
     return SFD_OK;
 }
 
@@ -1278,7 +1316,7 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     ctx->timing.loop_ms = ms;
     ctx->timing.device_ms = ms;
     ctx->timing.graph = batched ? 1 : 0;
-    ctx->timing.kernel_variant = visco ? 50 : 20 + ctx->plan.stages;
+    ctx->timing.kernel_variant = visco ? 50 : (ctx->plan.seg > 0 ? 23 : 20 + ctx->plan.stages);
     // forward, recomputation of the segments before the kept tail, adjoint
     double pts = 0;
     const int kkeep = ctx->grad_keep * ctx->grad_C;
@@ -2011,6 +2049,8 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
         c->plan.tz = kTileZ;
         c->plan.gz = 8;  // RSG halo 5, rounded for float4 staging
         c->plan.stages = 1;
+        const char* env = std::getenv("SFD_Q_FUSED");
+        c->q_one_kernel = env && std::atoi(env) == 1;
     }
     if (g->scheme == SFD_ELASTIC_2D) {
         // the staggered grid of yang_version is 10th order only (a100..a104, YMOD:23-27)
@@ -2475,8 +2515,8 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         };
         const size_t n = (size_t)sd.nx * nz;
         int rc2;
-        if (q_fast(ctx)) {  // merged fields; the shot's last step wrote parity nt & 1
-            const int o = sd.nt & 1;
+        if (q_fast(ctx)) {  // merged fields; the fused step's last step wrote parity nt & 1
+            const int o = q_fused(ctx) ? sd.nt & 1 : 0;
             if (field == SFD_FIELD_VX) return fetch(kQVX + o, out);
             if (field == SFD_FIELD_VZ) return fetch(kQVZ + o, out);
             if (field == SFD_FIELD_P) return fetch(kQS + o, out);

@@ -87,6 +87,11 @@ struct QArgs {
     int step;
     float* d1_out;                        // optional: Dx1 vx of this step (field layout), for the gradient
     float* d4_out;                        // optional: Dz1 vz of this step
+    // default (merged) mode: sigma = (sx + sz) + sr and r = (rx + rz) + rr kept summed for every
+    // cell; the split parts above are then read and written in the sponge bands only.  NULL:
+    // SFD_EXACT, the split parts everywhere in the reference's operation order.
+    float* sig;
+    float* rsum;
 };
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
 
@@ -271,6 +276,7 @@ struct Acou2DArgs {
     float bx_f, bz_f;       // float versions for the fast path
     float rdx_f, rdz_f;
     float coef[kMaxRadius];
+    float2 coef2[kMaxRadius];  // the same coefficients as (c, c) pairs: operands of paired FP32 math
     float sponge[256];      // sponge profile tab[q] = 1 - 0.38 q^2 / pml^2, q < pml (AFD:164-194)
     const ShotDev* shots;
     const int* slot_to_shot;   // active-slot -> shot id (shots sorted by nt, longest first)
@@ -340,8 +346,9 @@ cudaError_t acoustic2d_fma_launch(int radius, const Acou2DArgs& a, int active, b
 int acoustic2d_fma_gz(int radius);
 // Forward step of the FMA scheme on the x-marching kernel (bit-identical to the tile kernel):
 // one CTA per (shot, 64-wide z strip, segment of seg_cols columns), seg_cols a multiple of 16.
+// adj: the adjoint of step a.step (the adj_* arguments, as acoustic2d_fma_launch's adjoint mode).
 cudaError_t acoustic2d_march_launch(int radius, const Acou2DArgs& a, int active, bool varden, int seg_cols,
-                                   cudaStream_t st, bool pdl);
+                                   cudaStream_t st, bool pdl, bool adj = false);
 // TMA box extents (z, x) of the x-marching kernel's P, Vx and Vz loads.
 void acoustic2d_march_boxes(int box_p[2], int box_vx[2], int box_vz[2]);
 // Forward step of the default (FMA) scheme with the plan's kernel: x-marching when plan.seg > 0,

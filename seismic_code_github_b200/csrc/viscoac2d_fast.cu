@@ -174,6 +174,13 @@ __device__ __forceinline__ void chunk_body(const QFastArgs& A, unsigned char* sm
         const int r = tid >> 3, zb = tid & 7;
         const int x = xb + 5 + r;
         const int cb = 8 + KV * zb;  // sigma column of the first output
+        // buoyancy first: its latency is covered by the stencil
+        float2 bu[KV / 2];
+        {
+            const long long mi = midx(x, z0 - VH + KV * zb);
+#pragma unroll
+            for (int j = 0; j < KV; j += 2) bu[j / 2] = __ldg(reinterpret_cast<const float2*>(a.busg + mi + j));
+        }
         float d1[KV], d2[KV];
         rsg_all<KV, 0, SW, true, true>(sS, r, cb, a.a, d1, d2);
         const bool xin = x >= 0 && x < nx;
@@ -181,13 +188,11 @@ __device__ __forceinline__ void chunk_body(const QFastArgs& A, unsigned char* sm
         if (EDGE) fx = xin ? sponge_factor(x, nx, a.npx, tb + 0 * st, tb + 1 * st) : 0.0f;
         float* vxr = sVx + (CARRY + r) * VW + KV * zb;
         float* vzr = sVz + (CARRY + r) * VW + KV * zb;
-        const long long mi = midx(x, z0 - VH + KV * zb);
 #pragma unroll
         for (int j = 0; j < KV; j += 2) {
-            const float2 bu = __ldg(reinterpret_cast<const float2*>(a.busg + mi + j));
             float2 vx = *reinterpret_cast<const float2*>(vxr + j);
             float2 vz = *reinterpret_cast<const float2*>(vzr + j);
-            const float db0 = a.dt * bu.x, db1 = a.dt * bu.y;
+            const float db0 = a.dt * bu[j / 2].x, db1 = a.dt * bu[j / 2].y;
             vx.x = fmaf(db0, a.hx * d1[j], vx.x);
             vx.y = fmaf(db1, a.hx * d1[j + 1], vx.y);
             vz.x = fmaf(db0, a.hz * d2[j], vz.x);
@@ -230,33 +235,42 @@ __device__ __forceinline__ void chunk_body(const QFastArgs& A, unsigned char* sm
         const int x = xb + r;
         const int gz0 = z0 + KS * zq;
         const int cb = VH + KS * zq;  // velocity column of the first output
+        // model and (away from the bands) the merged state first: their latency is covered by the
+        // stencils
+        const long long mi = midx(x, gz0);
+        const long long c0 = cell(x, gz0);
+        float4 p1v[KS / 4], p2v[KS / 4], sov[KS / 4], rov[KS / 4];
+#pragma unroll
+        for (int h = 0; h < KS / 4; h++) {
+            p1v[h] = __ldg(reinterpret_cast<const float4*>(a.p1 + mi + 4 * h));
+            p2v[h] = __ldg(reinterpret_cast<const float4*>(a.p2 + mi + 4 * h));
+            if (!EDGE) {
+                sov[h] = *reinterpret_cast<const float4*>(A.s_in + c0 + 4 * h);
+                rov[h] = *reinterpret_cast<const float4*>(A.r + c0 + 4 * h);
+            }
+        }
         float d1[KS], d4[KS];
         rsg_all<KS, 1, VW, true, false>(sVx, r, cb, a.a, d1, nullptr);
         rsg_all<KS, 1, VW, false, true>(sVz, r, cb, a.a, nullptr, d4);
-        const long long mi = midx(x, gz0);
         float p1[KS], p2[KS];
 #pragma unroll
-        for (int h = 0; h < KS; h += 4) {
-            const float4 a1 = __ldg(reinterpret_cast<const float4*>(a.p1 + mi + h));
-            const float4 a2 = __ldg(reinterpret_cast<const float4*>(a.p2 + mi + h));
-            p1[h] = a1.x; p1[h + 1] = a1.y; p1[h + 2] = a1.z; p1[h + 3] = a1.w;
-            p2[h] = a2.x; p2[h + 1] = a2.y; p2[h + 2] = a2.z; p2[h + 3] = a2.w;
+        for (int h = 0; h < KS / 4; h++) {
+            p1[4 * h] = p1v[h].x; p1[4 * h + 1] = p1v[h].y; p1[4 * h + 2] = p1v[h].z; p1[4 * h + 3] = p1v[h].w;
+            p2[4 * h] = p2v[h].x; p2[4 * h + 1] = p2v[h].y; p2[4 * h + 2] = p2v[h].z; p2[4 * h + 3] = p2v[h].w;
         }
         const float wav = __ldg(a.wavelets + sd.wav_off + step);
         const bool xin = x < nx;
         const bool xband = EDGE && in_band(x, nx, a.npx);
         const float fxs = EDGE ? sponge_factor(x, nx, a.npx, tb + 4 * st, tb + 5 * st) : 1.0f;
-        const long long c0 = cell(x, gz0);
         // the strip's outputs: contiguous cells c0 .. c0 + 7 of column x
         float sn[KS], rn[KS];
         if (!EDGE) {
             float so[KS], ro[KS];
 #pragma unroll
-            for (int h = 0; h < KS; h += 4) {
-                const float4 s4 = *reinterpret_cast<const float4*>(A.s_in + c0 + h);
-                const float4 r4 = *reinterpret_cast<const float4*>(A.r + c0 + h);
-                so[h] = s4.x; so[h + 1] = s4.y; so[h + 2] = s4.z; so[h + 3] = s4.w;
-                ro[h] = r4.x; ro[h + 1] = r4.y; ro[h + 2] = r4.z; ro[h + 3] = r4.w;
+            for (int h = 0; h < KS / 4; h++) {
+                const float4 s4 = sov[h], r4 = rov[h];
+                so[4 * h] = s4.x; so[4 * h + 1] = s4.y; so[4 * h + 2] = s4.z; so[4 * h + 3] = s4.w;
+                ro[4 * h] = r4.x; ro[4 * h + 1] = r4.y; ro[4 * h + 2] = r4.z; ro[4 * h + 3] = r4.w;
             }
 #pragma unroll
             for (int j = 0; j < KS; j++) {
