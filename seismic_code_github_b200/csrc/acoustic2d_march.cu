@@ -39,7 +39,10 @@ constexpr int TZ = 64;         // strip width (z)
 constexpr int CH = 16;         // chunk (x columns)
 constexpr int HZ = 16;         // z halo of the staged P
 constexpr int VH = 8;          // z halo of the recomputed Vz
-constexpr int PW = TZ + 2 * HZ;        // 96: P row pitch = box width
+// P row pitch = box width: the z range z0-16 .. z0+80 plus 4 columns that are never read, so that
+// in phase C2 (a quarter-warp = two neighbouring columns x four 8-wide z groups, 16-byte loads)
+// the two columns fall on disjoint banks (pitch = 4 mod 8 words)
+constexpr int PW = TZ + 2 * HZ + 4;    // 100
 constexpr int PROWS = 2 * CH;          // 32: P columns per chunk (needs 2R <= CH)
 constexpr int VXROWS = CH + 2 * 8;     // 32: Vx columns per buffer (R <= 8)
 constexpr int NZV = TZ + 2 * VH;       // 80: Vz values per column
@@ -49,9 +52,9 @@ constexpr int KZB = NZV / 8;           // 10: phase B values per thread
 struct ML {
     // floats; every TMA destination is 128-byte aligned
     static constexpr int P = 0;
-    static constexpr int VX = P + PROWS * PW;          // 3072
+    static constexpr int VX = P + PROWS * PW;          // 3200
     static constexpr int VZ = VX + VXROWS * TZ;        // 5120
-    static constexpr int SET = VZ + CH * ZW;           // 6464 floats = 25856 bytes = 202 x 128
+    static constexpr int SET = VZ + CH * ZW;           // 6592 floats = 26368 bytes = 206 x 128
     static constexpr int TAB = 2 * SET;                // az[NZV], mz[NZV]
     static constexpr int BAR = TAB + 2 * NZV;          // two mbarriers (8 bytes each)
     static constexpr int FLOATS = BAR + 4;
@@ -261,7 +264,9 @@ __device__ __forceinline__ void chunk_body(const Acou2DArgs& a, float* smem, int
     // ---- phase C2: P(t) on columns xb .. xb+16 (AFD:289-314, 337-338); thread = column x 8 z ----
     const int step = a.step;
     {
-        const int r = tid >> 3, zq = tid & 7;
+        // lane bits b4..b0: column 2 b4 + b2 of the warp's four, z group b1 b0 + 4 b3 (a quarter-warp
+        // reads two columns whose rows sit 100 or 84 words apart: no bank is hit twice)
+        const int r = 4 * warp + 2 * (lane >> 4) + ((lane >> 2) & 1), zq = (lane & 3) + 4 * ((lane >> 3) & 1);
         const int x = xb + r, zo = 8 * zq, gz = z0 + zo;
         // model values first: their latency is covered by the z-stencil
         float4 vp4[2], dn4[2];
