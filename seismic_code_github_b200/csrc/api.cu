@@ -80,7 +80,7 @@ struct sfd_ctx {
     int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
     CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
     CUtensorMap mtmaps[6];     // the same buffers with the x-marching kernel's boxes
-    CUtensorMap qtmaps[6];     // fused viscoacoustic step: S0 S1 VX0 VX1 VZ0 VZ1 (viscoac2d_fast.cu boxes)
+    CUtensorMap qtmaps[2];     // one-kernel viscoacoustic step: sigma S0 S1 (viscoac2d_fast.cu box)
 
     // 3-D scheme: dense [x][y][pitch] slabs, 8 fields (P, Vx, Vy, Vz, two buffers each)
     Layout3D L3{};
@@ -212,15 +212,19 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // The viscoacoustic scheme runs the fused kernel (viscoac2d_fast.cu) unless SFD_EXACT is set.
 // Its slabs: vx (2 parities), vz (2), sigma (2), r, and the six split parts of the sponge bands.
-constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQFastSlabs = 13;
-constexpr int kQFastSeg = 256;  // columns per segment of the fused kernel
+constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQE = 13, kQFastSlabs = 15;
+constexpr int kQFastSeg = 256;  // columns per segment of the one-kernel step (SFD_QFAST_SEG overrides)
+int q_fast_seg() {
+    const char* env = std::getenv("SFD_QFAST_SEG");
+    const int v = env ? std::atoi(env) : 0;
+    return v >= 16 && v % 16 == 0 ? v : kQFastSeg;
+}
 bool q_fast(const sfd_ctx* c) { return c->g.scheme == SFD_VISCOAC_2D && !(c->g.flags & SFD_EXACT); }
 // The default mode runs the merged-state pair of kernels (viscoac2d.cu: sigma and r kept summed,
 // all fields in place); SFD_Q_FUSED=1 in the environment selects the one-kernel x-marching step
 // (viscoac2d_fast.cu, sigma, vx, vz ping-pong) instead.
 bool q_fused(const sfd_ctx* c) { return q_fast(c) && c->q_one_kernel; }
 // slab of TMA map b (S0 S1 VX0 VX1 VZ0 VZ1)
-int qfast_slab(int b) { return b < 2 ? kQS + b : b < 4 ? kQVX + (b - 2) : kQVZ + (b - 4); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -445,8 +449,8 @@ QFastArgs make_qfast(const sfd_ctx* c, int step) {
     A.q.sx = F + (kQSplit + 0) * fs; A.q.sz = F + (kQSplit + 1) * fs; A.q.sr = F + (kQSplit + 2) * fs;
     A.q.rx = F + (kQSplit + 3) * fs; A.q.rz = F + (kQSplit + 4) * fs; A.q.rr = F + (kQSplit + 5) * fs;
     A.tm_s = c->qtmaps[i];
-    A.tm_vx = c->qtmaps[2 + i];
-    A.tm_vz = c->qtmaps[4 + i];
+    A.e1 = F + kQE * fs;
+    A.e4 = F + (kQE + 1) * fs;
     A.err_flag = c->d_err;
     return A;
 }
@@ -696,8 +700,10 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
     if (q_fused(ctx)) {
         QFastArgs q = make_qfast(ctx, k);
         q.q.slot_to_shot = slots;
-        CK(viscoac2d_fast_launch(q, act, kQFastSeg, ctx->stream, pdl_enabled()));
-        *launches += 1;
+        int nx_max = 0;
+        for (const auto& d : ctx->h_shots) nx_max = std::max(nx_max, d.nx);
+        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), nx_max, ctx->stream, pdl_enabled()));
+        *launches += 2;
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
@@ -2377,12 +2383,11 @@ int sfd_set_shots(sfd_ctx* ctx, int nshot, const sfd_shot* shots) {
         dfree(ctx->d_spg);
         if ((rc = up(&ctx->d_spg, tab))) return rc;
         if (q_fast(ctx)) {
-            int bs[2], bv[2];
-            viscoac2d_fast_boxes(bs, bv);
+            int bs[2];
+            viscoac2d_fast_boxes(bs);
             const long long fs = (long long)nshot * L.shot_stride;
-            for (int b = 0; b < 6; b++) {
-                const int rc2 = encode_field_map(ctx, &ctx->qtmaps[b], ctx->d_state + qfast_slab(b) * fs, L, nshot,
-                                                 b < 2 ? bs : bv);
+            for (int b = 0; b < 2; b++) {
+                const int rc2 = encode_field_map(ctx, &ctx->qtmaps[b], ctx->d_state + (kQS + b) * fs, L, nshot, bs);
                 if (rc2) return rc2;
             }
         }

@@ -95,21 +95,23 @@ struct QArgs {
 };
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
 
-// Default (fused, FMA) viscoacoustic step (viscoac2d_fast.cu): merged sigma and r everywhere,
+// Default (fast, FMA) viscoacoustic step (viscoac2d_fast.cu): merged sigma and r everywhere,
 // split parts in the sponge bands only (q.sx .. q.rr); q.vx / q.vz unused.
 struct QFastArgs {
-    CUtensorMap tm_s, tm_vx, tm_vz;   // this step's input sigma, vx, vz (boxes of viscoac2d_fast_boxes)
+    CUtensorMap tm_s;                 // this step's input sigma (box of viscoac2d_fast_boxes)
     QArgs q;
     const float* s_in; float* s_out;  // merged stress, ping-pong
     const float* vx_in; float* vx_out;
     const float* vz_in; float* vz_out;
     float* r;                         // merged memory variable, in place
+    float* e1; float* e4;             // 0.5/dx Dx1 vx and 0.5/dz Dz1 vz of the cells near the bands
     int* err_flag;                    // set by a CTA whose bounded wait ran out
 };
-// one step of the active shots: one CTA per (shot, 64-wide z strip, segment of `seg` columns)
-cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, cudaStream_t st, bool pdl);
-// TMA box extents (z, x) of the sigma and velocity loads
-void viscoac2d_fast_boxes(int box_s[2], int box_v[2]);
+// one step of the active shots: the step kernel (one CTA per shot, 64-wide z strip and segment of
+// `seg` columns) and the band kernel (one CTA per shot and column, nx_max >= every active nx)
+cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, int nx_max, cudaStream_t st, bool pdl);
+// TMA box extents (z, x) of the sigma loads
+void viscoac2d_fast_boxes(int box_s[2]);
 
 // Visco-elastic split fields (viscoel2d.cu), in the order of their slabs in the state buffer.
 enum EField {
