@@ -69,7 +69,6 @@ struct sfd_ctx {
     int* d_torder = nullptr;   // FMA kernel's forward tile order: interior tiles, then edge tiles
     int tile_major = 1;        // forward steps of the FMA kernel: tile-major over d_torder
     int test_cta = -1, test_step = 0;      // sfd_test_wait_timeout
-    bool q_one_kernel = false;             // viscoacoustic default mode: the one-kernel step (SFD_Q_FUSED=1)
     unsigned long long test_wait_ns = 0;
     int l2_ahead = 0;          // FMA kernel, one tile per CTA: L2 prefetch distance in CTAs
     float* d_rec_tn = nullptr; // [nt][nrec] per shot
@@ -212,19 +211,17 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // The viscoacoustic scheme runs the fused kernel (viscoac2d_fast.cu) unless SFD_EXACT is set.
 // Its slabs: vx (2 parities), vz (2), sigma (2), r, and the six split parts of the sponge bands.
-constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQE = 13, kQFastSlabs = 15;
+constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQFastSlabs = 13;
 constexpr int kQFastSeg = 256;  // columns per segment of the one-kernel step (SFD_QFAST_SEG overrides)
 int q_fast_seg() {
     const char* env = std::getenv("SFD_QFAST_SEG");
     const int v = env ? std::atoi(env) : 0;
     return v >= 16 && v % 16 == 0 ? v : kQFastSeg;
 }
+// The default viscoacoustic mode: the one-kernel x-marching step (viscoac2d_fast.cu; sigma, vx,
+// vz ping-pong, r and the split parts of the sponge bands in place); SFD_EXACT runs the
+// reference-order pair of kernels (viscoac2d.cu, eight split fields in place).
 bool q_fast(const sfd_ctx* c) { return c->g.scheme == SFD_VISCOAC_2D && !(c->g.flags & SFD_EXACT); }
-// The default mode runs the merged-state pair of kernels (viscoac2d.cu: sigma and r kept summed,
-// all fields in place); SFD_Q_FUSED=1 in the environment selects the one-kernel x-marching step
-// (viscoac2d_fast.cu, sigma, vx, vz ping-pong) instead.
-bool q_fused(const sfd_ctx* c) { return q_fast(c) && c->q_one_kernel; }
-// slab of TMA map b (S0 S1 VX0 VX1 VZ0 VZ1)
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -431,7 +428,6 @@ Acou3DArgs make_args3(const sfd_ctx* c, int step) {
 
 // Arguments of the viscoacoustic step (fields in place, eight slabs per shot).
 QArgs make_qargs(const sfd_ctx* c, int step);
-QArgs make_qmerged(const sfd_ctx* c, int step);
 
 // Arguments of the fused viscoacoustic step (default mode), step k: reads parity k & 1 of sigma,
 // vx, vz and writes parity (k + 1) & 1; r and the split parts of the sponge bands in place.
@@ -449,25 +445,8 @@ QFastArgs make_qfast(const sfd_ctx* c, int step) {
     A.q.sx = F + (kQSplit + 0) * fs; A.q.sz = F + (kQSplit + 1) * fs; A.q.sr = F + (kQSplit + 2) * fs;
     A.q.rx = F + (kQSplit + 3) * fs; A.q.rz = F + (kQSplit + 4) * fs; A.q.rr = F + (kQSplit + 5) * fs;
     A.tm_s = c->qtmaps[i];
-    A.e1 = F + kQE * fs;
-    A.e4 = F + (kQE + 1) * fs;
     A.err_flag = c->d_err;
     return A;
-}
-
-// Arguments of the default (merged-state) viscoacoustic step: vx, vz, sigma and r in place in
-// the first slab of their pairs, the split parts of the sponge bands in the last six slabs.
-QArgs make_qmerged(const sfd_ctx* c, int step) {
-    QArgs a = make_qargs(c, step);
-    const long long fs = (long long)c->nshot * c->L.shot_stride;
-    float* F = c->d_state;
-    a.vx = F + kQVX * fs;
-    a.vz = F + kQVZ * fs;
-    a.sig = F + kQS * fs;
-    a.rsum = F + kQR * fs;
-    a.sx = F + (kQSplit + 0) * fs; a.sz = F + (kQSplit + 1) * fs; a.sr = F + (kQSplit + 2) * fs;
-    a.rx = F + (kQSplit + 3) * fs; a.rz = F + (kQSplit + 4) * fs; a.rr = F + (kQSplit + 5) * fs;
-    return a;
 }
 
 QArgs make_qargs(const sfd_ctx* c, int step) {
@@ -629,7 +608,7 @@ int snap_after_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         const long long fs = (long long)ctx->nshot * ctx->L.shot_stride;
         const float* F = ctx->d_state;
         if (q_fast(ctx)) {
-            const int o = q_fused(ctx) ? (k + 1) & 1 : 0;  // parity written by step k (merged: in place)
+            const int o = (k + 1) & 1;  // parity written by step k
             s.nsum = 1;
             s.f[0] = F + (sn.field == SFD_FIELD_VX ? kQVX + o : sn.field == SFD_FIELD_VZ ? kQVZ + o
                           : sn.field == SFD_FIELD_P ? kQS + o : kQR) * fs;
@@ -697,17 +676,15 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         *launches += 2 + (ctx->nrec_max > 0 ? 1 : 0);
         return SFD_OK;
     }
-    if (q_fused(ctx)) {
+    if (q_fast(ctx)) {
         QFastArgs q = make_qfast(ctx, k);
         q.q.slot_to_shot = slots;
-        int nx_max = 0;
-        for (const auto& d : ctx->h_shots) nx_max = std::max(nx_max, d.nx);
-        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), nx_max, ctx->stream, pdl_enabled()));
-        *launches += 2;
+        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), ctx->stream, pdl_enabled()));
+        *launches += 1;
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
-        QArgs q = q_fast(ctx) ? make_qmerged(ctx, k) : make_qargs(ctx, k);
+        QArgs q = make_qargs(ctx, k);
         q.slot_to_shot = slots;
         CK(viscoac2d_launch_step(q, act, ctx->stream));
         *launches += 2;
@@ -854,7 +831,7 @@ int tune_schedule(sfd_ctx* ctx) {
 
 int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_ACOUSTIC_3D) return 30;
-    if (ctx->g.scheme == SFD_VISCOAC_2D) return q_fused(ctx) ? 41 : q_fast(ctx) ? 42 : 40;
+    if (ctx->g.scheme == SFD_VISCOAC_2D) return q_fast(ctx) ? 41 : 40;
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
     if (ctx->g.flags & SFD_EXACT) return 1;
@@ -2055,8 +2032,6 @@ int sfd_create(const sfd_grid* g, int device, sfd_ctx** out) {
         c->plan.tz = kTileZ;
         c->plan.gz = 8;  // RSG halo 5, rounded for float4 staging
         c->plan.stages = 1;
-        const char* env = std::getenv("SFD_Q_FUSED");
-        c->q_one_kernel = env && std::atoi(env) == 1;
     }
     if (g->scheme == SFD_ELASTIC_2D) {
         // the staggered grid of yang_version is 10th order only (a100..a104, YMOD:23-27)
@@ -2520,8 +2495,8 @@ int sfd_get_wavefield(sfd_ctx* ctx, int shot, int field, float* out) {
         };
         const size_t n = (size_t)sd.nx * nz;
         int rc2;
-        if (q_fast(ctx)) {  // merged fields; the fused step's last step wrote parity nt & 1
-            const int o = q_fused(ctx) ? sd.nt & 1 : 0;
+        if (q_fast(ctx)) {  // merged fields; the shot's last step wrote parity nt & 1
+            const int o = sd.nt & 1;
             if (field == SFD_FIELD_VX) return fetch(kQVX + o, out);
             if (field == SFD_FIELD_VZ) return fetch(kQVZ + o, out);
             if (field == SFD_FIELD_P) return fetch(kQS + o, out);

@@ -87,11 +87,6 @@ struct QArgs {
     int step;
     float* d1_out;                        // optional: Dx1 vx of this step (field layout), for the gradient
     float* d4_out;                        // optional: Dz1 vz of this step
-    // default (merged) mode: sigma = (sx + sz) + sr and r = (rx + rz) + rr kept summed for every
-    // cell; the split parts above are then read and written in the sponge bands only.  NULL:
-    // SFD_EXACT, the split parts everywhere in the reference's operation order.
-    float* sig;
-    float* rsum;
 };
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st);
 
@@ -104,12 +99,10 @@ struct QFastArgs {
     const float* vx_in; float* vx_out;
     const float* vz_in; float* vz_out;
     float* r;                         // merged memory variable, in place
-    float* e1; float* e4;             // 0.5/dx Dx1 vx and 0.5/dz Dz1 vz of the cells near the bands
     int* err_flag;                    // set by a CTA whose bounded wait ran out
 };
-// one step of the active shots: the step kernel (one CTA per shot, 64-wide z strip and segment of
-// `seg` columns) and the band kernel (one CTA per shot and column, nx_max >= every active nx)
-cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, int nx_max, cudaStream_t st, bool pdl);
+// one step of the active shots: one CTA per (shot, 64-wide z strip, segment of `seg` columns)
+cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, cudaStream_t st, bool pdl);
 // TMA box extents (z, x) of the sigma loads
 void viscoac2d_fast_boxes(int box_s[2]);
 

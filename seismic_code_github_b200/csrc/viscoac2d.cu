@@ -107,14 +107,11 @@ __device__ __forceinline__ float xs(float u, int x, int nx, int np, const float*
     return u;
 }
 
-// MERGED: the default mode's state, where sigma is kept summed (a.sig) for every cell
-template <bool MERGED>
 __global__ void __launch_bounds__(kThreads) q_velocity_kernel(const __grid_constant__ QArgs a) {
     __shared__ __align__(16) float sS[SMEM];
     TileRef t;
     if (!tile_of(a, t)) return;
-    if (MERGED) stage<1>(sS, a, t, a.sig, nullptr, nullptr);
-    else stage<3>(sS, a, t, a.sx, a.sz, a.sr);  // sigma = (sx + sz) + sr  (QS:1294-1314)
+    stage<3>(sS, a, t, a.sx, a.sz, a.sr);  // sigma = (sx + sz) + sr  (QS:1294-1314)
     __syncthreads();
     const int nx = t.sd.nx, nz = a.nz;
     const float* tb = a.spg;
@@ -235,118 +232,14 @@ __global__ void __launch_bounds__(kThreads, 3) q_stress_kernel(const __grid_cons
     }
 }
 
-// Stress and memory variable of the default mode: sigma (a.sig) and r (a.rsum) are kept summed.
-// Away from the sponge bands, where the split parts only ever appear summed, the sums are updated
-// directly with FMA contraction:
-//   sigma += dt (p1 (d1 + d4) + r_old) + source,   r += f (p2 (d1 + d4) + r_old);
-// in the bands (x <= npx, x >= nx - npx - 1, z <= npz, z >= nz - npz - 1) the split sponge
-// multiplies the x and z parts separately, so there the six split parts are updated in the
-// reference's form (QS:993-1170) and summed into sigma and r.
-__global__ void __launch_bounds__(kThreads, 3) q_stress_merged_kernel(const __grid_constant__ QArgs a) {
-    __shared__ __align__(16) float sVx[SMEM];
-    __shared__ __align__(16) float sVz[SMEM];
-    TileRef t;
-    if (!tile_of(a, t)) return;
-    stage<1>(sVx, a, t, a.vx, nullptr, nullptr);
-    stage<1>(sVz, a, t, a.vz, nullptr, nullptr);
-    __syncthreads();
-    const int nx = t.sd.nx, nz = a.nz;
-    const float* tb = a.spg;
-    const int st = a.spg_stride;
-    const int step = a.step;
-    const float wav = __ldg(a.wavelets + t.sd.wav_off + step);
-    const ShotDev& sd = t.sd;
-    const bool tile_band = t.x0 <= a.npx || t.x0 + TX - 1 >= nx - a.npx - 1 || t.z0 <= a.npz ||
-                           t.z0 + TZ - 1 >= nz - a.npz - 1;
-    for (int j0 = 0; j0 < kPer; j0 += kNBS) {
-        float p1[kNBS], p2[kNBS], so[kNBS], ro[kNBS];
-        long long cc[kNBS];
-        bool ok[kNBS], band[kNBS];
-#pragma unroll
-        for (int u = 0; u < kNBS; u++) {
-            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
-            const int gx = t.x0 + r, gz = t.z0 + z;
-            ok[u] = gx < nx && gz < nz;
-            band[u] = tile_band && (gx <= a.npx || gx >= nx - a.npx - 1 || gz <= a.npz || gz >= nz - a.npz - 1);
-            cc[u] = cell(a, t.shot, gx, gz);
-            if (ok[u]) {
-                const long long mi = (long long)min(sd.x0 + gx, a.nx_model - 1) * a.mpitch + gz;
-                p1[u] = __ldg(a.p1 + mi);
-                p2[u] = __ldg(a.p2 + mi);
-                if (!band[u]) {
-                    so[u] = a.sig[cc[u]];
-                    ro[u] = a.rsum[cc[u]];
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kNBS; u++) {
-            if (!ok[u]) continue;
-            const int i = threadIdx.x + (j0 + u) * kThreads, r = i / TZ, z = i - r * TZ;
-            const int gx = t.x0 + r, gz = t.z0 + z;
-            const long long c = cc[u];
-            const float d1 = rsg<true, 1>(sVx, r + H, z + HZ, a.a, a.hx);
-            const float d4 = rsg<false, 1>(sVz, r + H, z + HZ, a.a, a.hz);
-            float sn, rn;
-            const int bx = gx - sd.stamp_x0, bz = gz - sd.stamp_z0;
-            const bool src = bx >= 0 && bx < sd.stamp_w && bz >= 0 && bz < sd.stamp_h;
-            const float add = src ? __fdiv_rn(fm(fm(wav, __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz)), a.dt),
-                                              a.dz2)
-                                  : 0.0f;
-            if (band[u]) {
-                const float rold = fa(fa(a.rx[c], a.rz[c]), a.rr[c]);
-                float sx = fa(a.sx[c], fm(a.dt, fm(p1[u], d1)));
-                float sz = fa(a.sz[c], fm(a.dt, fm(p1[u], d4)));
-                const float sr = fa(a.sr[c], fm(a.dt, rold));
-                sx = xs(sx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-                sz = xs(sz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
-                if (src) sx = fa(add, sx);
-                float rx = fa(a.rx[c], fm(a.f_mem, fm(p2[u], d1)));
-                float rz = fa(a.rz[c], fm(a.f_mem, fm(p2[u], d4)));
-                const float rr = fa(a.rr[c], fm(a.f_mem, rold));
-                rx = xs(rx, gx, nx, a.npx, tb + 4 * st, tb + 5 * st);
-                rz = xs(rz, gz, nz, a.npz, tb + 6 * st, tb + 7 * st);
-                a.sx[c] = sx; a.sz[c] = sz; a.sr[c] = sr;
-                a.rx[c] = rx; a.rz[c] = rz; a.rr[c] = rr;
-                sn = fa(fa(sx, sz), sr);
-                rn = fa(fa(rx, rz), rr);
-            } else {
-                const float dv = d1 + d4;
-                sn = fmaf(a.dt, fmaf(p1[u], dv, ro[u]), so[u]) + add;
-                rn = fmaf(a.f_mem, fmaf(p2[u], dv, ro[u]), ro[u]);
-            }
-            a.sig[c] = sn;
-            a.rsum[c] = rn;
-            if (a.d1_out) {
-                a.d1_out[c] = d1;
-                a.d4_out[c] = d4;
-            }
-        }
-    }
-    // receivers: strzz = sigma (QM:452-459)
-    const int* trp = a.tile_rec_ptr + sd.tile_rec_base + t.tile;
-    const int rb = trp[0], re = trp[1];
-    if (re > rb) {
-        __syncthreads();
-        for (int j = rb + threadIdx.x; j < re; j += kThreads) {
-            const int ridx = a.tile_rec_idx[j];
-            const long long c = cell(a, t.shot, a.rec_x[sd.rec_list + ridx], a.rec_z[sd.rec_list + ridx]);
-            a.records[sd.rec_base + (long long)step * sd.nrec + ridx] = a.sig[c];
-        }
-    }
-}
-
 }  // namespace
 
 cudaError_t viscoac2d_launch_step(const QArgs& a, int active, cudaStream_t st) {
     dim3 grid(a.L.ntx * a.L.ntz, active);
-    const bool merged = a.sig != nullptr;
-    if (merged) q_velocity_kernel<true><<<grid, kThreads, 0, st>>>(a);
-    else q_velocity_kernel<false><<<grid, kThreads, 0, st>>>(a);
+    q_velocity_kernel<<<grid, kThreads, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (merged) q_stress_merged_kernel<<<grid, kThreads, 0, st>>>(a);
-    else q_stress_kernel<<<grid, kThreads, 0, st>>>(a);
+    q_stress_kernel<<<grid, kThreads, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -105,16 +105,8 @@ def test_wavefield_readback():
     assert p[20, 20] == rec[-1]
 
 
-@pytest.fixture(params=["merged", "one-kernel"])
-def fast_kernel(request, monkeypatch):
-    """The default mode's two implementations: the merged-state kernel pair (default) and the
-    one-kernel x-marching step (SFD_Q_FUSED=1)."""
-    monkeypatch.setenv("SFD_Q_FUSED", "1" if request.param == "one-kernel" else "0")
-    return request.param
-
-
 @pytest.mark.parametrize("seed", [0, 1])
-def test_fused_single_shot_against_fp64(seed, fast_kernel):
+def test_fused_single_shot_against_fp64(seed):
     vp, rho, q = qmodel(seed=seed)
     npx, f0, dt, dx, nt = 11, 20.0, 5e-4, 10.0, 160
     decay = ol.q_decay(f0, dt)
@@ -125,11 +117,11 @@ def test_fused_single_shot_against_fp64(seed, fast_kernel):
     err = rel_l2(got, r64)
     print(f"seed {seed}: fused vs FP64 restatement relL2 {err:.2e}, kernel {t['kernel_variant']}, "
           f"{t['launches']} launches")
-    assert t["kernel_variant"] in (41, 42) and np.abs(got).max() > 0
+    assert t["kernel_variant"] == 41 and np.abs(got).max() > 0
     assert err <= TOL_FAST
 
 
-def test_fused_batched_uneven_shots_apertures_against_fp64(fast_kernel):
+def test_fused_batched_uneven_shots_apertures_against_fp64():
     """Shots of different record lengths and sources near the sponge bands and a grid corner, on
     a grid whose width is not a multiple of the strip or segment sizes."""
     vp, rho, q = qmodel(seed=3, nx=300, nz=150)
@@ -148,7 +140,7 @@ def test_fused_batched_uneven_shots_apertures_against_fp64(fast_kernel):
         assert err <= TOL_FAST, (isxe, isze, err)
 
 
-def test_fused_final_wavefields_against_fp64(fast_kernel):
+def test_fused_final_wavefields_against_fp64():
     """The final stress field (sigma = strxx) after the loop, everywhere on the padded grid
     (sponge bands, corners and interior), against the FP64 restatement."""
     vp, rho, q = qmodel(seed=6, nx=90, nz=76)
