@@ -289,6 +289,7 @@ bool acoustic2d_plan(int radius, Acou2DPlan* plan) {
         plan->gz = acoustic2d_fma_gz(RR);                             \
         plan->stages = 1;                                             \
         plan->seg = 0;                                                \
+        plan->forced = false;                                         \
         return true;
         SFD_PLAN(1) SFD_PLAN(2) SFD_PLAN(4) SFD_PLAN(5) SFD_PLAN(8)
 #undef SFD_PLAN

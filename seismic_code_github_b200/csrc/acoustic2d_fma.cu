@@ -783,7 +783,8 @@ bool pdl_enabled() {
 
 cudaError_t acoustic2d_fwd_launch(const Acou2DPlan& plan, int radius, const Acou2DArgs& a, int active, bool varden,
                                   cudaStream_t st) {
-    if (plan.seg > 0) return acoustic2d_march_launch(radius, a, active, varden, plan.seg, st, pdl_enabled());
+    if (acoustic2d_use_march(plan, a.L, active))
+        return acoustic2d_march_launch(radius, a, active, varden, plan.seg, st, pdl_enabled());
     return acoustic2d_fma_launch(radius, a, active, varden, plan.stages, st);
 }
 

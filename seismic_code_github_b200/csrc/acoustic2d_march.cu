@@ -628,6 +628,18 @@ cudaError_t acoustic2d_march_launch(int radius, const Acou2DArgs& a, int active,
     }
 }
 
+bool acoustic2d_march_fills(const Layout2D& L, int active, int seg_cols) {
+    static int nsm[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return true;
+    if (nsm[dev] == 0 && cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        nsm[dev] = 0;
+        return true;
+    }
+    const long long ctas = (long long)active * L.ntz * ((L.ntx * kTileX + seg_cols - 1) / seg_cols);
+    return ctas >= 4LL * nsm[dev];  // one wave at four CTAs per SM
+}
+
 void acoustic2d_march_boxes(int box_p[2], int box_vx[2], int box_vz[2]) {
     box_p[0] = PW; box_p[1] = PROWS;
     box_vx[0] = TZ; box_vx[1] = CH;

@@ -79,7 +79,7 @@ struct sfd_ctx {
     int* d_err = nullptr;      // bounded-wait timeout flag written by the step kernels
     CUtensorMap tmaps[6];      // TMA descriptors: P0 P1 VX0 VX1 VZ0 VZ1
     CUtensorMap mtmaps[6];     // the same buffers with the x-marching kernel's boxes
-    CUtensorMap qtmaps[2];     // one-kernel viscoacoustic step: sigma S0 S1 (viscoac2d_fast.cu box)
+    CUtensorMap qtmaps[2];     // default viscoacoustic step: sigma S0 S1 (viscoac2d_fast.cu box)
 
     // 3-D scheme: dense [x][y][pitch] slabs, 8 fields (P, Vx, Vy, Vz, two buffers each)
     Layout3D L3{};
@@ -211,16 +211,16 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // The viscoacoustic scheme runs the fused kernel (viscoac2d_fast.cu) unless SFD_EXACT is set.
 // Its slabs: vx (2 parities), vz (2), sigma (2), r, and the six split parts of the sponge bands.
-constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQFastSlabs = 13;
+constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQE = 13, kQFastSlabs = 15;
 constexpr int kQFastSeg = 256;  // columns per segment of the one-kernel step (SFD_QFAST_SEG overrides)
 int q_fast_seg() {
     const char* env = std::getenv("SFD_QFAST_SEG");
     const int v = env ? std::atoi(env) : 0;
     return v >= 16 && v % 16 == 0 ? v : kQFastSeg;
 }
-// The default viscoacoustic mode: the one-kernel x-marching step (viscoac2d_fast.cu; sigma, vx,
-// vz ping-pong, r and the split parts of the sponge bands in place); SFD_EXACT runs the
-// reference-order pair of kernels (viscoac2d.cu, eight split fields in place).
+// The default viscoacoustic mode: the x-marching step kernel and the sponge-band kernel
+// (viscoac2d_fast.cu; sigma, vx, vz ping-pong, r and the split parts of the bands in place);
+// SFD_EXACT runs the reference-order pair of kernels (viscoac2d.cu, eight split fields in place).
 bool q_fast(const sfd_ctx* c) { return c->g.scheme == SFD_VISCOAC_2D && !(c->g.flags & SFD_EXACT); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
@@ -445,6 +445,8 @@ QFastArgs make_qfast(const sfd_ctx* c, int step) {
     A.q.sx = F + (kQSplit + 0) * fs; A.q.sz = F + (kQSplit + 1) * fs; A.q.sr = F + (kQSplit + 2) * fs;
     A.q.rx = F + (kQSplit + 3) * fs; A.q.rz = F + (kQSplit + 4) * fs; A.q.rr = F + (kQSplit + 5) * fs;
     A.tm_s = c->qtmaps[i];
+    A.e1 = F + kQE * fs;
+    A.e4 = F + (kQE + 1) * fs;
     A.err_flag = c->d_err;
     return A;
 }
@@ -679,8 +681,10 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
     if (q_fast(ctx)) {
         QFastArgs q = make_qfast(ctx, k);
         q.q.slot_to_shot = slots;
-        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), ctx->stream, pdl_enabled()));
-        *launches += 1;
+        int nx_max = 0;
+        for (const auto& d : ctx->h_shots) nx_max = std::max(nx_max, d.nx);
+        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), nx_max, ctx->stream, pdl_enabled()));
+        *launches += 2;
         return SFD_OK;
     }
     if (ctx->g.scheme == SFD_VISCOAC_2D) {
@@ -784,6 +788,7 @@ int tune_schedule(sfd_ctx* ctx) {
         if (s == 1 || s == 2) {
             ctx->plan.stages = s;
             ctx->plan.seg = 0;
+            ctx->plan.forced = false;
             return SFD_OK;
         }
     }
@@ -792,6 +797,7 @@ int tune_schedule(sfd_ctx* ctx) {
         if (s >= 16 && s % 16 == 0) {
             ctx->plan.stages = 1;
             ctx->plan.seg = s;
+            ctx->plan.forced = true;
             return SFD_OK;
         }
     }
@@ -809,6 +815,7 @@ int tune_schedule(sfd_ctx* ctx) {
         for (size_t ci = 0; ci < cands.size(); ci++) {
             ctx->plan.stages = cands[ci].stages;
             ctx->plan.seg = cands[ci].seg;
+            ctx->plan.forced = false;
             int rc = prologue(ctx);
             if (rc) return rc;
             for (int k = 0; k < steps; k++) {
@@ -835,7 +842,7 @@ int kernel_variant(const sfd_ctx* ctx) {
     if (ctx->g.scheme == SFD_VISCOEL_2D) return 45;
     if (ctx->g.scheme == SFD_ELASTIC_2D) return 50;
     if (ctx->g.flags & SFD_EXACT) return 1;
-    return ctx->plan.seg > 0 ? 13 : 10 + ctx->plan.stages;
+    return acoustic2d_use_march(ctx->plan, ctx->L, active_shots(ctx, 0)) ? 13 : 10 + ctx->plan.stages;
 }
 
 int run_forward(sfd_ctx* ctx, float* out_dev) {
@@ -1087,7 +1094,7 @@ Acou2DArgs make_adj_args(const sfd_ctx* ctx, const GradRange& r, int k, const fl
 
 int grad_adj_step(sfd_ctx* ctx, const GradRange& r, int k, int act, const float* div) {
     if (ctx->g.scheme == SFD_VISCOAC_2D) return grad_adj_step_q(ctx, r, k, act, div);
-    if (ctx->plan.seg > 0)
+    if (acoustic2d_use_march(ctx->plan, ctx->L, act))
         CK(acoustic2d_march_launch(ctx->radius, make_adj_args(ctx, r, k, div), act, ctx->varden, ctx->plan.seg,
                                    ctx->stream, pdl_enabled(), true));
     else
@@ -1299,7 +1306,9 @@ int run_gradient(sfd_ctx* ctx, const float* obs, float* misfit, float* grad_vp, 
     ctx->timing.loop_ms = ms;
     ctx->timing.device_ms = ms;
     ctx->timing.graph = batched ? 1 : 0;
-    ctx->timing.kernel_variant = visco ? 50 : (ctx->plan.seg > 0 ? 23 : 20 + ctx->plan.stages);
+    ctx->timing.kernel_variant =
+        visco ? 50 : (acoustic2d_use_march(ctx->plan, ctx->L, batched ? active_shots(ctx, 0) : 1) ? 23
+                                                                                             : 20 + ctx->plan.stages);
     // forward, recomputation of the segments before the kept tail, adjoint
     double pts = 0;
     const int kkeep = ctx->grad_keep * ctx->grad_C;

@@ -99,10 +99,12 @@ struct QFastArgs {
     const float* vx_in; float* vx_out;
     const float* vz_in; float* vz_out;
     float* r;                         // merged memory variable, in place
+    float* e1; float* e4;             // 0.5/dx Dx1 vx and 0.5/dz Dz1 vz of the cells near the bands
     int* err_flag;                    // set by a CTA whose bounded wait ran out
 };
-// one step of the active shots: one CTA per (shot, 64-wide z strip, segment of `seg` columns)
-cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, cudaStream_t st, bool pdl);
+// one step of the active shots: the step kernel (one CTA per shot, 64-wide z strip and segment of
+// `seg` columns), then the band kernel (one CTA per shot and column, nx_max >= every active nx)
+cudaError_t viscoac2d_fast_launch(const QFastArgs& a, int active, int seg, int nx_max, cudaStream_t st, bool pdl);
 // TMA box extents (z, x) of the sigma loads
 void viscoac2d_fast_boxes(int box_s[2]);
 
@@ -327,6 +329,7 @@ struct Acou2DPlan {
     int gz;      // z ghost margin the step kernels need (multiple of 4)
     int stages;  // FMA tile kernel schedule (1 or 2)
     int seg;     // > 0: forward steps run the x-marching kernel with segments of `seg` columns
+    bool forced; // seg set by SFD_MARCH_SEG: x-marching even where its grid does not fill the device
 };
 // Model arrays on the device carry this many replicated rows above z = 0 and below z = nz - 1
 // so that vectorised halo reads stay inside the allocation and see finite values.
@@ -346,8 +349,15 @@ cudaError_t acoustic2d_march_launch(int radius, const Acou2DArgs& a, int active,
                                    cudaStream_t st, bool pdl, bool adj = false);
 // TMA box extents (z, x) of the x-marching kernel's P, Vx and Vz loads.
 void acoustic2d_march_boxes(int box_p[2], int box_vx[2], int box_vz[2]);
-// Forward step of the default (FMA) scheme with the plan's kernel: x-marching when plan.seg > 0,
-// else the tile kernel with plan.stages.
+// Whether an x-marching launch of `active` shots fills one wave of the device (four CTAs per SM);
+// with fewer CTAs (one shot of the per-shot baseline, the last shots of an uneven batch) the tile
+// kernel, which gives the same bits, runs instead.
+bool acoustic2d_march_fills(const Layout2D& L, int active, int seg_cols);
+inline bool acoustic2d_use_march(const Acou2DPlan& plan, const Layout2D& L, int active) {
+    return plan.seg > 0 && (plan.forced || acoustic2d_march_fills(L, active, plan.seg));
+}
+// Forward step of the default (FMA) scheme with the plan's kernel: x-marching when plan.seg > 0
+// and the launch fills the device, else the tile kernel with plan.stages.
 cudaError_t acoustic2d_fwd_launch(const Acou2DPlan& plan, int radius, const Acou2DArgs& a, int active, bool varden,
                                   cudaStream_t st);
 // Programmatic dependent launch of consecutive step kernels (SFD_PDL=0 turns it off).

@@ -1,6 +1,6 @@
 // Default (fast) viscoacoustic step of SFD_VISCOAC_2D: the rotated-staggered-grid scheme of
 // forward/Q_forward/Q_multishot_fd_subroutine_fsbc_zy_rotated.f90 (QS:751-835 and its leaves
-// QS:843-1337) with vs = 0, FMA contraction, one kernel per time step.
+// QS:843-1337) with vs = 0, FMA contraction, two kernels per time step.
 //
 // State.  Everywhere: vx, vz (ping-pong), the merged stress sigma = (sx + sz) + sr (QS strxx,
 // ping-pong) and the merged memory variable r = (rx + rz) + rr (in place).  Away from the sponge
@@ -10,24 +10,27 @@
 // d1 = 0.5/dx Dx1 vx, d4 = 0.5/dz Dz1 vz.  In the bands (x <= npx, x >= nx - npx - 1, z <= npz,
 // z >= nz - npz - 1) the split sponge of QS:609-654 multiplies the x and z parts separately, so
 // there the split parts sx, sz, sr, rx, rz, rr are kept (in place) and updated in the reference's
-// form (QS:993-1020, 1135-1170, sponges QS:800-834), and sigma and r are their sums.
+// form by the band kernel, which overwrites sigma and r of those cells.
 //
-// A CTA owns one 64-wide z strip of one shot over a segment of columns and walks down x in chunks
-// of 16 columns.  Chunk xb:
+// Step kernel (viscoac2d_fast_kernel).  A CTA owns one 64-wide z strip of one shot over a segment
+// of columns and walks down x in chunks of 16 columns.  Chunk xb:
 //   phase V: the new velocities of columns [xb+5, xb+21) on z0-8 .. z0+72 from sigma(t-1) on
 //            columns [xb, xb+25) (a TMA box, double-buffered one chunk ahead, no multicast), into a
 //            32-column ring in shared memory (column x in row x & 31) and, for the strip's own
 //            cells, to global memory;
-//   phase S: sigma and r of columns [xb, xb+16) from the ring (columns xb-4 .. xb+21), the source
-//            stamp (QS:1340-1390), and the receivers of the chunk (QM:452-459: strzz = sigma).
+//   phase S: sigma and r of columns [xb, xb+16) from the ring (columns xb-4 .. xb+21).
 // Each velocity column is computed once per segment (a first chunk per segment only computes
 // velocities), only the z halo of 8 on each side of the strip is recomputed.  The rotated
 // stencils (QS:843-966, (0.5/d) sum_m a_m t_m over four-point differences t_m) are evaluated as
-// sums of products, one input column at a time: a thread keeps one column's window in registers
-// and adds each tap with one FMA into the outputs it feeds (ten z values of one column in phase V,
-// four z values of two columns in phase S).  Chunks that touch a sponge band or the grid edge
-// also apply the velocity sponges, zero the velocities outside the grid and run the split update
-// of their band cells.
+// sums of products, one input column at a time: a thread keeps one column's window of 20 values in
+// registers and adds each tap with one FMA into the outputs of its column (ten z values in phase
+// V, eight in phase S).  Chunks that touch a sponge band or the grid edge also apply the velocity
+// sponges and zero the velocities outside the grid, and write d1 and d4 of their cells for the
+// band kernel.
+//
+// Band kernel (viscoac2d_band_kernel), one CTA per (shot, column): the split update of the band
+// cells of the column (QS:993-1020, 1135-1170 with the sponges of QS:800-834 and the source of
+// QS:1340-1390), then the receivers of the column (QM:452-459: strzz = sigma).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -286,110 +289,53 @@ __device__ __forceinline__ void chunk_body(const QFastArgs& A, unsigned char* sm
             }
         }
         const float wav = __ldg(a.wavelets + sd.wav_off + a.step);
-        const float* tb = a.spg;
-        const int st = a.spg_stride;
 #pragma unroll
         for (int u = 0; u < 2; u++) {
-            const int xx = x + u;
-            const float4 so = ld4(sS + (xx - xb) * SW + SH + 4 * zq);  // sigma(t-1) of the cells
+            const float4 so = ld4(sS + (x + u - xb) * SW + SH + 4 * zq);  // sigma(t-1) of the cells
             const float4 ro = rov[u], p1 = p1v[u], p2 = p2v[u];
             const float sof[4] = {so.x, so.y, so.z, so.w}, rof[4] = {ro.x, ro.y, ro.z, ro.w};
             const float p1f[4] = {p1.x, p1.y, p1.z, p1.w}, p2f[4] = {p2.x, p2.y, p2.z, p2.w};
-            // source: the Gaussian stamp into strxx (QS:1340-1390)
-            float add[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            const int bx = xx - sd.stamp_x0;
-            if (bx >= 0 && bx < sd.stamp_w && gz0 + 4 > sd.stamp_z0 && gz0 < sd.stamp_z0 + sd.stamp_h) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int bz = gz0 + j - sd.stamp_z0;
-                    if (bz >= 0 && bz < sd.stamp_h)
-                        add[j] = (wav * __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz) * a.dt) / a.dz2;
-                }
-            }
             float sn[4], rn[4], e1[4], e4[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 e1[j] = a.hx * d1[u][j];
                 e4[j] = a.hz * d4[u][j];
                 const float dv = e1[j] + e4[j];
-                sn[j] = fmaf(a.dt, fmaf(p1f[j], dv, rof[j]), sof[j]) + add[j];
+                sn[j] = fmaf(a.dt, fmaf(p1f[j], dv, rof[j]), sof[j]);
                 rn[j] = fmaf(a.f_mem, fmaf(p2f[j], dv, rof[j]), rof[j]);
             }
-            const long long c = cc[u];
-            if (EDGE && !own[u]) continue;
-            const bool full = !EDGE || gz0 + 4 <= nz;
-            if (EDGE) {
-                // sponge bands: the reference's split update (QS:993-1020, 1135-1170) with the
-                // sponges of QS:800-834; sigma and r of the band cells from their split parts
-                const bool xband = xx <= a.npx || xx >= nx - a.npx - 1;
-                if (xband || gz0 <= a.npz || gz0 + 3 >= nz - a.npz - 1) {
-                    const float fxs = sponge_factor(xx, nx, a.npx, tb + 4 * st, tb + 5 * st);  // spgxn1, spgxp2
-                    float* sp[6] = {a.sx, a.sz, a.sr, a.rx, a.rz, a.rr};
-                    float v[6][4];
+            // source: the Gaussian stamp into strxx (QS:1340-1390); the band kernel adds it again
+            // to the split part where the stamp reaches a band cell
+            const int bx = x + u - sd.stamp_x0;
+            if (bx >= 0 && bx < sd.stamp_w && gz0 + 4 > sd.stamp_z0 && gz0 < sd.stamp_z0 + sd.stamp_h) {
 #pragma unroll
-                    for (int f = 0; f < 6; f++) {
-                        if (full) {
-                            const float4 t = ld4(sp[f] + c);
-                            v[f][0] = t.x; v[f][1] = t.y; v[f][2] = t.z; v[f][3] = t.w;
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 4; j++) v[f][j] = gz0 + j < nz ? sp[f][c + j] : 0.0f;
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int z = gz0 + j;
-                        if (z >= nz || !(xband || z <= a.npz || z >= nz - a.npz - 1)) continue;
-                        const float fz = sponge_factor(z, nz, a.npz, tb + 6 * st, tb + 7 * st);  // spgzn1, spgzp2
-                        const float rold = (v[3][j] + v[4][j]) + v[5][j];
-                        const float sxv = fmaf(a.dt, p1f[j] * e1[j], v[0][j]) * fxs;
-                        const float szv = fmaf(a.dt, p1f[j] * e4[j], v[1][j]) * fz;
-                        const float srv = fmaf(a.dt, rold, v[2][j]);
-                        const float rxv = fmaf(a.f_mem, p2f[j] * e1[j], v[3][j]) * fxs;
-                        const float rzv = fmaf(a.f_mem, p2f[j] * e4[j], v[4][j]) * fz;
-                        const float rrv = fmaf(a.f_mem, rold, v[5][j]);
-                        sn[j] = ((sxv + szv) + srv) + add[j];
-                        rn[j] = (rxv + rzv) + rrv;
-                        v[0][j] = sxv + add[j]; v[1][j] = szv; v[2][j] = srv;
-                        v[3][j] = rxv; v[4][j] = rzv; v[5][j] = rrv;
-                    }
-#pragma unroll
-                    for (int f = 0; f < 6; f++) {
-                        if (full) {
-                            *reinterpret_cast<float4*>(sp[f] + c) = make_float4(v[f][0], v[f][1], v[f][2], v[f][3]);
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 4; j++)
-                                if (gz0 + j < nz) sp[f][c + j] = v[f][j];
-                        }
+                for (int j = 0; j < 4; j++) {
+                    const int bz = gz0 + j - sd.stamp_z0;
+                    if (bz >= 0 && bz < sd.stamp_h) {
+                        const float g = __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz);
+                        sn[j] += (wav * g * a.dt) / a.dz2;
                     }
                 }
             }
-            if (full) {
+            const long long c = cc[u];
+            if (EDGE && !own[u]) continue;
+            if (!EDGE || gz0 + 4 <= nz) {
                 *reinterpret_cast<float4*>(A.s_out + c) = make_float4(sn[0], sn[1], sn[2], sn[3]);
                 *reinterpret_cast<float4*>(A.r + c) = make_float4(rn[0], rn[1], rn[2], rn[3]);
+                if (EDGE) {
+                    *reinterpret_cast<float4*>(A.e1 + c) = make_float4(e1[0], e1[1], e1[2], e1[3]);
+                    *reinterpret_cast<float4*>(A.e4 + c) = make_float4(e4[0], e4[1], e4[2], e4[3]);
+                }
             } else {
 #pragma unroll
                 for (int j = 0; j < 4; j++)
                     if (gz0 + j < nz) {
                         A.s_out[c + j] = sn[j];
                         A.r[c + j] = rn[j];
+                        A.e1[c + j] = e1[j];
+                        A.e4[c + j] = e4[j];
                     }
             }
-        }
-    }
-    // ---- receivers of the chunk: strzz = sigma (QM:452-459) ----
-    const int* trp = a.tile_rec_ptr + sd.tile_rec_base + (xb / kTileX) * a.L.ntz + strip;
-    const int rb = __ldg(trp), re = __ldg(trp + 1);
-    if (re > rb) {
-        __syncthreads();  // this chunk's sigma is in global memory (written by this CTA)
-        for (int j = rb + threadIdx.x; j < re; j += kThreads) {
-            const int ridx = a.tile_rec_idx[j];
-            const int rx = a.rec_x[sd.rec_list + ridx];
-            if (rx < xb || rx >= xb + CH) continue;
-            const int rz = a.rec_z[sd.rec_list + ridx];
-            a.records[sd.rec_base + (long long)a.step * sd.nrec + ridx] =
-                A.s_out[soff + (long long)(rx + a.L.gx) * a.L.pitch + a.L.gz + rz];
         }
     }
 }
@@ -482,6 +428,72 @@ __global__ void __launch_bounds__(kThreads, 4) viscoac2d_fast_kernel(const __gri
     }
 }
 
+// One CTA per (column, active shot): the band cells of the column, then its receivers.
+__global__ void __launch_bounds__(kThreads) viscoac2d_band_kernel(const __grid_constant__ QFastArgs A) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the step kernel's fields are complete
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const QArgs& a = A.q;
+    const int shot = a.slot_to_shot[blockIdx.y];
+    const ShotDev& sd = a.shots[shot];
+    const int x = blockIdx.x;
+    const int nx = sd.nx, nz = a.nz;
+    if (x >= nx) return;
+    const long long soff = (long long)shot * a.L.shot_stride;
+    const long long col = soff + (long long)(x + a.L.gx) * a.L.pitch + a.L.gz;
+    const long long mcol = (long long)min(max(sd.x0 + x, 0), a.nx_model - 1) * a.mpitch;
+    const float* tb = a.spg;
+    const int st = a.spg_stride;
+    const bool xband = x <= a.npx || x >= nx - a.npx - 1;
+    const float fxs = sponge_factor(x, nx, a.npx, tb + 4 * st, tb + 5 * st);  // spgxn1, spgxp2
+    const float wav = __ldg(a.wavelets + sd.wav_off + a.step);
+    const int bx = x - sd.stamp_x0;
+    const bool stamp_col = bx >= 0 && bx < sd.stamp_w;
+    // band z of the column: all of it in an x band, else [0, npz] and [nz - npz - 1, nz)
+    const int top = min(a.npz + 1, nz), bot = max(nz - a.npz - 1, top);
+    const int n = xband ? nz : top + (nz - bot);
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+        const int z = xband ? i : (i < top ? i : bot + (i - top));
+        const long long c = col + z;
+        const float e1 = A.e1[c], e4 = A.e4[c];
+        const float p1 = __ldg(a.p1 + mcol + z), p2 = __ldg(a.p2 + mcol + z);
+        const float fz = sponge_factor(z, nz, a.npz, tb + 6 * st, tb + 7 * st);  // spgzn1, spgzp2
+        const float sx = a.sx[c], sz = a.sz[c], sr = a.sr[c], rx = a.rx[c], rz = a.rz[c], rr = a.rr[c];
+        // the reference's split update (QS:993-1020, 1135-1170) and sponges (QS:800-834)
+        const float rold = (rx + rz) + rr;
+        float sxv = fmaf(a.dt, p1 * e1, sx) * fxs;
+        const float szv = fmaf(a.dt, p1 * e4, sz) * fz;
+        const float srv = fmaf(a.dt, rold, sr);
+        const float rxv = fmaf(a.f_mem, p2 * e1, rx) * fxs;
+        const float rzv = fmaf(a.f_mem, p2 * e4, rz) * fz;
+        const float rrv = fmaf(a.f_mem, rold, rr);
+        float sn = (sxv + szv) + srv;
+        if (stamp_col) {  // the source stamp, after the sponge (QS:1340-1390)
+            const int bz = z - sd.stamp_z0;
+            if (bz >= 0 && bz < sd.stamp_h) {
+                const float add = (wav * __ldg(a.stamps + sd.stamp_off + bx * sd.stamp_h + bz) * a.dt) / a.dz2;
+                sn += add;
+                sxv += add;
+            }
+        }
+        a.sx[c] = sxv; a.sz[c] = szv; a.sr[c] = srv;
+        a.rx[c] = rxv; a.rz[c] = rzv; a.rr[c] = rrv;
+        A.s_out[c] = sn;
+        A.r[c] = (rxv + rzv) + rrv;
+    }
+    // receivers of the column: strzz = sigma (QM:452-459), from the tiles of its 64-column band
+    const int* trp = a.tile_rec_ptr + sd.tile_rec_base + (x / kTileX) * a.L.ntz;
+    const int rb = __ldg(trp), re = __ldg(trp + a.L.ntz);
+    if (re > rb) {
+        __syncthreads();  // this column's band cells are stored
+        for (int j = rb + threadIdx.x; j < re; j += kThreads) {
+            const int ridx = a.tile_rec_idx[j];
+            if (a.rec_x[sd.rec_list + ridx] != x) continue;
+            const int rz = a.rec_z[sd.rec_list + ridx];
+            a.records[sd.rec_base + (long long)a.step * sd.nrec + ridx] = A.s_out[col + rz];
+        }
+    }
+}
+
 cudaError_t launch_pdl(const void* fn, dim3 grid, int smem, cudaStream_t st, bool pdl, void** args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -498,8 +510,8 @@ cudaError_t launch_pdl(const void* fn, dim3 grid, int smem, cudaStream_t st, boo
 
 }  // namespace
 
-cudaError_t viscoac2d_fast_launch(const QFastArgs& A, int active, int seg, cudaStream_t st, bool pdl) {
-    if (seg < CH || seg % CH != 0 || A.q.L.tz != TZ) return cudaErrorInvalidValue;
+cudaError_t viscoac2d_fast_launch(const QFastArgs& A, int active, int seg, int nx_max, cudaStream_t st, bool pdl) {
+    if (seg < CH || seg % CH != 0 || A.q.L.tz != TZ || nx_max <= 0) return cudaErrorInvalidValue;
     static bool attr[kMaxDevices] = {};
     if (cudaError_t e = smem_attr_once((const void*)viscoac2d_fast_kernel, FL::BYTES, attr)) return e;
     QFGeo geo;
@@ -508,8 +520,11 @@ cudaError_t viscoac2d_fast_launch(const QFastArgs& A, int active, int seg, cudaS
     geo.nseg = (A.q.L.ntx * kTileX + seg - 1) / seg;
     QFastArgs a = A;
     void* args[3] = {&a, &active, &geo};
-    return launch_pdl((const void*)viscoac2d_fast_kernel, dim3((unsigned)(active * geo.nstrip * geo.nseg)),
-                      FL::BYTES, st, pdl, args);
+    if (cudaError_t e = launch_pdl((const void*)viscoac2d_fast_kernel, dim3((unsigned)(active * geo.nstrip * geo.nseg)),
+                                   FL::BYTES, st, pdl, args))
+        return e;
+    void* bargs[1] = {&a};
+    return launch_pdl((const void*)viscoac2d_band_kernel, dim3((unsigned)nx_max, (unsigned)active), 0, st, pdl, bargs);
 }
 
 void viscoac2d_fast_boxes(int box_s[2]) {
