@@ -29,7 +29,7 @@ BYTES_PER_POINT = {False: 28, True: 32}  # algorithmic bytes per grid-point upda
 GRAD_BYTES_PER_POINT_STEP = 100          # 2-D acoustic gradient, per point-step of a shot
 GRAD3_BYTES_PER_POINT_STEP = 124         # 3-D: forward 36, recomputation 36 + 4, adjoint 36 + 4 (D) + 8 (sum)
 FALLBACK_HBM_GBS = 6650.0
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "acoustic2d_step_config2.md")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "acoustic2d_march_config2.md")
 
 
 def dist_env():
