@@ -1,5 +1,5 @@
 """Physics pin of the GPU viscoacoustic path (SFD_VISCOAC_2D through the C ABI, in both modes:
-the reference-order kernels of SFD_EXACT and the default fused kernel): measured attenuation and
+the reference-order kernels of SFD_EXACT and the default step and band kernels): measured attenuation and
 dispersion against the 1-SLS law with the reference's Blanch tau (QS:473-551), at Q = 20, 60 and
 200 on a homogeneous model, at the configuration's time step and at half of it (tests/qlaw.py
 states the method and the laws).

@@ -1,7 +1,7 @@
 """GPU viscoacoustic path (SFD_VISCOAC_2D, the vs = 0 reduction of forward/Q_forward) through
 the C ABI, against the restatement of the Fortran code (oracle/q_oracle.cpp).  With SFD_EXACT the
 two kernels per step keep the reference's operation order, so records must be bit-identical to
-the FP32 restatement.  The default mode (one fused kernel per step, merged stress and memory
+the FP32 restatement.  The default mode (x-marching step kernel and sponge-band kernel, merged stress and memory
 variable away from the sponge bands, FMA contraction) must stay within relative L2 <= 1e-5 of
 the FP64 restatement."""
 import numpy as np
