@@ -213,10 +213,22 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 // Its slabs: vx (2 parities), vz (2), sigma (2), r, and the six split parts of the sponge bands.
 constexpr int kQVX = 0, kQVZ = 2, kQS = 4, kQR = 6, kQSplit = 7, kQE = 13, kQFastSlabs = 15;
 constexpr int kQFastSeg = 256;  // columns per segment of the one-kernel step (SFD_QFAST_SEG overrides)
-int q_fast_seg() {
+// Segment length of a step with `act` active shots: 256 columns, halved (down to 64) while the
+// grid would not fill one wave of four CTAs per SM -- the last shots of an uneven batch get more,
+// shorter segments (each pays a warm-up chunk; the results do not depend on the length).
+int q_fast_seg(const sfd_ctx* c, int act) {
     const char* env = std::getenv("SFD_QFAST_SEG");
     const int v = env ? std::atoi(env) : 0;
-    return v >= 16 && v % 16 == 0 ? v : kQFastSeg;
+    if (v >= 16 && v % 16 == 0) return v;
+    static int nsm[kMaxDevices] = {};
+    if (c->device >= 0 && c->device < kMaxDevices && nsm[c->device] == 0 &&
+        cudaDeviceGetAttribute(&nsm[c->device], cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+        nsm[c->device] = 0;
+    const int sms = (c->device >= 0 && c->device < kMaxDevices) ? nsm[c->device] : 0;
+    const long long width = (long long)c->L.ntx * kTileX;
+    int seg = kQFastSeg;
+    while (seg > 64 && sms > 0 && (long long)act * c->L.ntz * ((width + seg - 1) / seg) < 4LL * sms) seg /= 2;
+    return seg;
 }
 // The default viscoacoustic mode: the x-marching step kernel and the sponge-band kernel
 // (viscoac2d_fast.cu; sigma, vx, vz ping-pong, r and the split parts of the bands in place);
@@ -683,7 +695,7 @@ int launch_one_step(sfd_ctx* ctx, int k, const int* slots, int act, long long* l
         q.q.slot_to_shot = slots;
         int nx_max = 0;
         for (const auto& d : ctx->h_shots) nx_max = std::max(nx_max, d.nx);
-        CK(viscoac2d_fast_launch(q, act, q_fast_seg(), nx_max, ctx->stream, pdl_enabled()));
+        CK(viscoac2d_fast_launch(q, act, q_fast_seg(ctx, act), nx_max, ctx->stream, pdl_enabled()));
         *launches += 2;
         return SFD_OK;
     }

@@ -140,6 +140,23 @@ def test_fused_batched_uneven_shots_apertures_against_fp64():
         assert err <= TOL_FAST, (isxe, isze, err)
 
 
+@pytest.mark.parametrize("seg", ["16", "64", "512"])
+def test_fused_segment_length_keeps_bits(monkeypatch, seg):
+    """The step kernel's segment length (the engine halves it for steps with few active shots; a
+    first chunk per segment recomputes the velocities it needs) does not change any bit of the
+    records of the uneven batch above."""
+    vp, rho, q = qmodel(seed=3, nx=300, nz=150)
+    npx, f0, dt, dx = 20, 25.0, 5e-4, 10.0
+    spec = [(npx + 12, npx + 3, 150, 1), (npx + 160, npx + 60, 90, 55), (npx + 290, npx + 140, 120, 134),
+            (3, 4, 100, 1)]
+    monkeypatch.delenv("SFD_QFAST_SEG", raising=False)
+    ref, _ = run_gpu(vp, rho, q, npx, f0, dt, dx, spec, flags=0)
+    monkeypatch.setenv("SFD_QFAST_SEG", seg)
+    got, _ = run_gpu(vp, rho, q, npx, f0, dt, dx, spec, flags=0)
+    for a, b in zip(ref, got):
+        assert np.abs(a).max() > 0 and bits_equal(a, b)
+
+
 def test_fused_final_wavefields_against_fp64():
     """The final stress field (sigma = strxx) after the loop, everywhere on the padded grid
     (sponge bands, corners and interior), against the FP64 restatement."""
