@@ -1,4 +1,4 @@
-"""CPU checks of the FP64 3-D adjoint oracle (oracle/adj3d_oracle.cpp) before it judges the GPU
+"""CPU checks of the FP64 3-D adjoint oracle (oracle/adj3d_oracle.cpp) before it checks the GPU
 3-D gradient: its forward equals the FP64 forward restatement (oracle/afd3d_oracle.cpp), its
 wavelet gradient passes the dot-product test, and its model gradient matches central finite
 differences of its own misfit along a seeded smooth perturbation."""

@@ -1,4 +1,4 @@
-"""CPU checks of the FP64 adjoint oracle (oracle/adj_oracle.cpp) before it is used to judge
+"""CPU checks of the FP64 adjoint oracle (oracle/adj_oracle.cpp) before it is used to check
 the GPU gradient: its forward equals the FP64 forward restatement, the adjoint passes the
 dot-product test, and the gradient matches central finite differences of the misfit."""
 import numpy as np
